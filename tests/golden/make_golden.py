@@ -1,0 +1,269 @@
+"""Write the golden fixtures in this folder by running the REFERENCE's own code.
+
+Run from the repository root, in a container where the reference checkout is
+available (it is read only, nothing is written there):
+
+    LENS_REF=/root/reference python tests/golden/make_golden.py
+
+The reference (s1alknau/lens_sensor) is pure NumPy here (CuPy absent), so its
+primitives are imported and driven for a fixed number of steps in the loop order
+of planar_beads/fdtd2d_core.py:781-847 and planar_3d/fdtd3d_core.py:1106-1158.
+The fixtures pin the oracle (tests/test_oracle_golden.py) and give the GPU
+parity tests seeded inputs whose reference outputs are known.
+
+Outputs:
+  g2d_te.npz, g2d_tm.npz, g3d_tm.npz   setup arrays + fields/phasors after N steps
+  characterization.json                run_beads / run_3d / run_3d_stitched known
+                                       answers at the reference HEAD
+"""
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+REF = os.environ.get('LENS_REF', '/root/reference')
+OUT = os.path.dirname(os.path.abspath(__file__))
+os.environ['PYTHONDONTWRITEBYTECODE'] = '1'
+sys.dont_write_bytecode = True
+for p in (REF, os.path.join(REF, 'planar_beads'), os.path.join(REF, 'planar_3d')):
+    sys.path.insert(0, p)
+
+import fdtd2d_core as d2                     # noqa: E402
+import fdtd3d_core as d3                     # noqa: E402
+from boundaries import make_boundary          # noqa: E402
+from boundaries3d import make_boundary_3d     # noqa: E402
+from common import vcsel                      # noqa: E402
+from common.flux import PlaneFluxDFT, pairs_2d, pairs_3d  # noqa: E402
+
+C0, EPS0, MU0 = d2.C0, d2.EPS0, d2.MU0
+
+
+def _stack(spec):
+    return [dict(name=f'L{i}', t_um=t, n=complex(n), kappa=complex(n).imag, mat=None)
+            for i, (t, n) in enumerate(spec)]
+
+
+# --------------------------------------------------------------------------- 2D
+CASE_2D = dict(
+    te=dict(pol='s', Nx=140, Ny=96, dx=50e-9, tear_m=2.0e-6, wg_n=1.49, wg_um=1.2,
+            stack=[(0.9, 1.333), (0.4, 1.34)], n_sub=1.376, bead=dict(d_um=0.6, x_um=3.3),
+            npml=10, steps=240, lam_nm=850.0, ramp=None, seed=11),
+    tm=dict(pol='p', Nx=140, Ny=96, dx=50e-9, tear_m=2.0e-6, wg_n=1.49, wg_um=1.2,
+            stack=[(0.9, complex(1.333, 0.002)), (0.4, 1.34)], n_sub=1.376,
+            bead=dict(d_um=0.6, x_um=3.3), npml=12, steps=240, lam_nm=850.0, ramp=None, seed=12),
+)
+
+
+def run_2d(c):
+    d2.TEAR_BUFFER = c['tear_m']
+    d2.LAM_LOSS = c['lam_nm'] * 1e-9
+    Nx, Ny, dx = c['Nx'], c['Ny'], c['dx']
+    dt = 0.5 * dx / (C0 * np.sqrt(2))
+    src_ix = c['npml'] + 2
+    x_facet_um, air, zsrc = d2._vcsel_geom_2d(src_ix, dx, 0.0)
+    stack = _stack(c['stack'])
+    bp = {}
+    T_WG = c['wg_um'] * 1e-6
+    eps, sig = d2.build_materials(Nx, Ny, dx, c['wg_n'], 1.59, T_WG, c['bead']['x_um'],
+                                  c['bead']['d_um'], 0.0, True, n_cornea=c['n_sub'],
+                                  input_gap_um=x_facet_um, length_um=Nx * dx * 1e6,
+                                  tm_patch=(bp if c['pol'] == 'p' else None), stack=stack)
+    ce_e, ce_h = d2._coeffs(eps, sig, dt, dx)
+    out = dict(eps=eps, sig=sig, ce_e=ce_e, ce_h=ce_h, dt=dt, dx=dx, src_ix=src_ix,
+               x_facet_um=x_facet_um, zsrc=zsrc)
+    da_x = da_y = None
+    if c['pol'] == 'p':
+        ca_x, ca_y, ch_tm = d2._tm_coeffs(eps, dt, dx)
+        d2._apply_bead_tm(bp, ca_x, ca_y, dt, dx)
+        da_x, da_y = d2._tm_loss(eps, sig, ca_x, ca_y, dt)
+        out.update(ca_x=ca_x, ca_y=ca_y)
+        if da_x is not None:
+            out.update(da_x=da_x, da_y=da_y)
+    f0 = C0 / (c['lam_nm'] * 1e-9)
+    sigma_t = 4 / (2 * np.pi * f0)
+    y0 = -c['tear_m']
+    iy, vs, vs_ey = d2._vcsel_source_2d(Ny, dx, dt, T_WG, src_ix, 0.0, 3.0, c['lam_nm'], 0.0,
+                                        1.0, zsrc, f0, y0_m=y0)
+    src = vs_ey if c['pol'] == 'p' else vs
+    out.update(src_amp=src.amp, src_ph1=src.ph1, src_ph2=src.ph2)
+    bnd = make_boundary('cpml', c['pol'], Nx, Ny, dx, dt, npml=c['npml'], lam_m=c['lam_nm'] * 1e-9)
+    for nm in ('kex', 'bex', 'cex', 'khx', 'bhx', 'chx', 'key', 'bey', 'cey', 'khy', 'bhy', 'chy'):
+        out['cpml_' + nm] = getattr(bnd, nm)
+    Ch = np.float32(dt / (MU0 * dx))
+    Ez = np.zeros((Nx, Ny), np.float32)
+    Hx = np.zeros((Nx, Ny - 1), np.float32)
+    Hy = np.zeros((Nx - 1, Ny), np.float32)
+    Ex = np.zeros((Nx - 1, Ny), np.float32)
+    Ey = np.zeros((Nx, Ny - 1), np.float32)
+    Hz = np.zeros((Nx - 1, Ny - 1), np.float32)
+    omega = 2 * np.pi * f0
+    steps = c['steps']
+    n_dft = 48
+    acc = np.zeros((Nx, Ny), np.complex64)
+    acc_ex = np.zeros((Nx, Ny), np.complex64)
+    acc_I = np.zeros((Nx, Ny), np.float32)
+    box = (slice(40, 60), slice(30, 60))
+    P = np.zeros((), np.float64)
+    flux = PlaneFluxDFT(omega, dt)
+    planes = {'in': 70, 'src_up': src.plane_up, 'src_dn': src.plane_dn}
+    snaps = {}
+    for n in range(steps):
+        t = n * dt
+        env = float(1 - np.exp(-((t / (2 * sigma_t)) ** 2)))
+        if c['pol'] == 'p':
+            bnd.update_H(Ex, Ey, Hz, Ch)
+            if da_x is not None:
+                Ex *= da_x
+                Ey *= da_y
+            bnd.update_E(Ex, Ey, Hz, ca_x, ca_y)
+            src.inject(Ey, t, env)
+            bnd.terminate(Ex, Ey)
+            field = d2._tm_node_field(Ey)
+            I_E = field * field + d2._tm_ex2_node(Ex)
+        else:
+            bnd.update_H(Ez, Hx, Hy, Ch)
+            bnd.update_E(Ez, Hx, Hy, ce_e, ce_h)
+            src.inject(Ez, t, env)
+            bnd.terminate(Ez)
+            field = Ez
+            I_E = field * field
+        P += np.sum(I_E[box], dtype=np.float64)
+        if n >= steps - n_dft:
+            acc += field.astype(np.complex64) * np.exp(-1j * omega * t)
+            if c['pol'] == 'p':
+                acc_ex += d2._tm_ex_node(Ex).astype(np.complex64) * np.exp(-1j * omega * t)
+            for k, il in planes.items():
+                flux.add(k, t, pairs_2d(c['pol'], il, Ez=Ez, Hy=Hy, Ey=Ey, Hz=Hz))
+        if n >= steps // 2:
+            acc_I += I_E
+        if n + 1 in (steps // 2, steps):
+            tag = f'_n{n + 1}'
+            if c['pol'] == 'p':
+                snaps.update({'Ex' + tag: Ex.copy(), 'Ey' + tag: Ey.copy(), 'Hz' + tag: Hz.copy()})
+            else:
+                snaps.update({'Ez' + tag: Ez.copy(), 'Hx' + tag: Hx.copy(), 'Hy' + tag: Hy.copy()})
+    out.update(snaps)
+    out.update(acc=acc, acc_I=acc_I, P_box=P, n_dft=n_dft,
+               flux_in=flux.flux('in'), flux_up=flux.flux('src_up'), flux_dn=flux.flux('src_dn'))
+    if c['pol'] == 'p':
+        out['acc_ex'] = acc_ex
+    return out
+
+
+# --------------------------------------------------------------------------- 3D
+CASE_3D = dict(pol='p', Nx=64, Ny=48, Nz=40, dx_nm=50.0, t_wg_um=0.8, air_um=0.5,
+               tear_um=1.1, stack=[(0.6, complex(1.333, 0.003)), (0.3, 1.34)], n_sub=1.376,
+               wg_n=1.49, bead=dict(x_um=1.9, d_um=0.5, n=1.59, z_um=0.1), npml=10,
+               steps=90, lam_nm=850.0)
+
+
+def run_3d_case(c):
+    Nx, Ny, Nz = c['Nx'], c['Ny'], c['Nz']
+    dx_um = c['dx_nm'] / 1000.0
+    dx = c['dx_nm'] * 1e-9
+    dt = 0.5 * dx / (C0 * np.sqrt(3))
+    LAM = c['lam_nm'] * 1e-9
+    d3.LAM_LOSS = LAM
+    y0_um = -c['tear_um']
+    z0_um = -Nz * dx_um / 2.0
+    n_sp = d3._sponge_cells(None, 1.2, dx_um, (Nx, Ny, Nz), warn=False)
+    x_src_um, x_wg_start_um, air, zsrc = d3._vcsel_geom_3d(n_sp, dx_um, 0.0)
+    stack = _stack(c['stack'])
+    tp = {}
+    eps = d3.build_eps3d(Nx, Ny, Nz, dx_um, y0_um, z0_um, c['wg_n'], c['t_wg_um'],
+                         0.0, 0.0, 0.0, 1.48, 1.333, 1.34, c['n_sub'], c['bead'],
+                         x_wg_start_um=x_wg_start_um, tensor_patch=tp, stack=stack)
+    eps_r, eim = d3._split_eps3(eps)
+    inv, da = d3._inv_loss(eps_r, eim, dt, dx, LAM)
+    ce_x, ce_y, ce_z = d3._ce_arrays(inv, tp, dt, dx, dx_um, da=da)
+    da3 = d3._stagger_da(da)
+    pol, Nj, Nk = d3._resolve_pol(c['pol'], Ny, Nz)
+    src_ix, j_src, k_src, vs = d3._build_gauss_source(
+        n_sp, c['t_wg_um'], y0_um, z0_um, dx_um, dx, LAM, Nj, Nk, 1.0, 1.0, 0.0, 0.0, 0.0,
+        n_src_fn=lambda j, k: 1.0, pol=pol, dt=dt, z_prop_um=zsrc)
+    bnd = make_boundary_3d('cpml', dx, dt, d3.ALL_FACES, shape=(Nx, Ny, Nz), lam_m=LAM)
+    Ch = np.float32(dt / (MU0 * dx))
+    Ex = np.zeros((Nx - 1, Ny, Nz), np.float32)
+    Ey = np.zeros((Nx, Ny - 1, Nz), np.float32)
+    Ez = np.zeros((Nx, Ny, Nz - 1), np.float32)
+    Hx = np.zeros((Nx, Ny - 1, Nz - 1), np.float32)
+    Hy = np.zeros((Nx - 1, Ny, Nz - 1), np.float32)
+    Hz = np.zeros((Nx - 1, Ny - 1, Nz), np.float32)
+    f0 = C0 / LAM
+    omega = 2 * np.pi * f0
+    sigma_t = 4 / (2 * np.pi * f0)
+    steps = c['steps']
+    n_dft = 30
+    acc = np.zeros_like(Ey, dtype=np.complex64)
+    Iavg = np.zeros_like(Ey)
+    P = np.zeros((), np.float64)
+    zs = slice(n_sp, -n_sp) if 2 * n_sp < Nz else slice(0, Nz)
+    box = (slice(36, 44), slice(20, 34), zs)
+    flux = PlaneFluxDFT(omega, dt)
+    planes = {'in': 40, 'src_up': vs.plane_up, 'src_dn': vs.plane_dn}
+    out = dict(eps=eps, ce_x=ce_x, ce_y=ce_y, ce_z=ce_z, dt=dt, dx=dx, n_sp=n_sp,
+               src_ix=src_ix, x_wg_start_um=x_wg_start_um, zsrc=zsrc,
+               src_amp=vs.amp, src_ph1=vs.ph1, src_ph2=vs.ph2)
+    if da3 is not None:
+        out.update(da_x=da3[0], da_y=da3[1], da_z=da3[2])
+    for ax in 'xyz':
+        for t in ('b', 'c', 'k'):
+            for s in ('e', 'h'):
+                out[f'cpml_{t}{ax}{s}'] = getattr(bnd, f'{t}{ax}{s}')
+    for n in range(steps):
+        t = n * dt
+        env = float(1 - np.exp(-((t / (2 * sigma_t)) ** 2)))
+        bnd.step(Ex, Ey, Ez, Hx, Hy, Hz, ce_x, ce_y, ce_z, Ch, da=da3)
+        vs.inject(Ey, t, env)
+        P += d3._box_E2(Ex, Ey, Ez, *box)
+        if n >= steps // 2 and (n - steps // 2) % 3 == 0:
+            d3._accum_E2(Iavg, Ex, Ey, Ez)
+        if n >= steps - n_dft:
+            acc += Ey.astype(np.complex64) * np.exp(-1j * omega * t)
+            for k, il in planes.items():
+                flux.add(k, t, pairs_3d(il, Ey, Ez, Hy, Hz))
+    out.update(Ex=Ex, Ey=Ey, Ez=Ez, Hx=Hx, Hy=Hy, Hz=Hz, acc=acc, Iavg=Iavg, P_box=P,
+               n_dft=n_dft, flux_in=flux.flux('in'), flux_up=flux.flux('src_up'),
+               flux_dn=flux.flux('src_dn'))
+    return out
+
+
+def characterization():
+    """The reference's own golden-master cases (tests/test_characterization.py:73-116)
+    re-run at HEAD; its stored constants are stale, these are the live values."""
+    sys.path.insert(0, os.path.join(REF, 'tests'))
+    import test_characterization as tc
+    prev = os.getcwd()
+    tmp = tempfile.mkdtemp(prefix='lens_golden_')
+    try:
+        os.chdir(tmp)
+        r3 = tc._run_3d_case()
+        r2 = tc._run_2d_case()
+    finally:
+        os.chdir(prev)
+        shutil.rmtree(tmp, ignore_errors=True)
+    return dict(case_3d=r3, case_2d=r2)
+
+
+def main():
+    ch = characterization()          # first: the cases below change module globals
+    with open(os.path.join(OUT, 'characterization.json'), 'w') as f:
+        json.dump(ch, f, indent=1)
+    print('wrote characterization.json')
+    for name, c in CASE_2D.items():
+        o = run_2d(c)
+        o = {k: (np.asarray(v) if not isinstance(v, (int, float)) else np.asarray(v)) for k, v in o.items()}
+        np.savez_compressed(os.path.join(OUT, f'g2d_{name}.npz'), **o)
+        print('wrote', name, sorted(o))
+    o = run_3d_case(CASE_3D)
+    np.savez_compressed(os.path.join(OUT, 'g3d_tm.npz'), **{k: np.asarray(v) for k, v in o.items()})
+    print('wrote g3d_tm')
+    with open(os.path.join(OUT, 'cases.json'), 'w') as f:
+        json.dump(dict(d2=CASE_2D, d3=CASE_3D), f, indent=1, default=lambda v: [v.real, v.imag])
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,185 @@
+/*
+ * lens_fdtd.h - C ABI of the B200 (sm_100a) FDTD time-stepping engine.
+ *
+ * Drop-in for the hot loop of s1alknau/lens_sensor's native solver:
+ *   2D TE  CPML step   planar_beads/boundaries.py:164-221 (CPML_TE.update_H/update_E/terminate)
+ *                      planar_beads/fused2d.py:41-68, 105-115 (te_update_H / te_update_E)
+ *   2D TM  CPML step   planar_beads/boundaries.py:224-274, fused2d.py:69-94, 118-126
+ *                      + loss damping planar_beads/fdtd2d_core.py:796-797
+ *   3D     CPML step   planar_3d/boundaries3d.py:262-362 (CPML_3D.step/step_H/step_E)
+ *   source             common/vcsel.py:151-156 (HuygensSource.inject)
+ *   epilogues          planar_beads/fdtd2d_core.py:834-850, planar_3d/fdtd3d_core.py:1139-1158,
+ *                      common/flux.py:19-57 (PlaneFluxDFT.add)
+ *
+ * Conventions
+ *  - Plain C: no CUDA or torch types.  Every pointer is a DEVICE pointer owned by
+ *    the caller (the Python host allocates with PyTorch); the library allocates
+ *    nothing and keeps no global state, so distinct solves are independent.
+ *  - Every entry point returns an int status (LENS_OK = 0, negative on error) and
+ *    never aborts.  `stream` is a cudaStream_t passed as void* (NULL = legacy
+ *    default stream); all work is enqueued on it asynchronously.
+ *  - Layout: every 2D array of a grid is stored as nx rows of `pitch` floats
+ *    (pitch >= ny, multiple of 32); every 3D array as nx*ny rows of `pitch`
+ *    floats along z (pitch >= nz, multiple of 32).  A staggered component
+ *    occupies the leading part of its rows (e.g. 2D Hx = (nx, ny-1)); padding is
+ *    never read for a valid update and stays zero.
+ *  - CPML psi lives only in the strips where the profile's c != 0 (leading `lo`
+ *    and trailing `hi` entries of the profile); the strip arrays are documented
+ *    per field below.  Outside the strips psi is identically zero.
+ */
+#ifndef LENS_FDTD_H
+#define LENS_FDTD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LENS_OK 0
+#define LENS_ERR_ARG (-1)
+#define LENS_ERR_CUDA (-2)
+#define LENS_ERR_SIZE (-3)
+
+#define LENS_MAX_BOX 4
+#define LENS_MAX_PLANE 4
+
+/* One staggering of one CPML axis: b, c and 1/kappa, each of length n. */
+typedef struct {
+    const float *b, *c, *ik;
+    int n;      /* profile length (N integer nodes, or N-1 half nodes) */
+    int lo, hi; /* psi strip widths: entries [0,lo) and [n-hi,n) carry psi */
+} LensProfile;
+
+typedef struct {
+    LensProfile e; /* integer nodes, length N     (boundaries.py:104-151 "e") */
+    LensProfile h; /* half nodes,    length N - 1 (boundaries.py:104-151 "h") */
+} LensAxis;
+
+/* Per-step scalars computed once on the host (float64 math, float32 stored).
+ * Step n reads entry n - t0 (0 <= n - t0 < n_table). */
+typedef struct {
+    const float *wt;  /* float32(omega * n * dt)        (vcsel.py:154-155)       */
+    const float *env; /* source envelope at t = n*dt    (fdtd2d_core.py:784-787)  */
+    const float *pe;  /* (re, im) of exp(-i w t_n)              : DFT of E       */
+    const float *ph;  /* (re, im) of exp(-i w (t_n - dt/2))     : DFT of H (flux) */
+    int t0, n_table;
+} LensStepTable;
+
+/* One-way Huygens soft-source pair on x-planes ix (+) and ix+1 (-). */
+typedef struct {
+    int ix;                        /* -1: no source                       */
+    const float *amp, *ph1, *ph2;  /* 2D: length nj; 3D: (nj, pitch_k)    */
+    int nj, nk, pitch_k;           /* source plane extent (2D: nk = 1)    */
+} LensSource;
+
+/* ---------------------------------------------------------------- 2D grids */
+typedef struct {
+    int nx, ny, pitch;           /* node counts; row pitch of every array      */
+    float *ez, *hx, *hy;         /* Ez (nx,ny) Hx (nx,ny-1) Hy (nx-1,ny)       */
+    const float *ce_e, *ce_h;    /* Ce_E, Ce_H (nx,ny)  fdtd2d_core.py:262-270 */
+    float ch;                    /* dt/(mu0 dx)                                */
+    LensAxis ax, ay;
+    float *psi_hxy;              /* (nx, ay.h.lo+ay.h.hi)                      */
+    float *psi_hyx;              /* (ax.h.lo+ax.h.hi, pitch)                   */
+    float *psi_ezx;              /* (ax.e.lo+ax.e.hi, pitch)                   */
+    float *psi_ezy;              /* (nx, ay.e.lo+ay.e.hi)                      */
+    int pec[4];                  /* PEC on x-lo, x-hi, y-lo, y-hi              */
+    LensSource src;              /* drives Ez                                  */
+} LensTE2D;
+
+typedef struct {
+    int nx, ny, pitch;
+    float *ex, *ey, *hz;         /* Ex (nx-1,ny) Ey (nx,ny-1) Hz (nx-1,ny-1)   */
+    const float *ca_x, *ca_y;    /* Ca_ex (nx-1,ny) Ca_ey (nx,ny-1)            */
+    const float *da_x, *da_y;    /* loss damping D or NULL (lossless)          */
+    float ch;
+    LensAxis ax, ay;
+    float *psi_hzx;              /* (ax.h.lo+ax.h.hi, pitch)                   */
+    float *psi_hzy;              /* (nx, ay.h.lo+ay.h.hi)                      */
+    float *psi_exy;              /* (nx, ay.e.lo+ay.e.hi)                      */
+    float *psi_eyx;              /* (ax.e.lo+ax.e.hi, pitch)                   */
+    int pec[4];
+    LensSource src;              /* drives Ey (source on the Ey grid)          */
+} LensTM2D;
+
+/* Epilogue of a 2D step (all optional; a NULL pointer or empty window = off).
+ * "field" is Ez (TE) or Ey averaged onto the nodes (TM, fdtd2d_core.py:458-465);
+ * I = |E|^2 on the nodes (TE Ez^2, TM field^2 + <Ex^2> fdtd2d_core.py:477-486). */
+typedef struct {
+    int nbox;
+    int box[LENS_MAX_BOX][4];    /* [x0,x1) x [y0,y1) on the nodes            */
+    double *box_acc;             /* nbox float64 sums of I, added every step  */
+    int dft_n0, dft_n1;          /* steps [n0,n1): acc += field * pe[n]        */
+    float *dft;                  /* (nx, pitch) x {re, im, c_re, c_im}: Kahan  */
+    float *dft_ex;               /* TM: same for Ex on the nodes, or NULL      */
+    int prev_n0, prev_n1;        /* second window (CW convergence test)        */
+    float *dft_prev;             /* same layout as dft, or NULL                */
+    int iavg_n0;                 /* steps >= iavg_n0: iavg += I                */
+    float *iavg;                 /* (nx, pitch) or NULL                        */
+    int nplane;
+    int plane[LENS_MAX_PLANE];   /* x-planes il (1 <= il <= nx-2)              */
+    double *plane_acc;           /* per plane: 4 rows of pitch doubles:
+                                    E re, E im, H re, H im (H = mean of il-1, il);
+                                    accumulated during the dft window          */
+} LensEpi2D;
+
+/* Advance `nsteps` steps starting at step n0 (t = n*dt, n = n0 ... n0+nsteps-1). */
+int lens_te2d_step(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                   int n0, int nsteps, void *stream);
+int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                   int n0, int nsteps, void *stream);
+
+/* ---------------------------------------------------------------- 3D grid */
+typedef struct {
+    int nx, ny, nz, pitch;       /* node counts; z pitch of every array        */
+    float *ex, *ey, *ez;         /* Ex (nx-1,ny,nz) Ey (nx,ny-1,nz) Ez (nx,ny,nz-1) */
+    float *hx, *hy, *hz;         /* Hx (nx,ny-1,nz-1) Hy (nx-1,ny,nz-1) Hz (nx-1,ny-1,nz) */
+    const float *ce_x, *ce_y, *ce_z;  /* staggered update factors (fdtd3d_core.py:305-378) */
+    const float *da_x, *da_y, *da_z;  /* staggered loss damping or NULL (fdtd3d_core.py:606-613) */
+    float ch;
+    LensAxis ax, ay, az;
+    /* psi strips (boundaries3d.py:286-302); w = lo+hi of the profile named:
+       z-strips  hx_z, hy_z (az.h)  ex_z, ey_z (az.e):  (nx, ny, w)      floats
+       y-strips  hx_y, hz_y (ay.h)  ex_y, ez_y (ay.e):  (nx, w, pitch)   floats
+       x-strips  hy_x, hz_x (ax.h)  ey_x, ez_x (ax.e):  (w, ny, pitch)   floats
+       (row-major; rows belonging to no valid cell of the component are unused) */
+    float *psi_hx_z, *psi_hx_y, *psi_hy_x, *psi_hy_z, *psi_hz_y, *psi_hz_x;
+    float *psi_ex_y, *psi_ex_z, *psi_ey_z, *psi_ey_x, *psi_ez_x, *psi_ez_y;
+    int pec[6];                  /* PEC on x-lo, x-hi, y-lo, y-hi, z-lo, z-hi  */
+    LensSource src;              /* plane (nj, nk) of the driven component     */
+    int src_comp;                /* 0 Ex, 1 Ey, 2 Ez                           */
+} LensGrid3D;
+
+typedef struct {
+    int nbox;
+    int box[LENS_MAX_BOX][6];    /* [x0,x1) [y0,y1) [z0,z1), applied to Ex, Ey, Ez */
+    double *box_acc;             /* nbox sums of Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481) */
+    int dft_n0, dft_n1;
+    float *dft[3];               /* per component (or NULL): (nx,ny,pitch) x {re,im,c_re,c_im} */
+    int conv_k;                  /* z index of the convergence plane (driven component) */
+    int prev_n0, prev_n1;        /* previous window for the convergence test */
+    float *conv_prev, *conv_last;/* (nx, nj) x {re,im,c_re,c_im} planes or NULL */
+    int nplane;
+    int plane[LENS_MAX_PLANE];
+    double *plane_acc;           /* per plane: 2 pairs (Ey/Hz, Ez/Hy) x 4 x (ny*pitch) doubles */
+} LensEpi3D;
+
+int lens_fdtd3d_step(const LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
+                     int n0, int nsteps, void *stream);
+
+/* Iavg += |E|^2 of all three components mapped onto the grid of component
+ * `target` (1 Ey, 2 Ez) exactly as fdtd3d_core.py:438-474 (_sq_on_grid/_accum_E2). */
+int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, float *iavg, void *stream);
+
+/* Library identity and error text. */
+int lens_version(void);
+const char *lens_status_string(int status);
+
+/* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
+ * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D.
+ * Writes min(n, 9) entries and returns 9 (bindings check their mirrors). */
+int lens_abi_sizes(int *sizes, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LENS_FDTD_H */

@@ -1,0 +1,356 @@
+"""Device state of one FDTD solve and its stepping through liblens_fdtd.so.
+
+PyTorch provides the device buffers and the stream; every update runs in the
+hand-written sm_100a kernels behind the C ABI (include/lens_fdtd.h).  There is
+no CPU path: constructing a grid without a CUDA device or without the built
+library raises.
+
+Arrays are stored padded (rows of ``pitch`` floats, pitch a multiple of 32);
+the ``view`` helpers return the reference-shaped slices
+(planar_beads/fdtd2d_core.py:761-768, planar_3d/fdtd3d_core.py:957-962).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .physics import MU0
+
+F32 = np.float32
+
+
+def pitch_of(n):
+    return (int(n) + 31) // 32 * 32
+
+
+def _device(device=None):
+    if not torch.cuda.is_available():
+        raise N.LensError('lens_sensor_b200 needs a CUDA device (no CPU fallback)')
+    return torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
+
+
+def _ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream_ptr(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _pad_upload(a, shape, dev):
+    """Zero tensor of `shape` with the numpy array `a` in its leading corner."""
+    t = torch.zeros(shape, dtype=torch.float32, device=dev)
+    a = np.ascontiguousarray(a, dtype=F32)
+    t[tuple(slice(0, s) for s in a.shape)] = torch.from_numpy(a).to(dev, non_blocking=False)
+    return t
+
+
+def strip_widths(c):
+    """Leading / trailing run of c != 0 (the psi strips, boundaries3d.py:209-221)."""
+    c = np.asarray(c)
+    n = len(c)
+    lo = 0
+    while lo < n and c[lo] != 0.0:
+        lo += 1
+    hi = 0
+    while hi < n and c[n - 1 - hi] != 0.0:
+        hi += 1
+    if lo + hi >= n:
+        lo, hi = n, 0
+    return lo, hi
+
+
+class _Axis:
+    """Device copy of one CPML axis (b, c, 1/kappa on integer and half nodes)."""
+
+    def __init__(self, prof, n, dev):
+        self.keep = []
+        self.ax = N.Axis()
+        for tag, length in (('e', n), ('h', n - 1)):
+            b = np.asarray(prof['b' + tag], F32)
+            c = np.asarray(prof['c' + tag], F32)
+            ik = (F32(1.0) / np.asarray(prof['k' + tag], F32)).astype(F32)
+            assert len(b) == length, (tag, len(b), length)
+            tb, tc, ti = (torch.from_numpy(v.copy()).to(dev) for v in (b, c, ik))
+            self.keep += [tb, tc, ti]
+            lo, hi = strip_widths(c)
+            setattr(self.ax, tag, N.Profile(_ptr(tb), _ptr(tc), _ptr(ti), length, lo, hi))
+
+    def w(self, tag):
+        p = getattr(self.ax, tag)
+        return p.lo + p.hi
+
+
+class StepTable:
+    """Per-step scalars for steps [t0, t0+n): float32(w_src t), envelope, DFT phases.
+
+    wt follows vcsel.py:153-155 (float32 of the float64 product), the envelope is
+    evaluated in float64 (fdtd2d_core.py:784-787) and the DFT phases are
+    exp(-i w t) and exp(-i w (t - dt/2)) (flux.py:30-33)."""
+
+    def __init__(self, t0, n, dt, omega_src, omega_dft, envelope, device=None):
+        dev = _device(device)
+        steps = np.arange(t0, t0 + n, dtype=np.int64)
+        t = steps * dt
+        self.t0, self.n = int(t0), int(n)
+        wt = (omega_src * t).astype(F32)
+        env = np.asarray(envelope(t), dtype=np.float64).astype(F32)
+        pe = np.exp(-1j * omega_dft * t)
+        ph = np.exp(-1j * omega_dft * (t - 0.5 * dt))
+        pe2 = np.stack([pe.real, pe.imag], 1).astype(F32)
+        ph2 = np.stack([ph.real, ph.imag], 1).astype(F32)
+        self.wt, self.env, self.pe, self.ph = (torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+                                               for v in (wt, env, pe2, ph2))
+        self.s = N.StepTable(_ptr(self.wt), _ptr(self.env), _ptr(self.pe), _ptr(self.ph),
+                             self.t0, self.n)
+
+
+def cw_envelope(f0, ramp_periods=None):
+    """Vectorised CW ramp 1 - exp(-(t/(2 sigma_t))^2) (fdtd2d_core.py:784-787);
+    sigma_t = 4/(2 pi f0), or ramp_periods/(6 f0) to stretch the 6-sigma start-up."""
+    st = 4.0 / (2 * np.pi * f0) if ramp_periods is None else ramp_periods / (6.0 * f0)
+    return lambda t: 1 - np.exp(-((np.asarray(t) / (2 * st)) ** 2))
+
+
+def _kahan_value(buf):
+    """Compensated (sum, carry) float32 pairs -> complex128 value sum - carry."""
+    b = buf.double()
+    return torch.complex(b[..., 0] - b[..., 2], b[..., 1] - b[..., 3])
+
+
+# ============================================================================ 2D
+class Grid2D:
+    """One 2D CPML solve (TE: Ez/Hx/Hy, TM: Ex/Ey/Hz) resident on the GPU.
+
+    coef: TE {'ce_e','ce_h'} (nx,ny); TM {'ca_x' (nx-1,ny), 'ca_y' (nx,ny-1),
+    optional 'da_x','da_y'} - the arrays of fdtd2d_core._coeffs / _tm_coeffs /
+    _tm_loss.  cx, cy: CPML profiles {'ke','be','ce','kh','bh','ch'} along x and y.
+    src: dict(ix, amp, ph1, ph2) of the Huygens pair (TM: on the Ey grid)."""
+
+    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None):
+        self.lib = N.load()
+        dev = self.dev = _device(device)
+        self.pol = 'p' if str(pol).lower() in ('p', 'tm') else 's'
+        self.nx, self.ny, self.dx, self.dt = int(nx), int(ny), dx, dt
+        P = self.pitch = pitch_of(ny)
+        shp = (nx, P)
+        z = lambda *s: torch.zeros(s if s else shp, dtype=torch.float32, device=dev)
+        self.ch = F32(dt / (MU0 * dx))
+        self.axx, self.axy = _Axis(cx, nx, dev), _Axis(cy, ny, dev)
+        wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
+        self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
+                      for k in ('amp', 'ph1', 'ph2')}
+        s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
+                     _ptr(self.src_t['ph2']), len(src['amp']), 1, len(src['amp']))
+        pec4 = (ctypes.c_int * 4)(*[int(bool(v)) for v in pec])
+        if self.pol == 's':
+            self.ez, self.hx, self.hy = z(), z(), z()
+            self.ce_e = _pad_upload(coef['ce_e'], shp, dev)
+            self.ce_h = _pad_upload(coef['ce_h'], shp, dev)
+            self.psi = dict(hxy=z(nx, max(1, wyh)), hyx=z(max(1, wxh), P),
+                            ezx=z(max(1, wxe), P), ezy=z(nx, max(1, wye)))
+            self.s = N.TE2D(nx, ny, P, _ptr(self.ez), _ptr(self.hx), _ptr(self.hy),
+                            _ptr(self.ce_e), _ptr(self.ce_h), float(self.ch),
+                            self.axx.ax, self.axy.ax, _ptr(self.psi['hxy']), _ptr(self.psi['hyx']),
+                            _ptr(self.psi['ezx']), _ptr(self.psi['ezy']), pec4, s)
+        else:
+            self.ex, self.ey, self.hz = z(), z(), z()
+            self.ca_x = _pad_upload(coef['ca_x'], shp, dev)
+            self.ca_y = _pad_upload(coef['ca_y'], shp, dev)
+            da = coef.get('da_x') is not None
+            self.da_x = _pad_upload(coef['da_x'], shp, dev) if da else None
+            self.da_y = _pad_upload(coef['da_y'], shp, dev) if da else None
+            self.psi = dict(hzx=z(max(1, wxh), P), hzy=z(nx, max(1, wyh)),
+                            exy=z(nx, max(1, wye)), eyx=z(max(1, wxe), P))
+            self.s = N.TM2D(nx, ny, P, _ptr(self.ex), _ptr(self.ey), _ptr(self.hz),
+                            _ptr(self.ca_x), _ptr(self.ca_y), _ptr(self.da_x), _ptr(self.da_y),
+                            float(self.ch), self.axx.ax, self.axy.ax,
+                            _ptr(self.psi['hzx']), _ptr(self.psi['hzy']), _ptr(self.psi['exy']),
+                            _ptr(self.psi['eyx']), pec4, s)
+
+    # reference-shaped views of the resident fields
+    def view(self, name):
+        nx, ny = self.nx, self.ny
+        shapes = dict(ez=(nx, ny), hx=(nx, ny - 1), hy=(nx - 1, ny),
+                      ex=(nx - 1, ny), ey=(nx, ny - 1), hz=(nx - 1, ny - 1))
+        a, b = shapes[name]
+        return getattr(self, name)[:a, :b]
+
+    def step(self, table, n0, nsteps, epi=None, stream=None):
+        fn = self.lib.lens_te2d_step if self.pol == 's' else self.lib.lens_tm2d_step
+        e = epi.s if epi is not None else None
+        N.check(fn(ctypes.byref(self.s), ctypes.byref(table.s),
+                   ctypes.byref(e) if e is not None else None, int(n0), int(nsteps),
+                   _stream_ptr(stream)))
+
+
+class Epi2D:
+    """Epilogue buffers of a 2D solve (detector boxes, DFTs, Iavg, flux planes)."""
+
+    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=()):
+        dev, nx, P = grid.dev, grid.nx, grid.pitch
+        self.grid = grid
+        self.boxes = [tuple(int(v) for v in b) for b in boxes]
+        self.box_acc = torch.zeros(max(1, len(boxes)), dtype=torch.float64, device=dev)
+        d4 = lambda: torch.zeros((nx, P, 4), dtype=torch.float32, device=dev)
+        self.dft = d4() if dft is not None else None
+        self.dft_ex = d4() if (dft is not None and dft_ex) else None
+        self.prev = d4() if prev is not None else None
+        self.iavg = torch.zeros((nx, P), dtype=torch.float32, device=dev) if iavg_n0 is not None else None
+        self.planes = dict(planes)
+        self.plane_acc = torch.zeros((max(1, len(self.planes)), 4, P), dtype=torch.float64, device=dev)
+        s = N.Epi2D()
+        s.nbox = len(self.boxes)
+        for q, b in enumerate(self.boxes):
+            s.box[q] = (ctypes.c_int * 4)(*b)
+        s.box_acc = _ptr(self.box_acc)
+        s.dft_n0, s.dft_n1 = dft if dft is not None else (0, 0)
+        s.dft, s.dft_ex = _ptr(self.dft), _ptr(self.dft_ex)
+        s.prev_n0, s.prev_n1 = prev if prev is not None else (0, 0)
+        s.dft_prev = _ptr(self.prev)
+        s.iavg_n0 = int(iavg_n0) if iavg_n0 is not None else (1 << 30)
+        s.iavg = _ptr(self.iavg)
+        s.nplane = len(self.planes)
+        for q, il in enumerate(self.planes.values()):
+            s.plane[q] = int(il)
+        s.plane_acc = _ptr(self.plane_acc)
+        self.s = s
+
+    def phasor(self, which='dft'):
+        """Accumulated sum(F e^{-i w t}) on the nodes (nx, ny), complex128."""
+        return _kahan_value(getattr(self, which))[:, :self.grid.ny]
+
+    def flux(self, name, n_acc):
+        """Net +x Poynting flux through plane `name` (flux.py:45-57)."""
+        q = list(self.planes).index(name)
+        a = self.plane_acc[q]
+        ny = self.grid.ny if self.grid.pol == 's' else self.grid.ny - 1
+        aE = torch.complex(a[0, :ny], a[1, :ny])
+        aH = torch.complex(a[2, :ny], a[3, :ny])
+        sign = -1.0 if self.grid.pol == 's' else 1.0
+        return float(sign * 0.5 * torch.real(torch.sum(aE * torch.conj(aH)))) * (2.0 / n_acc) ** 2
+
+
+# ============================================================================ 3D
+class Grid3D:
+    """One 3D CPML solve resident on the GPU (fdtd3d_core.run_3d hot loop state).
+
+    ce: (ce_x, ce_y, ce_z) staggered update factors; da: staggered damping
+    (D_x, D_y, D_z) or None; cpml: three profile dicts (x, y, z);
+    src: dict(ix, amp (nj,nk), ph1, ph2) on the grid of component src_comp."""
+
+    def __init__(self, nx, ny, nz, dx, dt, ce, da, cpml, src, src_comp=1, pec=(1,) * 6,
+                 device=None):
+        self.lib = N.load()
+        dev = self.dev = _device(device)
+        self.nx, self.ny, self.nz, self.dx, self.dt = int(nx), int(ny), int(nz), dx, dt
+        P = self.pitch = pitch_of(nz)
+        shp = (nx, ny, P)
+        z = lambda *s: torch.zeros(s if s else shp, dtype=torch.float32, device=dev)
+        self.ch = F32(dt / (MU0 * dx))
+        self.ax = [_Axis(cpml[a], n, dev) for a, n in enumerate((nx, ny, nz))]
+        X, Y, Z = self.ax
+        for nm in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
+            setattr(self, nm, z())
+        self.ce = [_pad_upload(a, shp, dev) for a in ce]
+        self.da = None if da is None else [_pad_upload(a, shp, dev) for a in da]
+        m1 = lambda w: max(1, w)
+        self.psi = dict(
+            hx_z=z(nx, ny, m1(Z.w('h'))), hy_z=z(nx, ny, m1(Z.w('h'))),
+            ex_z=z(nx, ny, m1(Z.w('e'))), ey_z=z(nx, ny, m1(Z.w('e'))),
+            hx_y=z(nx, m1(Y.w('h')), P), hz_y=z(nx, m1(Y.w('h')), P),
+            ex_y=z(nx, m1(Y.w('e')), P), ez_y=z(nx, m1(Y.w('e')), P),
+            hy_x=z(m1(X.w('h')), ny, P), hz_x=z(m1(X.w('h')), ny, P),
+            ey_x=z(m1(X.w('e')), ny, P), ez_x=z(m1(X.w('e')), ny, P))
+        amp = np.ascontiguousarray(src['amp'], F32)
+        self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
+                      for k in ('amp', 'ph1', 'ph2')}
+        nj, nk = amp.shape
+        s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
+                     _ptr(self.src_t['ph2']), nj, nk, nk)
+        self.src_comp = int(src_comp)
+        ps = self.psi
+        dn = (lambda q: _ptr(None if self.da is None else self.da[q]))
+        self.s = N.Grid3D(nx, ny, nz, P, *(_ptr(getattr(self, f)) for f in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')),
+                          *(_ptr(c) for c in self.ce), dn(0), dn(1), dn(2), float(self.ch),
+                          X.ax, Y.ax, Z.ax,
+                          *(_ptr(ps[k]) for k in ('hx_z', 'hx_y', 'hy_x', 'hy_z', 'hz_y', 'hz_x',
+                                                  'ex_y', 'ex_z', 'ey_z', 'ey_x', 'ez_x', 'ez_y')),
+                          (ctypes.c_int * 6)(*[int(bool(v)) for v in pec]), s, self.src_comp)
+
+    def view(self, name):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        shapes = dict(ex=(nx - 1, ny, nz), ey=(nx, ny - 1, nz), ez=(nx, ny, nz - 1),
+                      hx=(nx, ny - 1, nz - 1), hy=(nx - 1, ny, nz - 1), hz=(nx - 1, ny - 1, nz))
+        a, b, c = shapes[name]
+        return getattr(self, name)[:a, :b, :c]
+
+    def step(self, table, n0, nsteps, epi=None, stream=None):
+        e = epi.s if epi is not None else None
+        N.check(self.lib.lens_fdtd3d_step(ctypes.byref(self.s), ctypes.byref(table.s),
+                                          ctypes.byref(e) if e is not None else None,
+                                          int(n0), int(nsteps), _stream_ptr(stream)))
+
+    def accum_e2(self, iavg, target=None, stream=None):
+        t = self.src_comp if target is None else target
+        N.check(self.lib.lens_fdtd3d_accum_e2(ctypes.byref(self.s), int(t), _ptr(iavg),
+                                              _stream_ptr(stream)))
+
+
+class Epi3D:
+    """Epilogue buffers of a 3D solve."""
+
+    def __init__(self, grid, boxes=(), dft=None, comps=(1,), planes=(), conv=None, iavg=False):
+        dev, nx, ny, P = grid.dev, grid.nx, grid.ny, grid.pitch
+        self.grid = grid
+        self.boxes = [tuple(int(v) for v in b) for b in boxes]
+        self.box_acc = torch.zeros(max(1, len(boxes)), dtype=torch.float64, device=dev)
+        self.dft = [None, None, None]
+        if dft is not None:
+            for c in comps:
+                self.dft[c] = torch.zeros((nx, ny, P, 4), dtype=torch.float32, device=dev)
+        self.planes = dict(planes)
+        self.plane_acc = torch.zeros((max(1, len(self.planes)), 2, 4, ny, P), dtype=torch.float64,
+                                     device=dev)
+        nj = grid.s.src.nj
+        self.conv_prev = self.conv_last = None
+        if conv is not None:
+            self.conv_prev = torch.zeros((nx, nj, 4), dtype=torch.float32, device=dev)
+            self.conv_last = torch.zeros((nx, nj, 4), dtype=torch.float32, device=dev)
+        self.iavg = torch.zeros((nx, ny, P), dtype=torch.float32, device=dev) if iavg else None
+        s = N.Epi3D()
+        s.nbox = len(self.boxes)
+        for q, b in enumerate(self.boxes):
+            s.box[q] = (ctypes.c_int * 6)(*b)
+        s.box_acc = _ptr(self.box_acc)
+        s.dft_n0, s.dft_n1 = dft if dft is not None else (0, 0)
+        for c in range(3):
+            s.dft[c] = _ptr(self.dft[c])
+        if conv is not None:
+            s.conv_k, (s.prev_n0, s.prev_n1) = int(conv[0]), conv[1]
+        s.conv_prev, s.conv_last = _ptr(self.conv_prev), _ptr(self.conv_last)
+        s.nplane = len(self.planes)
+        for q, il in enumerate(self.planes.values()):
+            s.plane[q] = int(il)
+        s.plane_acc = _ptr(self.plane_acc)
+        self.s = s
+
+    def phasor(self, comp=1):
+        g = self.grid
+        nx, ny, nz = g.nx, g.ny, g.nz
+        shape = {0: (nx - 1, ny, nz), 1: (nx, ny - 1, nz), 2: (nx, ny, nz - 1)}[comp]
+        return _kahan_value(self.dft[comp])[:shape[0], :shape[1], :shape[2]]
+
+    def flux(self, name, n_acc):
+        """Net +x Poynting flux (pairs_3d, flux.py:84-90 and :45-57)."""
+        g = self.grid
+        q = list(self.planes).index(name)
+        tot = 0.0
+        for pair, (sign, nj, nk) in enumerate(((1.0, g.ny - 1, g.nz), (-1.0, g.ny, g.nz - 1))):
+            a = self.plane_acc[q, pair]
+            aE = torch.complex(a[0, :nj, :nk], a[1, :nj, :nk])
+            aH = torch.complex(a[2, :nj, :nk], a[3, :nj, :nk])
+            tot += sign * 0.5 * float(torch.real(torch.sum(aE * torch.conj(aH))))
+        return tot * (2.0 / n_acc) ** 2

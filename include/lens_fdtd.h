@@ -129,24 +129,37 @@ int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D 
                    int n0, int nsteps, void *stream);
 
 /* ---------------------------------------------------------------- 3D grid */
+/* psi strip arrays (boundaries3d.py:286-302), in this order; w = lo+hi of the
+ * profile named, every array row-major:
+ *   z-strips  HX_Z, HY_Z (az.h)  EX_Z, EY_Z (az.e):  (nx, ny, w)
+ *   y-strips  HX_Y, HZ_Y (ay.h)  EX_Y, EZ_Y (ay.e):  (nx, w, pitch)
+ *   x-strips  HY_X, HZ_X (ax.h)  EY_X, EZ_X (ax.e):  (w, ny, pitch)            */
+enum {
+    LENS_PSI_HX_Z, LENS_PSI_HX_Y, LENS_PSI_HY_X, LENS_PSI_HY_Z, LENS_PSI_HZ_Y, LENS_PSI_HZ_X,
+    LENS_PSI_EX_Y, LENS_PSI_EX_Z, LENS_PSI_EY_Z, LENS_PSI_EY_X, LENS_PSI_EZ_X, LENS_PSI_EZ_Y,
+    LENS_NPSI
+};
+
 typedef struct {
     int nx, ny, nz, pitch;       /* node counts; z pitch of every array        */
-    float *ex, *ey, *ez;         /* Ex (nx-1,ny,nz) Ey (nx,ny-1,nz) Ez (nx,ny,nz-1) */
-    float *hx, *hy, *hz;         /* Hx (nx,ny-1,nz-1) Hy (nx-1,ny,nz-1) Hz (nx-1,ny-1,nz) */
+    /* Field buffers b = 0, 1: f[b] = {Ex, Ey, Ez, Hx, Hy, Hz} with
+       Ex (nx-1,ny,nz) Ey (nx,ny-1,nz) Ez (nx,ny,nz-1)
+       Hx (nx,ny-1,nz-1) Hy (nx-1,ny,nz-1) Hz (nx-1,ny-1,nz).
+       With buffer 1 present (all six pointers and all psi[1]) a step reads
+       buffer `cur`, writes buffer 1-cur in one fused pass and flips `cur`;
+       with buffer 1 NULL the step updates buffer `cur` in place (two passes). */
+    float *f[2][6];
+    float *psi[2][LENS_NPSI];
+    int cur;
     const float *ce_x, *ce_y, *ce_z;  /* staggered update factors (fdtd3d_core.py:305-378) */
     const float *da_x, *da_y, *da_z;  /* staggered loss damping or NULL (fdtd3d_core.py:606-613) */
     float ch;
     LensAxis ax, ay, az;
-    /* psi strips (boundaries3d.py:286-302); w = lo+hi of the profile named:
-       z-strips  hx_z, hy_z (az.h)  ex_z, ey_z (az.e):  (nx, ny, w)      floats
-       y-strips  hx_y, hz_y (ay.h)  ex_y, ez_y (ay.e):  (nx, w, pitch)   floats
-       x-strips  hy_x, hz_x (ax.h)  ey_x, ez_x (ax.e):  (w, ny, pitch)   floats
-       (row-major; rows belonging to no valid cell of the component are unused) */
-    float *psi_hx_z, *psi_hx_y, *psi_hy_x, *psi_hy_z, *psi_hz_y, *psi_hz_x;
-    float *psi_ex_y, *psi_ex_z, *psi_ey_z, *psi_ey_x, *psi_ez_x, *psi_ez_y;
     int pec[6];                  /* PEC on x-lo, x-hi, y-lo, y-hi, z-lo, z-hi  */
     LensSource src;              /* plane (nj, nk) of the driven component     */
     int src_comp;                /* 0 Ex, 1 Ey, 2 Ez                           */
+    int *flag;                   /* optional device int, set nonzero when a
+                                    pipeline wait gave up (results invalid)    */
 } LensGrid3D;
 
 typedef struct {
@@ -163,7 +176,8 @@ typedef struct {
     double *plane_acc;           /* per plane: 2 pairs (Ey/Hz, Ez/Hy) x 4 x (ny*pitch) doubles */
 } LensEpi3D;
 
-int lens_fdtd3d_step(const LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
+/* Advance nsteps; updates g->cur when the fused (double-buffered) path runs. */
+int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
                      int n0, int nsteps, void *stream);
 
 /* Iavg += |E|^2 of all three components mapped onto the grid of component

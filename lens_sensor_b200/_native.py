@@ -60,18 +60,18 @@ class Epi2D(ctypes.Structure):
                 ('nplane', c_int), ('plane', c_int * MAX_PLANE), ('plane_acc', c_void_p)]
 
 
+NPSI = 12
+PSI_NAMES = ('hx_z', 'hx_y', 'hy_x', 'hy_z', 'hz_y', 'hz_x',
+             'ex_y', 'ex_z', 'ey_z', 'ey_x', 'ez_x', 'ez_y')   # LENS_PSI_* order
+
+
 class Grid3D(ctypes.Structure):
     _fields_ = [('nx', c_int), ('ny', c_int), ('nz', c_int), ('pitch', c_int),
-                ('ex', c_void_p), ('ey', c_void_p), ('ez', c_void_p),
-                ('hx', c_void_p), ('hy', c_void_p), ('hz', c_void_p),
+                ('f', (c_void_p * 6) * 2), ('psi', (c_void_p * NPSI) * 2), ('cur', c_int),
                 ('ce_x', c_void_p), ('ce_y', c_void_p), ('ce_z', c_void_p),
                 ('da_x', c_void_p), ('da_y', c_void_p), ('da_z', c_void_p),
                 ('ch', c_float), ('ax', Axis), ('ay', Axis), ('az', Axis),
-                ('psi_hx_z', c_void_p), ('psi_hx_y', c_void_p), ('psi_hy_x', c_void_p),
-                ('psi_hy_z', c_void_p), ('psi_hz_y', c_void_p), ('psi_hz_x', c_void_p),
-                ('psi_ex_y', c_void_p), ('psi_ex_z', c_void_p), ('psi_ey_z', c_void_p),
-                ('psi_ey_x', c_void_p), ('psi_ez_x', c_void_p), ('psi_ez_y', c_void_p),
-                ('pec', c_int * 6), ('src', Source), ('src_comp', c_int)]
+                ('pec', c_int * 6), ('src', Source), ('src_comp', c_int), ('flag', c_void_p)]
 
 
 class Epi3D(ctypes.Structure):

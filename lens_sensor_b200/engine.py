@@ -239,10 +239,14 @@ class Grid3D:
 
     ce: (ce_x, ce_y, ce_z) staggered update factors; da: staggered damping
     (D_x, D_y, D_z) or None; cpml: three profile dicts (x, y, z);
-    src: dict(ix, amp (nj,nk), ph1, ph2) on the grid of component src_comp."""
+    src: dict(ix, amp (nj,nk), ph1, ph2) on the grid of component src_comp.
+    fused=True keeps two field/psi buffers and runs the single-pass TMA kernel;
+    fused=False updates one buffer in place with two streaming passes."""
+
+    FIELDS = ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')
 
     def __init__(self, nx, ny, nz, dx, dt, ce, da, cpml, src, src_comp=1, pec=(1,) * 6,
-                 device=None):
+                 device=None, fused=True):
         self.lib = N.load()
         dev = self.dev = _device(device)
         self.nx, self.ny, self.nz, self.dx, self.dt = int(nx), int(ny), int(nz), dx, dt
@@ -251,19 +255,20 @@ class Grid3D:
         z = lambda *s: torch.zeros(s if s else shp, dtype=torch.float32, device=dev)
         self.ch = F32(dt / (MU0 * dx))
         self.ax = [_Axis(cpml[a], n, dev) for a, n in enumerate((nx, ny, nz))]
-        X, Y, Z = self.ax
-        for nm in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
-            setattr(self, nm, z())
+        X, Y, Zp = self.ax
+        nbuf = 2 if fused else 1
+        self.bufs = [{f: z() for f in self.FIELDS} for _ in range(nbuf)]
+        m1 = lambda w: max(1, w)
+        psi_shape = dict(
+            hx_z=(nx, ny, m1(Zp.w('h'))), hy_z=(nx, ny, m1(Zp.w('h'))),
+            ex_z=(nx, ny, m1(Zp.w('e'))), ey_z=(nx, ny, m1(Zp.w('e'))),
+            hx_y=(nx, m1(Y.w('h')), P), hz_y=(nx, m1(Y.w('h')), P),
+            ex_y=(nx, m1(Y.w('e')), P), ez_y=(nx, m1(Y.w('e')), P),
+            hy_x=(m1(X.w('h')), ny, P), hz_x=(m1(X.w('h')), ny, P),
+            ey_x=(m1(X.w('e')), ny, P), ez_x=(m1(X.w('e')), ny, P))
+        self.psi = [{q: z(*psi_shape[q]) for q in N.PSI_NAMES} for _ in range(nbuf)]
         self.ce = [_pad_upload(a, shp, dev) for a in ce]
         self.da = None if da is None else [_pad_upload(a, shp, dev) for a in da]
-        m1 = lambda w: max(1, w)
-        self.psi = dict(
-            hx_z=z(nx, ny, m1(Z.w('h'))), hy_z=z(nx, ny, m1(Z.w('h'))),
-            ex_z=z(nx, ny, m1(Z.w('e'))), ey_z=z(nx, ny, m1(Z.w('e'))),
-            hx_y=z(nx, m1(Y.w('h')), P), hz_y=z(nx, m1(Y.w('h')), P),
-            ex_y=z(nx, m1(Y.w('e')), P), ez_y=z(nx, m1(Y.w('e')), P),
-            hy_x=z(m1(X.w('h')), ny, P), hz_x=z(m1(X.w('h')), ny, P),
-            ey_x=z(m1(X.w('e')), ny, P), ez_x=z(m1(X.w('e')), ny, P))
         amp = np.ascontiguousarray(src['amp'], F32)
         self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
                       for k in ('amp', 'ph1', 'ph2')}
@@ -271,14 +276,30 @@ class Grid3D:
         s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
                      _ptr(self.src_t['ph2']), nj, nk, nk)
         self.src_comp = int(src_comp)
-        ps = self.psi
-        dn = (lambda q: _ptr(None if self.da is None else self.da[q]))
-        self.s = N.Grid3D(nx, ny, nz, P, *(_ptr(getattr(self, f)) for f in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')),
-                          *(_ptr(c) for c in self.ce), dn(0), dn(1), dn(2), float(self.ch),
-                          X.ax, Y.ax, Z.ax,
-                          *(_ptr(ps[k]) for k in ('hx_z', 'hx_y', 'hy_x', 'hy_z', 'hz_y', 'hz_x',
-                                                  'ex_y', 'ex_z', 'ey_z', 'ey_x', 'ez_x', 'ez_y')),
-                          (ctypes.c_int * 6)(*[int(bool(v)) for v in pec]), s, self.src_comp)
+        self.flag = torch.zeros(1, dtype=torch.int32, device=dev)
+        g = N.Grid3D()
+        g.nx, g.ny, g.nz, g.pitch = nx, ny, nz, P
+        for b in range(nbuf):
+            for c, f in enumerate(self.FIELDS):
+                g.f[b][c] = self.bufs[b][f].data_ptr()
+            for q, name in enumerate(N.PSI_NAMES):
+                g.psi[b][q] = self.psi[b][name].data_ptr()
+        g.cur = 0
+        g.ce_x, g.ce_y, g.ce_z = (c.data_ptr() for c in self.ce)
+        if self.da is not None:
+            g.da_x, g.da_y, g.da_z = (d.data_ptr() for d in self.da)
+        g.ch = float(self.ch)
+        g.ax, g.ay, g.az = X.ax, Y.ax, Zp.ax
+        g.pec = (ctypes.c_int * 6)(*[int(bool(v)) for v in pec])
+        g.src = s
+        g.src_comp = self.src_comp
+        g.flag = self.flag.data_ptr()
+        self.s = g
+
+    def __getattr__(self, name):
+        if name in Grid3D.FIELDS:
+            return self.__dict__['bufs'][self.__dict__['s'].cur][name]
+        raise AttributeError(name)
 
     def view(self, name):
         nx, ny, nz = self.nx, self.ny, self.nz
@@ -292,6 +313,11 @@ class Grid3D:
         N.check(self.lib.lens_fdtd3d_step(ctypes.byref(self.s), ctypes.byref(table.s),
                                           ctypes.byref(e) if e is not None else None,
                                           int(n0), int(nsteps), _stream_ptr(stream)))
+
+    def check_flag(self):
+        """Raise if a pipeline wait in the fused kernel gave up (results invalid)."""
+        if int(self.flag.item()) != 0:
+            raise N.LensError('fused 3D kernel: a pipeline wait timed out')
 
     def accum_e2(self, iavg, target=None, stream=None):
         t = self.src_comp if target is None else target

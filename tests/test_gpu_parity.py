@@ -92,7 +92,7 @@ def test_2d_phasor_against_fp64_oracle():
     assert err < 1e-4, err
 
 
-def run_engine_3d(c, setup=None, iavg_every=3, n_dft=30):
+def run_engine_3d(c, setup=None, iavg_every=3, n_dft=30, fused=True):
     import torch
     from lens_sensor_b200 import engine as E
     s = setup or H.setup_3d(c)
@@ -100,7 +100,7 @@ def run_engine_3d(c, setup=None, iavg_every=3, n_dft=30):
     comp = 1 if c['pol'] == 'p' else 2
     src = dict(ix=s['src'].ix, amp=s['src'].amp, ph1=s['src'].ph1, ph2=s['src'].ph2)
     g = E.Grid3D(Nx, Ny, Nz, s['dx'], s['dt'], (s['ce_x'], s['ce_y'], s['ce_z']), s['da'],
-                 s['cpml'], src, src_comp=comp)
+                 s['cpml'], src, src_comp=comp, fused=fused)
     steps = c['steps']
     tab = E.StepTable(0, steps, s['dt'], s['src'].omega, 2 * np.pi * s['f0'], E.cw_envelope(s['f0']))
     n_sp = s['n_sp']
@@ -113,6 +113,7 @@ def run_engine_3d(c, setup=None, iavg_every=3, n_dft=30):
         if n >= steps // 2 and (n - steps // 2) % iavg_every == 0:
             g.accum_e2(ep.iavg)
     torch.cuda.synchronize()
+    g.check_flag()
     out = {nm: _np(g.view(nm.lower())) for nm in ('Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz')}
     out['acc'] = _np(ep.phasor(comp))
     sh = out['Ey' if comp == 1 else 'Ez'].shape
@@ -136,10 +137,11 @@ def check_fields_3d(r, g):
             assert e < TOL_FIELD, (n, e)
 
 
-def test_3d_against_reference_fixture():
+@pytest.mark.parametrize('fused', [True, False], ids=['fused', 'two_pass'])
+def test_3d_against_reference_fixture(fused):
     c = CASES['d3']
     g = dict(np.load(os.path.join(G, 'g3d_tm.npz')))
-    r = run_engine_3d(c)
+    r = run_engine_3d(c, fused=fused)
     check_fields_3d(r, g)
     for key in ('acc', 'Iavg'):
         assert rel_l2(r[key], g[key]) < TOL_FIELD, (key, rel_l2(r[key], g[key]))
@@ -155,13 +157,25 @@ def test_3d_phasor_against_fp64_oracle():
     assert err < 1e-4, err
 
 
-def test_3d_te_polarisation_and_lossless():
+@pytest.mark.parametrize('fused', [True, False], ids=['fused', 'two_pass'])
+def test_3d_te_polarisation_and_lossless(fused):
     """s-pol drives Ez; lossless stack (no damping arrays)."""
     c = dict(CASES['d3'], pol='s', stack=[[0.6, 1.333], [0.3, 1.34]], steps=60)
     s = H.setup_3d(c)
     assert s['da'] is None
-    r = run_engine_3d(c, setup=s, n_dft=20)
+    r = run_engine_3d(c, setup=s, n_dft=20, fused=fused)
     o = H.run_3d(c, setup=s, n_dft=20)
     check_fields_3d(r, o)
     for key in ('acc', 'Iavg'):
         assert rel_l2(r[key], o[key]) < TOL_FIELD, (key, rel_l2(r[key], o[key]))
+
+
+def test_3d_uneven_tiles_and_chunks():
+    """Grid sizes that are not multiples of the 8 x 32 tile, several x-chunks,
+    odd step count (fused path ends on the second buffer)."""
+    c = dict(CASES['d3'], Nx=97, Ny=37, Nz=45, steps=41, bead=dict(x_um=2.6, d_um=0.4, n=1.59, z_um=-0.2))
+    s = H.setup_3d(c)
+    r = run_engine_3d(c, setup=s, n_dft=15)
+    o = H.run_3d(c, setup=s, n_dft=15, box=(slice(36, 44), slice(20, 34), slice(8, 37)))
+    check_fields_3d(r, o)
+    assert rel_l2(r['acc'], o['acc']) < TOL_FIELD

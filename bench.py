@@ -1,0 +1,297 @@
+#!/usr/bin/env python
+"""Benchmark: Yee cell-updates/s of the 3D CPML time-stepping hot path.
+
+Workload (config 1): 3D TM planar waveguide 480 x 192 x 256 cells @ 30 nm,
+float32 fields, 10-cell CPML, absorbing aqueous (1.333+0.001i), two seeded
+polystyrene beads, 4000-step CW schedule with Ex/Ey/Ez phasors.  One "step" is
+one leapfrog time step over the whole grid.  The K timed steps sample the
+schedule in its own proportions: steps outside the 8-period DFT window and
+steps inside it (detector boxes every step, |E|^2 averaging at its cadence).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun): the path
+has no exchange step, so there is no collective in the data path; the timing is
+the max over ranks.  --impl reference times the reference algorithm's CPU
+implementation (the NumPy oracle restatement of the reference path; the
+reference package itself is pure NumPy/CuPy Python and is not installed on the
+GPU machine).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = 'yee_cell_updates_per_s'
+UNIT = 'cell-updates/s'
+WORKLOAD = ('config1: 3D TM planar waveguide 480x192x256 @ 30 nm, fp32, 10-cell CPML, '
+            'lossy aqueous 1.333+0.001i, 2 seeded PS beads, 4000-step CW schedule, Ex/Ey/Ez phasors')
+
+
+def dist_env():
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    return ws, int(os.environ.get('RANK', '0')), int(os.environ.get('LOCAL_RANK', '0'))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class Clocks:
+    """nvidia-smi sampler of SM clock and throttle reasons during a region."""
+    Q = ('timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, dev_uuid=None):
+        cmd = ['nvidia-smi', '--query-gpu=' + self.Q, '--format=csv,noheader,nounits', '-lms', '100']
+        if dev_uuid:
+            cmd.insert(1, '--id=' + dev_uuid)
+        try:
+            self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=10)
+        except Exception:
+            self.p.kill()
+            out = ''
+        rows = [[c.strip() for c in ln.split(',')] for ln in out.splitlines() if ln.count(',') >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace('.', '').isdigit()]
+        load = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return dict(sm_mhz=statistics.median(load) if load else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(rows))
+
+
+def split_steps(K, steps_total, n_acc):
+    """K timed steps split in the schedule's proportions (outside / inside the DFT window)."""
+    kb = int(round(K * n_acc / steps_total))
+    return K - kb, kb
+
+
+def cpu_baseline(spec, steps=8):
+    """The NumPy oracle (restatement of the reference path) on a bounded sample:
+    `steps` consecutive full-grid steps with the detector sums, one host thread."""
+    from oracle import harness as H
+    from oracle import fdtd_oracle as O
+    c = oracle_case(spec)
+    s = H.setup_3d(c)
+    g = O.Grid3D(spec.nx, spec.ny, spec.nz, s['dx'], s['dt'], s['cpml'], (s['ce_x'], s['ce_y'], s['ce_z']),
+                 s['da'], s['src'], 'Ey' if spec.pol == 'p' else 'Ez')
+    nsp = s['n_sp']
+    box = (slice(64, 130), slice(100, 167), slice(nsp, spec.nz - nsp))
+    g.step(0, 0.0)
+    t0 = time.perf_counter()
+    for n in range(1, steps + 1):
+        g.step(n, 0.5)
+        g.box_e2(*box)
+    dt = time.perf_counter() - t0
+    cells = spec.nx * spec.ny * spec.nz
+    return cells * steps / dt, dict(sample=f'{steps} consecutive full-grid steps of the config-1 3D CPML '
+                                           f'step + detector box sums on the NumPy oracle (float32), '
+                                           f'{dt:.1f} s', cores=1)
+
+
+def oracle_case(spec):
+    st = spec.stack
+    return dict(pol=spec.pol, Nx=spec.nx, Ny=spec.ny, Nz=spec.nz, dx_nm=spec.dx_nm, t_wg_um=st.t_wg_um,
+                tear_um=spec.tear_um, stack=[[t, [complex(n).real, complex(n).imag]] for t, n in st.layers],
+                n_sub=st.n_sub, wg_n=st.wg_n, npml=spec.npml, lam_nm=spec.lam_nm, waist_um=spec.waist_um,
+                beads=[dict(x_um=b.x_um, d_um=b.d_um, n=b.n, y_um=b.y_um, z_um=b.z_um) for b in spec.beads])
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from lens_sensor_b200.workloads import config1
+    spec, steps_total = config1()
+    # each step: one full-grid oracle step; bounded so the arm ends within minutes
+    k = max(1, min(args.steps, 12))
+    value, info = cpu_baseline(spec, steps=k)
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=k, warmup=1,
+                ms_per_step=spec.nx * spec.ny * spec.nz / value * 1e3, higher_is_better=True,
+                scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
+                config=dict(workload=WORKLOAD, cells=spec.nx * spec.ny * spec.nz, steps_total=steps_total),
+                impl='reference', cpu_baseline=dict(value=value, unit=UNIT, cores=info['cores'], kind='port',
+                                                   sample=info['sample']),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(spec, steps_total, cells, ws, pg):
+    """The whole solve through the public API from host inputs: host setup,
+    upload, the 4000-step schedule, read-back of the three phasors."""
+    import torch
+    from lens_sensor_b200.solver3d import Solve3D
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    s2.run()
+    ph = [s2.phasor(c).cpu() for c in (0, 1, 2)]
+    res = s2.results()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([t_e2e], device='cuda')
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    d2h = sum(p.numel() * 16 for p in ph) + 64
+    out = dict(value=cells * steps_total * ws / t_e2e, unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
+               d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
+               transmission=res['transmission'], cw_rel_change=res['cw_rel_change'])
+    del s2
+    torch.cuda.empty_cache()
+    return out
+
+
+def ours_arm(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device('cuda', local))
+        pg = dist
+    from lens_sensor_b200.solver3d import Solve3D
+    from lens_sensor_b200.workloads import config1
+    spec, steps_total = config1()
+    cells = spec.nx * spec.ny * spec.nz
+    solve = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    W = max(3, args.warmup)
+    ka, kb = split_steps(args.steps, steps_total, solve.n_acc)
+    ka = min(ka, solve.dft[0] - W)
+    kb = min(kb, solve.n_acc)
+    K = ka + kb
+    uuid = None
+    try:
+        uuid = 'GPU-' + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = Clocks(uuid)
+    time.sleep(0.5)
+    solve.run(W)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    l0 = solve.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    solve.n = W
+    solve.run(W + ka)
+    solve.n = steps_total - kb
+    solve.run(steps_total)
+    ev1.record()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ck = clocks.stop()
+    launches = solve.launches - l0
+    ms = ev0.elapsed_time(ev1)
+    if pg:
+        t = torch.tensor([ms], device='cuda')
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * K * ws / (ms * 1e-3)
+    # algorithmic bytes: 72 B per cell update (6 fields R+W, 3 ce + 3 D read), +32 B per
+    # compensated DFT component in the DFT window, +20 B per |E|^2 accumulation pass
+    n_iavg = len(solve.iavg_steps(W, W + ka)) + len(solve.iavg_steps(steps_total - kb, steps_total))
+    alg = cells * (72 * K + 32 * len(solve.comps) * kb + 20 * n_iavg)
+    peak, peak_src = peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, 'profiles', 'fused3d_config1_traffic.json')) as f:
+            traffic = json.load(f).get('bytes_per_step')
+    except Exception:
+        pass
+    # end to end through the public API: host setup, H2D, the whole 4000-step schedule, D2H of phasors
+    del solve
+    torch.cuda.empty_cache()
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(spec, steps_total, cells, ws, pg)
+    cpu = None
+    s2 = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    s2.run()
+    ph = [s2.phasor(c).cpu() for c in (0, 1, 2)]
+    res = s2.results()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([t_e2e], device='cuda')
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    d2h = sum(p.numel() * 16 for p in ph) + 64
+    e2e = dict(value=cells * steps_total * ws / t_e2e, unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
+               d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
+               transmission=res['transmission'])
+    del s2
+    torch.cuda.empty_cache()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, info = cpu_baseline(spec)
+        cpu = dict(value=v, unit=UNIT, cores=info['cores'], kind='port', sample=info['sample'])
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=K, warmup=W,
+                    ms_per_step=ms / K, higher_is_better=True, scaling='weak', vs_baseline=None,
+                    dtype='f32', data='synthetic',
+                    config=dict(workload=WORKLOAD, cells=cells, steps_total=steps_total,
+                                timed_steps_outside_dft=ka, timed_steps_in_dft=kb,
+                                l2='inputs larger than L2: ~1.7 GB of fields and coefficients stream per step',
+                                parallelism=f'replicas{ws}' if ws > 1 else 'single'),
+                    roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s',
+                                  frac=achieved / peak, traffic=traffic, peak_source=peak_src,
+                                  alg_bytes_per_cell_update=alg / (cells * K)),
+                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches)
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=1000)
+    ap.add_argument('--warmup', type=int, default=20)
+    ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        reference_arm(args)
+    else:
+        ours_arm(args)
+
+
+if __name__ == '__main__':
+    main()

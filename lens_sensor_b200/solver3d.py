@@ -1,0 +1,133 @@
+"""One 3D solve on the GPU: setup, the run_3d time-stepping schedule and its
+results.  This is the engine behind fdtd3d_core.run_3d's full-domain CPML path
+(planar_3d/fdtd3d_core.py:793-1308):
+
+  * detector boxes of |E|^2 every step (:1139-1142), the input box kept
+    downstream of the source and entry facet (flux.py:64-74),
+  * time-averaged |E|^2 every steps_per_T//8 steps in the second half (:1144-1148),
+  * steady-state DFT over the last 8 periods on the selected components and
+    the plane-flux DFT (:1150-1158),
+  * the convergence DFT of the driven component on the z mid-plane for the
+    window before (:1159-1175).
+"""
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import engine as E
+from .geometry import Spec3D, build_3d
+
+
+def guard_in_plane(i_in, src_ix, n_max, margin=5):
+    """Input detector plane at least `margin` cells downstream of the source
+    (common/flux.py:64-74)."""
+    lo = int(src_ix) + int(margin)
+    return int(i_in) if i_in >= lo else min(lo, int(n_max) - 2)
+
+
+class Solve3D:
+    """Resident 3D solve.  comps: components whose phasor is accumulated
+    (0 Ex, 1 Ey, 2 Ez; default the driven one)."""
+
+    def __init__(self, spec: Spec3D, steps_total, comps=None, fused=True, device=None, geo=None):
+        self.spec = sp = spec
+        self.steps_total = int(steps_total)
+        t0 = time.perf_counter()
+        self.geo = geo if geo is not None else build_3d(sp)
+        self.t_setup_host = time.perf_counter() - t0
+        g = self.geo
+        Nx, Ny, Nz = sp.nx, sp.ny, sp.nz
+        dx_um = sp.dx_nm / 1000.0
+        self.grid = E.Grid3D(Nx, Ny, Nz, sp.dx, sp.dt, g['ce'], g['da'], g['cpml'], g['src'],
+                             src_comp=sp.src_comp, fused=fused, device=device)
+        self.h2d_bytes = sum(a.nbytes for a in g['ce']) + (0 if g['da'] is None else sum(a.nbytes for a in g['da'])) \
+            + sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
+        f0 = sp.f0
+        self.omega = 2 * np.pi * f0
+        self.steps_per_T = max(4, int(round((1.0 / f0) / sp.dt)))
+        n = self.steps_total
+        self.n_acc = min(n, 8 * self.steps_per_T)
+        self.dft = (n - self.n_acc, n)
+        self.prev = (max(0, n - 2 * self.n_acc), n - self.n_acc)
+        self.n_avg0 = n // 2
+        self.m_I = max(1, self.steps_per_T // 8)
+        # detector boxes (fdtd3d_core.py:1038-1062)
+        y0_um = -sp.tear_um
+        j_wg0 = int(round((0.0 - y0_um) / dx_um))
+        j_wg1 = int(round((sp.stack.t_wg_um - y0_um) / dx_um))
+        hw = max(2, int(round(1.0 / dx_um)))
+        lx = Nx * dx_um
+
+        def xr(xu):
+            c = int(round(xu / dx_um))
+            return max(0, c - hw), min(Nx, c + hw)
+        iin0, iin1 = xr(0.2 * lx)
+        iout0, iout1 = xr(0.8 * lx)
+        ci = (iin0 + iin1) // 2
+        sh = guard_in_plane(ci, max(sp.src_ix, int(round(g['x_facet_um'] / dx_um))), Nx) - ci
+        iin0, iin1 = iin0 + sh, min(Nx, iin1 + sh)
+        nsp = sp.n_sp
+        self.boxes = [(iin0, iin1, j_wg0, j_wg1, nsp, Nz - nsp), (iout0, iout1, j_wg0, j_wg1, nsp, Nz - nsp)]
+        self.planes = {'in': max(1, (iin0 + iin1) // 2), 'out': max(1, (iout0 + iout1) // 2),
+                       'src_up': sp.src_ix - 1, 'src_dn': sp.src_ix + 3}
+        self.comps = tuple(comps) if comps is not None else (sp.src_comp,)
+        src_shape = (Ny - 1, Nz) if sp.src_comp == 1 else (Ny, Nz - 1)
+        self.kc = src_shape[1] // 2
+        self.table = E.StepTable(0, n, sp.dt, g['src']['omega'], self.omega,
+                                 E.cw_envelope(f0, sp.ramp_periods), device=device)
+        self.epi = E.Epi3D(self.grid, boxes=self.boxes, dft=self.dft, comps=self.comps,
+                           planes=self.planes, conv=(self.kc, self.prev), iavg=True)
+        self.n = 0
+        self.launches = 0
+
+    def iavg_steps(self, n0, n1):
+        """Steps in [n0, n1) after which |E|^2 is accumulated."""
+        a = max(n0, self.n_avg0)
+        a += (-(a - self.n_avg0)) % self.m_I
+        return list(range(a, n1, self.m_I))
+
+    def run(self, n1=None, stream=None):
+        """Advance from the current step to n1 (default: the end of the schedule)."""
+        n1 = self.steps_total if n1 is None else min(int(n1), self.steps_total)
+        n = self.n
+        per_step = 2                      # two launches per step (strip + lean blocks, or H + E)
+        for m in self.iavg_steps(n, n1) + [None]:
+            stop = n1 if m is None else m + 1
+            if stop > n:
+                self.grid.step(self.table, n, stop - n, self.epi, stream)
+                self.launches += per_step * (stop - n)
+                n = stop
+            if m is not None:
+                self.grid.accum_e2(self.epi.iavg, stream=stream)
+                self.launches += 1
+        self.n = n
+        return self
+
+    # ---------------------------------------------------------------- results
+    def phasor(self, comp=None):
+        """Complex CW amplitude (2/N) sum F e^{-i w t} (fdtd3d_core.py:1271)."""
+        comp = self.spec.src_comp if comp is None else comp
+        return (2.0 / self.n_acc) * self.epi.phasor(comp)
+
+    def results(self):
+        sp, ep = self.spec, self.epi
+        torch.cuda.synchronize()
+        self.grid.check_flag()
+        dx = sp.dx
+        box = ep.box_acc.double().cpu().numpy()
+        P_in, P_out = float(box[0]) * dx ** 3, float(box[1]) * dx ** 3
+        S_in, S_out = ep.flux('in', self.n_acc), ep.flux('out', self.n_acc)
+        S_up, S_dn = ep.flux('src_up', self.n_acc), ep.flux('src_dn', self.n_acc)
+        a = ep.conv_last.double()
+        b = ep.conv_prev.double()
+        na, nb = self.n_acc, self.prev[1] - self.prev[0]
+        ca = torch.complex(a[..., 0] - a[..., 2], a[..., 1] - a[..., 3]) / max(na, 1)
+        cb = torch.complex(b[..., 0] - b[..., 2], b[..., 1] - b[..., 3]) / max(nb, 1)
+        rel = float(torch.linalg.norm(ca - cb) / max(float(torch.linalg.norm(ca)), 1e-30)) if nb > 0 else float('nan')
+        n_I = len(self.iavg_steps(0, self.steps_total))
+        return dict(P_in=P_in, P_out=P_out, transmission=(S_out / S_in if S_in else P_out / max(P_in, 1e-30)),
+                    transmission_intensity=P_out / max(P_in, 1e-30), S_in=S_in, S_out=S_out,
+                    p_in_si=S_in * dx * dx, p_emit=(S_dn - S_up) * dx * dx, cw_rel_change=rel,
+                    n_iavg=n_I, steps_total=self.steps_total)

@@ -240,23 +240,6 @@ def ours_arm(args):
     if not args.no_e2e:
         e2e = run_e2e(spec, steps_total, cells, ws, pg)
     cpu = None
-    s2 = Solve3D(spec, steps_total, comps=(0, 1, 2))
-    s2.run()
-    ph = [s2.phasor(c).cpu() for c in (0, 1, 2)]
-    res = s2.results()
-    torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([t_e2e], device='cuda')
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    d2h = sum(p.numel() * 16 for p in ph) + 64
-    e2e = dict(value=cells * steps_total * ws / t_e2e, unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
-               d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
-               transmission=res['transmission'])
-    del s2
-    torch.cuda.empty_cache()
-    cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, info = cpu_baseline(spec)
         cpu = dict(value=v, unit=UNIT, cores=info['cores'], kind='port', sample=info['sample'])

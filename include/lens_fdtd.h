@@ -23,9 +23,10 @@
  *    floats along z (pitch >= nz, multiple of 32).  A staggered component
  *    occupies the leading part of its rows (e.g. 2D Hx = (nx, ny-1)); padding is
  *    never read for a valid update and stays zero.
- *  - CPML psi lives only in the strips where the profile's c != 0 (leading `lo`
- *    and trailing `hi` entries of the profile); the strip arrays are documented
- *    per field below.  Outside the strips psi is identically zero.
+ *  - CPML psi is updated only in the strips where the profile's c != 0 (leading
+ *    `lo` and trailing `hi` entries of the profile); the 2D strip arrays and the
+ *    3D psi volumes are documented with each grid.  Outside the strips psi is
+ *    identically zero.
  */
 #ifndef LENS_FDTD_H
 #define LENS_FDTD_H
@@ -129,11 +130,10 @@ int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D 
                    int n0, int nsteps, void *stream);
 
 /* ---------------------------------------------------------------- 3D grid */
-/* psi strip arrays (boundaries3d.py:286-302), in this order; w = lo+hi of the
- * profile named, every array row-major:
- *   z-strips  HX_Z, HY_Z (az.h)  EX_Z, EY_Z (az.e):  (nx, ny, w)
- *   y-strips  HX_Y, HZ_Y (ay.h)  EX_Y, EZ_Y (ay.e):  (nx, w, pitch)
- *   x-strips  HY_X, HZ_X (ax.h)  EY_X, EZ_X (ax.e):  (w, ny, pitch)            */
+/* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
+ * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same
+ * TMA tiles as the fields; only cells inside the strip of the named profile are
+ * ever read or written (elsewhere psi is identically zero).                    */
 enum {
     LENS_PSI_HX_Z, LENS_PSI_HX_Y, LENS_PSI_HY_X, LENS_PSI_HY_Z, LENS_PSI_HZ_Y, LENS_PSI_HZ_X,
     LENS_PSI_EX_Y, LENS_PSI_EX_Z, LENS_PSI_EY_Z, LENS_PSI_EY_X, LENS_PSI_EZ_X, LENS_PSI_EZ_Y,

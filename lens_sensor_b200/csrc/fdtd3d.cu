@@ -66,16 +66,16 @@ __device__ __forceinline__ Hv h_cell(const K3 &g, int i, int j, int k, Hv h, flo
     const int sz = strip_of(k, g.az.h.lo, g.az.h.hi, g.az.h.n);
     const int sy = strip_of(j, g.ay.h.lo, g.ay.h.hi, g.ay.h.n);
     const int sx = strip_of(i, g.ax.h.lo, g.ax.h.hi, g.ax.h.n);
-    const int wz = g.az.h.lo + g.az.h.hi, wy = g.ay.h.lo + g.ay.h.hi;
+    const size_t c = ((size_t)i * ny + j) * P + k;  // psi is full-domain, same index as the fields
     Hv o = h;
     if (j < ny - 1 && k < nz - 1) {
         const float d1 = eyk - ey, d2 = ezj - ez;
         float v = h.x + ch * (d1 - d2);
         if (sz >= 0)
-            v = v + ch * psi_upd(g.pr[LENS_PSI_HX_Z], g.pw[LENS_PSI_HX_Z], ((size_t)i * ny + j) * wz + sz,
+            v = v + ch * psi_upd(g.pr[LENS_PSI_HX_Z], g.pw[LENS_PSI_HX_Z], c,
                                  own, g.az.h, k, d1);
         if (sy >= 0)
-            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HX_Y], g.pw[LENS_PSI_HX_Y], ((size_t)i * wy + sy) * P + k,
+            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HX_Y], g.pw[LENS_PSI_HX_Y], c,
                                     own, g.ay.h, j, d2);
         o.x = v;
     }
@@ -83,10 +83,10 @@ __device__ __forceinline__ Hv h_cell(const K3 &g, int i, int j, int k, Hv h, flo
         const float d1 = ezn - ez, d2 = exk - ex;
         float v = h.y + ch * (d1 - d2);
         if (sx >= 0)
-            v = v + ch * psi_upd(g.pr[LENS_PSI_HY_X], g.pw[LENS_PSI_HY_X], ((size_t)sx * ny + j) * P + k,
+            v = v + ch * psi_upd(g.pr[LENS_PSI_HY_X], g.pw[LENS_PSI_HY_X], c,
                                  own, g.ax.h, i, d1);
         if (sz >= 0)
-            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HY_Z], g.pw[LENS_PSI_HY_Z], ((size_t)i * ny + j) * wz + sz,
+            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HY_Z], g.pw[LENS_PSI_HY_Z], c,
                                     own, g.az.h, k, d2);
         o.y = v;
     }
@@ -94,10 +94,10 @@ __device__ __forceinline__ Hv h_cell(const K3 &g, int i, int j, int k, Hv h, flo
         const float d1 = exj - ex, d2 = eyn - ey;
         float v = h.z + ch * (d1 - d2);
         if (sy >= 0)
-            v = v + ch * psi_upd(g.pr[LENS_PSI_HZ_Y], g.pw[LENS_PSI_HZ_Y], ((size_t)i * wy + sy) * P + k,
+            v = v + ch * psi_upd(g.pr[LENS_PSI_HZ_Y], g.pw[LENS_PSI_HZ_Y], c,
                                  own, g.ay.h, j, d1);
         if (sx >= 0)
-            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HZ_X], g.pw[LENS_PSI_HZ_X], ((size_t)sx * ny + j) * P + k,
+            v = v + (-ch) * psi_upd(g.pr[LENS_PSI_HZ_X], g.pw[LENS_PSI_HZ_X], c,
                                     own, g.ax.h, i, d2);
         o.z = v;
     }
@@ -128,7 +128,7 @@ __device__ __forceinline__ Hv e_cell(const K3 &g, const LensStepTable &tab, int 
                                      Hv e, Hv h, float hxk, float hyk, float hxj, float hzj, float hym,
                                      float hzm, const Coef &c, bool lossy) {
     const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
-    const int wz = g.az.e.lo + g.az.e.hi, wy = g.ay.e.lo + g.ay.e.hi;
+    const size_t c0 = ((size_t)i * ny + j) * P + k;  // psi index (full-domain)
     const int sz = strip_of(k, g.az.e.lo, g.az.e.hi, g.az.e.n);
     const int sy = strip_of(j, g.ay.e.lo, g.ay.e.hi, g.ay.e.n);
     const int sx = strip_of(i, g.ax.e.lo, g.ax.e.hi, g.ax.e.n);
@@ -140,10 +140,10 @@ __device__ __forceinline__ Hv e_cell(const K3 &g, const LensStepTable &tab, int 
             const float d1 = h.z - hzj, d2 = h.y - hyk;
             v = v + c.cx * (d1 - d2);
             if (sy >= 0)
-                v = v + c.cx * psi_upd(g.pr[LENS_PSI_EX_Y], g.pw[LENS_PSI_EX_Y], ((size_t)i * wy + sy) * P + k,
+                v = v + c.cx * psi_upd(g.pr[LENS_PSI_EX_Y], g.pw[LENS_PSI_EX_Y], c0,
                                        true, g.ay.e, j, d1);
             if (sz >= 0)
-                v = v + (-c.cx) * psi_upd(g.pr[LENS_PSI_EX_Z], g.pw[LENS_PSI_EX_Z], ((size_t)i * ny + j) * wz + sz,
+                v = v + (-c.cx) * psi_upd(g.pr[LENS_PSI_EX_Z], g.pw[LENS_PSI_EX_Z], c0,
                                           true, g.az.e, k, d2);
         }
         if ((g.pec[2] && j == 0) || (g.pec[3] && j == ny - 1) || (g.pec[4] && k == 0) ||
@@ -158,10 +158,10 @@ __device__ __forceinline__ Hv e_cell(const K3 &g, const LensStepTable &tab, int 
             const float d1 = h.x - hxk, d2 = h.z - hzm;
             v = v + c.cy * (d1 - d2);
             if (sz >= 0)
-                v = v + c.cy * psi_upd(g.pr[LENS_PSI_EY_Z], g.pw[LENS_PSI_EY_Z], ((size_t)i * ny + j) * wz + sz,
+                v = v + c.cy * psi_upd(g.pr[LENS_PSI_EY_Z], g.pw[LENS_PSI_EY_Z], c0,
                                        true, g.az.e, k, d1);
             if (sx >= 0)
-                v = v + (-c.cy) * psi_upd(g.pr[LENS_PSI_EY_X], g.pw[LENS_PSI_EY_X], ((size_t)sx * ny + j) * P + k,
+                v = v + (-c.cy) * psi_upd(g.pr[LENS_PSI_EY_X], g.pw[LENS_PSI_EY_X], c0,
                                           true, g.ax.e, i, d2);
         }
         if ((g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1) || (g.pec[4] && k == 0) ||
@@ -176,10 +176,10 @@ __device__ __forceinline__ Hv e_cell(const K3 &g, const LensStepTable &tab, int 
             const float d1 = h.y - hym, d2 = h.x - hxj;
             v = v + c.cz * (d1 - d2);
             if (sx >= 0)
-                v = v + c.cz * psi_upd(g.pr[LENS_PSI_EZ_X], g.pw[LENS_PSI_EZ_X], ((size_t)sx * ny + j) * P + k,
+                v = v + c.cz * psi_upd(g.pr[LENS_PSI_EZ_X], g.pw[LENS_PSI_EZ_X], c0,
                                        true, g.ax.e, i, d1);
             if (sy >= 0)
-                v = v + (-c.cz) * psi_upd(g.pr[LENS_PSI_EZ_Y], g.pw[LENS_PSI_EZ_Y], ((size_t)i * wy + sy) * P + k,
+                v = v + (-c.cz) * psi_upd(g.pr[LENS_PSI_EZ_Y], g.pw[LENS_PSI_EZ_Y], c0,
                                           true, g.ay.e, j, d2);
         }
         if ((g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1) || (g.pec[2] && j == 0) ||
@@ -207,7 +207,7 @@ __device__ __forceinline__ void plane3(const LensEpi3D &ep, const LensStepTable 
 //   flux planes:    FP64 DFT of E and of the x-averaged H (flux.py:28-41)
 __device__ __forceinline__ void epi_cell(const K3 &g, const LensStepTable &tab, const LensEpi3D &ep,
                                          int n, int i, int j, int k, bool in, Hv e, float hym,
-                                         float hzm, Hv h) {
+                                         float hzm, Hv h, bool vol_dft = true) {
     const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
     const bool vx = in && i < nx - 1, vy = in && j < ny - 1, vz = in && k < nz - 1;
     if (ep.nbox > 0) {
@@ -238,9 +238,11 @@ __device__ __forceinline__ void epi_cell(const K3 &g, const LensStepTable &tab, 
     if (prevw && vf && k == ep.conv_k)
         kahan_add(reinterpret_cast<float4 *>(ep.conv_prev) + (size_t)i * g.src.nj + j, f * pr, f * pim);
     if (!win) return;
-    if (ep.dft[0] && vx) kahan_add(reinterpret_cast<float4 *>(ep.dft[0]) + o, e.x * pr, e.x * pim);
-    if (ep.dft[1] && vy) kahan_add(reinterpret_cast<float4 *>(ep.dft[1]) + o, e.y * pr, e.y * pim);
-    if (ep.dft[2] && vz) kahan_add(reinterpret_cast<float4 *>(ep.dft[2]) + o, e.z * pr, e.z * pim);
+    if (vol_dft) {
+        if (ep.dft[0] && vx) kahan_add(reinterpret_cast<float4 *>(ep.dft[0]) + o, e.x * pr, e.x * pim);
+        if (ep.dft[1] && vy) kahan_add(reinterpret_cast<float4 *>(ep.dft[1]) + o, e.y * pr, e.y * pim);
+        if (ep.dft[2] && vz) kahan_add(reinterpret_cast<float4 *>(ep.dft[2]) + o, e.z * pr, e.z * pim);
+    }
     if (ep.conv_last && vf && k == ep.conv_k)
         kahan_add(reinterpret_cast<float4 *>(ep.conv_last) + (size_t)i * g.src.nj + j, f * pr, f * pim);
     for (int p = 0; p < ep.nplane; ++p) {
@@ -370,7 +372,11 @@ constexpr int OFF_H = NSE * 3 * E_SLOT;
 constexpr int OFF_C = OFF_H + NSH * 3 * H_SLOT;
 constexpr int OFF_SH = OFF_C + NSC * 6 * C_BYTES;
 constexpr int OFF_BAR = OFF_SH + ((2 * 3 * SH_N * 4 + 127) / 128) * 128;
-constexpr int SMEM_FUSED = OFF_BAR + (NSE + NSH + NSC) * 8;
+constexpr int SMEM_LEAN = OFF_BAR + (NSE + NSH + NSC) * 8;
+// strip CTAs also stage psi: 6 H-psi tiles per H stage, 6 E-psi tiles per C stage
+constexpr int OFF_HP = ((SMEM_LEAN + 127) / 128) * 128;
+constexpr int OFF_EP = OFF_HP + NSH * 6 * H_SLOT;
+constexpr int SMEM_STRIP = OFF_EP + NSC * 6 * C_BYTES;
 static_assert(E_SLOT % 128 == 0 && E_SLOT >= E_BYTES, "E slot");
 static_assert(H_SLOT % 128 == 0 && H_SLOT >= H_BYTES, "H slot");
 static_assert(OFF_H % 128 == 0 && OFF_C % 128 == 0 && OFF_SH % 128 == 0, "alignment");
@@ -379,6 +385,7 @@ struct TMaps {
     CUtensorMap e[3];  // E of the read buffer, box EK x EJ x 1
     CUtensorMap h[3];  // H of the read buffer, box HK x HJ x 1
     CUtensorMap c[6];  // ce_x, ce_y, ce_z, D_x, D_y, D_z, box BK x BJ x 1
+    CUtensorMap p[12]; // psi of the read buffer (LENS_PSI_* order): H-psi box HK x HJ, E-psi BK x BJ
 };
 
 __device__ __forceinline__ uint32_t s_addr(const void *p) {
@@ -394,15 +401,17 @@ __device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded wait for phase `parity` of an mbarrier; false if it gave up.
+// Bounded wait for phase `parity` of an mbarrier; false if it gave up.  Each
+// try_wait may suspend the thread for up to 1 us (suspend-time hint), so the
+// bound (2^20 tries) is about a second.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok = 0;
-    for (int t = 0; t < (1 << 22) && !ok; ++t) {
+    for (int t = 0; t < (1 << 20) && !ok; ++t) {
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
             " selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(ok)
-            : "r"(bar), "r"(parity)
+            : "r"(bar), "r"(parity), "r"(1000u)
             : "memory");
     }
     return ok != 0;
@@ -417,7 +426,7 @@ __device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap *m, int c0,
         : "memory");
 }
 
-// CPML values of one coordinate: psi strip slot (-1 outside) and b, c, 1/kappa - 1.
+// CPML values of one coordinate: inside a psi strip?  and b, c, 1/kappa - 1.
 struct PV {
     int s;
     float b, c, km;
@@ -436,12 +445,16 @@ __device__ __forceinline__ PV pv_at(const LensProfile &p, int m) {
     return r;
 }
 
-// psi update with the old value already in a register: stores the new psi
-// (owner only) and returns psi + (1/kappa - 1)*d.
+// psi update: stores the new psi (owner only) and returns psi + (1/kappa - 1)*d.
 __device__ __forceinline__ float psi_u(float old, const PV &v, float d, float *pw, size_t idx, bool wr) {
     const float p = v.b * old + v.c * d;
     if (wr) pw[idx] = p;
     return p + v.km * d;
+}
+
+// does [a, b] meet a psi strip of profile p?
+__device__ __forceinline__ bool meets(int a, int b, const LensProfile &p) {
+    return (p.lo > 0 && a < p.lo) || (p.hi > 0 && b >= p.n - p.hi);
 }
 
 constexpr int MAXCH = 96;
@@ -453,11 +466,23 @@ struct Chunks {
     int strip[MAXCH];
 };
 
+// Ring slot (stage) and phase parity of the u-th use, tracked incrementally.
+struct Ring {
+    int s, ph;
+    int n;
+    __device__ __forceinline__ void next() {
+        if (++s == n) {
+            s = 0;
+            ph ^= 1;
+        }
+    }
+};
+
 // One launch per block category: ST = false runs only the blocks whose tile
-// and x-chunk touch no CPML strip (no psi at all), ST = true the others, with
-// the psi of the next plane prefetched into registers while the current plane
-// is computed.
-template <bool ST>
+// and x-chunk meet no CPML strip (no psi at all), ST = true the others, whose
+// psi tiles are staged by TMA next to the field tiles.  Only the producer lane
+// waits on the mbarriers; the other warps sleep in the CTA barrier.
+template <bool ST, bool DF>
 __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
     fused3d(const __grid_constant__ TMaps tm, const K3 g, const LensStepTable tab,
             const LensEpi3D ep, int n, int epi, const __grid_constant__ Chunks chs) {
@@ -465,20 +490,19 @@ __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
     const int k0 = blockIdx.x * BK, j0 = blockIdx.y * BJ;
     const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
     const int x0 = chs.x[blockIdx.z], x1 = chs.x[blockIdx.z + 1];
-    {   // block category (uniform)
-        auto hits = [](int a, int b, const LensProfile &p, int shift) {  // [a, b] meets a strip of p
-            return (p.lo > 0 && a < p.lo + shift) || (p.hi > 0 && b >= p.n - p.hi + shift);
-        };
-        const bool yz = hits(j0 - 1, j0 + BJ - 1, g.ay.h, 0) || hits(j0, j0 + BJ - 1, g.ay.e, 0) ||
-                        hits(k0 - 1, k0 + BK - 1, g.az.h, 0) || hits(k0, k0 + BK - 1, g.az.e, 0);
-        if ((yz || chs.strip[blockIdx.z] != 0) != ST) return;
-    }
+    // block category (uniform); psi tiles this CTA needs
+    const bool nz_h = meets(k0 - 1, k0 + BK - 1, g.az.h), ny_h = meets(j0 - 1, j0 + BJ - 1, g.ay.h);
+    const bool nz_e = meets(k0, k0 + BK - 1, g.az.e), ny_e = meets(j0, j0 + BJ - 1, g.ay.e);
+    if ((nz_h || ny_h || nz_e || ny_e || chs.strip[blockIdx.z] != 0) != ST) return;
     extern __shared__ __align__(128) unsigned char smem[];
-    float *sE = reinterpret_cast<float *>(smem);
-    float *sHo = reinterpret_cast<float *>(smem + OFF_H);
-    float *sC = reinterpret_cast<float *>(smem + OFF_C);
+    const float *sE = reinterpret_cast<const float *>(smem);
+    const float *sHo = reinterpret_cast<const float *>(smem + OFF_H);
+    const float *sC = reinterpret_cast<const float *>(smem + OFF_C);
     float *sH = reinterpret_cast<float *>(smem + OFF_SH);
-    const uint32_t bar0 = s_addr(smem + OFF_BAR);
+    const float *sHP = reinterpret_cast<const float *>(smem + OFF_HP);
+    const float *sEP = reinterpret_cast<const float *>(smem + OFF_EP);
+    const uint32_t sbase = s_addr(smem);
+    const uint32_t bar0 = sbase + OFF_BAR;
     const int xs = x0 > 0 ? x0 - 1 : 0;  // plane x0-1: its H feeds E(x0)
     const bool lossy = g.da_x != nullptr;
     const int ncoef = lossy ? 6 : 3;
@@ -499,7 +523,6 @@ __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
     const bool hact = hrole && j >= 0 && j < ny && k >= 0 && k < nz;
     const int ea = ej * EK + ek, ha = ej * HK + ek;
     const bool hx_ok = hact && j < ny - 1 && k < nz - 1, hy_k = hact && k < nz - 1, hz_j = hact && j < ny - 1;
-    const size_t jny = (size_t)ny;
     const bool ein = own && j < ny && k < nz;
     const bool jin = j >= 1 && j <= ny - 2, kin = k >= 1 && k <= nz - 2;
     const bool pec_j = (g.pec[2] && j == 0) || (g.pec[3] && j == ny - 1);
@@ -511,98 +534,90 @@ __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
         s_ph1 = g.src.ph1[m];
         s_ph2 = g.src.ph2[m];
     }
-    // strip data of this thread's cell (ST only)
     PV zh{-1, 1.f, 0.f, 0.f}, yh = zh, ze = zh, ye = zh;
-    int wzh = 0, wyh = 0, wze = 0, wye = 0;
-    size_t xoff = 0;
-    float hp[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, epv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    auto load_hpsi = [&](int p) {
-        const PV xh = pv_at(g.ax.h, p);
-        const bool iok = p < nx - 1;
-        const size_t zb = ((size_t)p * jny + j) * wzh + zh.s, yb = ((size_t)p * wyh + yh.s) * P + k;
-        const size_t xb = xoff + (size_t)xh.s * jny * P;
-        hp[0] = (hx_ok && zh.s >= 0) ? g.pr[LENS_PSI_HX_Z][zb] : 0.f;
-        hp[1] = (hx_ok && yh.s >= 0) ? g.pr[LENS_PSI_HX_Y][yb] : 0.f;
-        hp[2] = (iok && hy_k && xh.s >= 0) ? g.pr[LENS_PSI_HY_X][xb] : 0.f;
-        hp[3] = (iok && hy_k && zh.s >= 0) ? g.pr[LENS_PSI_HY_Z][zb] : 0.f;
-        hp[4] = (iok && hz_j && yh.s >= 0) ? g.pr[LENS_PSI_HZ_Y][yb] : 0.f;
-        hp[5] = (iok && hz_j && xh.s >= 0) ? g.pr[LENS_PSI_HZ_X][xb] : 0.f;
-    };
-    auto load_epsi = [&](int p) {
-        const PV xe = pv_at(g.ax.e, p);
-        const bool iok = p < nx - 1, iin = p >= 1 && p <= nx - 2;
-        const size_t zb = ((size_t)p * jny + j) * wze + ze.s, yb = ((size_t)p * wye + ye.s) * P + k;
-        const size_t xb = xoff + (size_t)xe.s * jny * P;
-        const bool vx = ein && iok && jin && kin, vy = ein && j < ny - 1 && iin && kin,
-                   vz = ein && k < nz - 1 && iin && jin;
-        epv[0] = (vx && ye.s >= 0) ? g.pr[LENS_PSI_EX_Y][yb] : 0.f;
-        epv[1] = (vx && ze.s >= 0) ? g.pr[LENS_PSI_EX_Z][zb] : 0.f;
-        epv[2] = (vy && ze.s >= 0) ? g.pr[LENS_PSI_EY_Z][zb] : 0.f;
-        epv[3] = (vy && xe.s >= 0) ? g.pr[LENS_PSI_EY_X][xb] : 0.f;
-        epv[4] = (vz && xe.s >= 0) ? g.pr[LENS_PSI_EZ_X][xb] : 0.f;
-        epv[5] = (vz && ye.s >= 0) ? g.pr[LENS_PSI_EZ_Y][yb] : 0.f;
-    };
     if (ST) {
         zh = pv_at(g.az.h, k); yh = pv_at(g.ay.h, j);
         ze = pv_at(g.az.e, k); ye = pv_at(g.ay.e, j);
-        wzh = g.az.h.lo + g.az.h.hi; wyh = g.ay.h.lo + g.ay.h.hi;
-        wze = g.az.e.lo + g.az.e.hi; wye = g.ay.e.lo + g.ay.e.hi;
-        xoff = (size_t)j * P + k;
-        load_hpsi(xs);
-        if (x0 < x1) load_epsi(x0);
     }
+    const size_t S = (size_t)ny * P;
+    size_t o = ((size_t)xs * ny + j) * P + k;  // field / psi index of (xs, j, k)
 
+    auto issue_e = [&](int p, int s) {
+        const uint32_t bar = bar0 + 8u * s;
+        mbar_expect(bar, 3 * E_BYTES);
+        for (int c = 0; c < 3; ++c) tma3(sbase + (s * 3 + c) * E_SLOT, &tm.e[c], k0 - 4, j0 - 1, p, bar);
+    };
+    auto issue_h = [&](int p, int s) {
+        const uint32_t bar = bar0 + 8u * (NSE + s);
+        int np = 0;
+        bool pn[6] = {false, false, false, false, false, false};
+        if (ST) {
+            const bool xh = meets(p, p, g.ax.h);
+            pn[0] = nz_h; pn[1] = ny_h; pn[2] = xh; pn[3] = nz_h; pn[4] = ny_h; pn[5] = xh;
+            for (int q = 0; q < 6; ++q) np += pn[q];
+        }
+        mbar_expect(bar, (3 + np) * H_BYTES);
+        for (int c = 0; c < 3; ++c) tma3(sbase + OFF_H + (s * 3 + c) * H_SLOT, &tm.h[c], k0 - 4, j0 - 1, p, bar);
+        if (ST)
+            for (int q = 0; q < 6; ++q)
+                if (pn[q]) tma3(sbase + OFF_HP + (s * 6 + q) * H_SLOT, &tm.p[q], k0 - 4, j0 - 1, p, bar);
+    };
+    auto issue_c = [&](int p, int s) {
+        const uint32_t bar = bar0 + 8u * (NSE + NSH + s);
+        int np = 0;
+        bool pn[6] = {false, false, false, false, false, false};
+        if (ST) {
+            const bool xe = meets(p, p, g.ax.e);
+            pn[0] = ny_e; pn[1] = nz_e; pn[2] = nz_e; pn[3] = xe; pn[4] = xe; pn[5] = ny_e;
+            for (int q = 0; q < 6; ++q) np += pn[q];
+        }
+        mbar_expect(bar, (ncoef + np) * C_BYTES);
+        for (int c = 0; c < ncoef; ++c) tma3(sbase + OFF_C + (s * 6 + c) * C_BYTES, &tm.c[c], k0, j0, p, bar);
+        if (ST)
+            for (int q = 0; q < 6; ++q)
+                if (pn[q]) tma3(sbase + OFF_EP + (s * 6 + q) * C_BYTES, &tm.p[6 + q], k0, j0, p, bar);
+    };
+    // rings: E holds planes xs.., H planes xs.., C planes x0..; the producer lane
+    // issues and waits, everybody else only uses __syncthreads
+    Ring we{0, 0, NSE}, wh{0, 0, NSH}, wc{0, 0, NSC};  // waiter cursors
+    Ring fe{0, 0, NSE}, fh{0, 0, NSH}, fc{0, 0, NSC};  // fill cursors
+    bool ok = true;
     if (prod) {
         for (int q = 0; q < NSE + NSH + NSC; ++q) mbar_init(bar0 + 8u * q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int p = xs; p <= min(x1, xs + NSE - 1); ++p, fe.next()) issue_e(p, fe.s);
+        for (int p = xs; p <= min(x1 - 1, xs + NSH - 1); ++p, fh.next()) issue_h(p, fh.s);
+        for (int p = x0; p <= min(x1 - 1, x0 + NSC - 1); ++p, fc.next()) issue_c(p, fc.s);
+        ok &= mbar_wait(bar0 + 8u * we.s, we.ph);  // E(xs)
+        we.next();
+        ok &= mbar_wait(bar0 + 8u * we.s, we.ph);  // E(xs+1)
+        ok &= mbar_wait(bar0 + 8u * (NSE + wh.s), wh.ph);  // H(xs)
+        wh.next();
     }
     __syncthreads();
-    auto bar_e = [&](int q) { return bar0 + 8u * q; };
-    auto bar_h = [&](int q) { return bar0 + 8u * (NSE + q); };
-    auto bar_c = [&](int q) { return bar0 + 8u * (NSE + NSH + q); };
-    auto issue_e = [&](int p) {
-        const int q = (p - xs) % NSE;
-        mbar_expect(bar_e(q), 3 * E_BYTES);
-        for (int c = 0; c < 3; ++c)
-            tma3(s_addr(reinterpret_cast<unsigned char *>(sE) + (q * 3 + c) * E_SLOT), &tm.e[c], k0 - 4,
-                 j0 - 1, p, bar_e(q));
-    };
-    auto issue_h = [&](int p) {
-        const int q = (p - xs) % NSH;
-        mbar_expect(bar_h(q), 3 * H_BYTES);
-        for (int c = 0; c < 3; ++c)
-            tma3(s_addr(reinterpret_cast<unsigned char *>(sHo) + (q * 3 + c) * H_SLOT), &tm.h[c], k0 - 4,
-                 j0 - 1, p, bar_h(q));
-    };
-    auto issue_c = [&](int p) {
-        const int q = (p - x0) % NSC;
-        mbar_expect(bar_c(q), ncoef * C_BYTES);
-        for (int c = 0; c < ncoef; ++c)
-            tma3(s_addr(reinterpret_cast<unsigned char *>(sC) + (q * 6 + c) * C_BYTES), &tm.c[c], k0, j0, p,
-                 bar_c(q));
-    };
-    if (prod) {
-        for (int p = xs; p <= min(x1, xs + NSE - 1); ++p) issue_e(p);
-        for (int p = xs; p <= min(x1 - 1, xs + NSH - 1); ++p) issue_h(p);
-        for (int p = x0; p <= min(x1 - 1, x0 + NSC - 1); ++p) issue_c(p);
-    }
-    bool ok = mbar_wait(bar_e(0), 0);
     const int EF = E_SLOT / 4, HF = H_SLOT / 4, CF = C_BYTES / 4;
     const int q0 = n - tab.t0;
     const float env = tab.env[q0], wt = tab.wt[q0];
+    const bool win = DF && epi && n >= ep.dft_n0 && n < ep.dft_n1;
     float hym = 0.f, hzm = 0.f;  // own H(i-1), new
-    for (int i = xs; i < x1; ++i) {
-        const int u = i - xs;
+    int se = 0, sh = 0, sc = 0;  // stage of E(i), H(i), C(i)
+    for (int i = xs; i < x1; ++i, o += S) {
         const bool eon = i >= x0;
-        ok &= mbar_wait(bar_e((u + 1) % NSE), ((u + 1) / NSE) & 1);
-        ok &= mbar_wait(bar_h(u % NSH), (u / NSH) & 1);
-        if (eon && own) ok &= mbar_wait(bar_c((i - x0) % NSC), ((i - x0) / NSC) & 1);
-        const float *eC = sE + (u % NSE) * 3 * EF;
-        const float *eN = sE + ((u + 1) % NSE) * 3 * EF;
-        const float *hO = sHo + (u % NSH) * 3 * HF;
-        float *shw = sH + (u & 1) * 3 * SH_N;
+        const int se1 = se + 1 == NSE ? 0 : se + 1;
+        const float *eC = sE + se * 3 * EF;
+        const float *eN = sE + se1 * 3 * EF;
+        const float *hO = sHo + sh * 3 * HF;
+        float *shw = sH + ((i - xs) & 1) * 3 * SH_N;
         const bool iok = i < nx - 1;
 
+        // DFT accumulators of this plane: loaded now, used after the H phase
+        float4 acc[DF ? 3 : 1];
+        const bool dft_now = DF && win && ein && eon;
+        if (DF && dft_now) {
+#pragma unroll
+            for (int c = 0; c < (DF ? 3 : 1); ++c)
+                if (ep.dft[c]) acc[c] = reinterpret_cast<const float4 *>(ep.dft[c])[o];
+        }
         // ---- H(i) at (j, k)
         const float ex = eC[ea], ey = eC[EF + ea], ez = eC[2 * EF + ea];
         float hx = 0.f, hy = 0.f, hz = 0.f;
@@ -610,37 +625,27 @@ __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
             hx = hO[ha];
             hy = hO[HF + ha];
             hz = hO[2 * HF + ha];
-            if (hx_ok) {
-                const float d1 = eC[EF + ea + 1] - ey, d2 = eC[2 * EF + ea + EK] - ez;
-                hx = hx + ch * (d1 - d2);
-            }
-            if (iok && hy_k) {
-                const float d1 = eN[2 * EF + ea] - ez, d2 = eC[ea + 1] - ex;
-                hy = hy + ch * (d1 - d2);
-            }
-            if (iok && hz_j) {
-                const float d1 = eC[ea + EK] - ex, d2 = eN[EF + ea] - ey;
-                hz = hz + ch * (d1 - d2);
-            }
+            const float dxz = eC[EF + ea + 1] - ey, dxy = eC[2 * EF + ea + EK] - ez;  // Hx terms
+            const float dyx = eN[2 * EF + ea] - ez, dyz = eC[ea + 1] - ex;          // Hy terms
+            const float dzy = eC[ea + EK] - ex, dzx = eN[EF + ea] - ey;             // Hz terms
+            if (hx_ok) hx = hx + ch * (dxz - dxy);
+            if (iok && hy_k) hy = hy + ch * (dyx - dyz);
+            if (iok && hz_j) hz = hz + ch * (dzy - dzx);
             if (ST) {
                 const bool wr = own && eon;  // psi of this plane is written by its owner only
                 const PV xh = pv_at(g.ax.h, i);
-                const size_t zb = ((size_t)i * jny + j) * wzh + zh.s, yb = ((size_t)i * wyh + yh.s) * P + k;
-                const size_t xb = xoff + (size_t)xh.s * jny * P;
+                const float *hp = sHP + sh * 6 * HF + ha;
                 if (hx_ok) {
-                    const float d1 = eC[EF + ea + 1] - ey, d2 = eC[2 * EF + ea + EK] - ez;
-                    if (zh.s >= 0) hx = hx + ch * psi_u(hp[0], zh, d1, g.pw[LENS_PSI_HX_Z], zb, wr);
-                    if (yh.s >= 0) hx = hx + (-ch) * psi_u(hp[1], yh, d2, g.pw[LENS_PSI_HX_Y], yb, wr);
+                    if (zh.s >= 0) hx = hx + ch * psi_u(hp[0], zh, dxz, g.pw[LENS_PSI_HX_Z], o, wr);
+                    if (yh.s >= 0) hx = hx + (-ch) * psi_u(hp[HF], yh, dxy, g.pw[LENS_PSI_HX_Y], o, wr);
                 }
                 if (iok && hy_k) {
-                    const float d1 = eN[2 * EF + ea] - ez, d2 = eC[ea + 1] - ex;
-                    if (xh.s >= 0) hy = hy + ch * psi_u(hp[2], xh, d1, g.pw[LENS_PSI_HY_X], xb, wr);
-                    if (zh.s >= 0) hy = hy + (-ch) * psi_u(hp[3], zh, d2, g.pw[LENS_PSI_HY_Z], zb, wr);
+                    if (xh.s >= 0) hy = hy + ch * psi_u(hp[2 * HF], xh, dyx, g.pw[LENS_PSI_HY_X], o, wr);
+                    if (zh.s >= 0) hy = hy + (-ch) * psi_u(hp[3 * HF], zh, dyz, g.pw[LENS_PSI_HY_Z], o, wr);
                 }
                 if (iok && hz_j) {
-                    const float d1 = eC[ea + EK] - ex, d2 = eN[EF + ea] - ey;
-                    if (yh.s >= 0) hz = hz + ch * psi_u(hp[4], yh, d1, g.pw[LENS_PSI_HZ_Y], yb, wr);
-                    if (xh.s >= 0) hz = hz + (-ch) * psi_u(hp[5], xh, d2, g.pw[LENS_PSI_HZ_X], xb, wr);
+                    if (yh.s >= 0) hz = hz + ch * psi_u(hp[4 * HF], yh, dzy, g.pw[LENS_PSI_HZ_Y], o, wr);
+                    if (xh.s >= 0) hz = hz + (-ch) * psi_u(hp[5 * HF], xh, dzx, g.pw[LENS_PSI_HZ_X], o, wr);
                 }
             }
         }
@@ -649,92 +654,130 @@ __global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
             shw[SH_N + sa] = hy;
             shw[2 * SH_N + sa] = hz;
         }
-        if (ST && i + 1 < x1) load_hpsi(i + 1);
+        if (prod) {  // data of this plane's E phase and of the next plane's H phase
+            if (eon) {
+                ok &= mbar_wait(bar0 + 8u * (NSE + NSH + wc.s), wc.ph);
+                wc.next();
+            }
+            if (i + 2 <= x1) {
+                we.next();
+                ok &= mbar_wait(bar0 + 8u * we.s, we.ph);
+            }
+            if (i + 1 <= x1 - 1) {
+                ok &= mbar_wait(bar0 + 8u * (NSE + wh.s), wh.ph);
+                wh.next();
+            }
+        }
         __syncthreads();
         // E(i) and H(i) stages are free now, and the coefficients of plane i-1
         if (prod) {
-            if (i + NSE <= x1) issue_e(i + NSE);
-            if (i + NSH <= x1 - 1) issue_h(i + NSH);
-            if (i - 1 >= x0 && i - 1 + NSC <= x1 - 1) issue_c(i - 1 + NSC);
+            if (i + NSE <= x1) {
+                issue_e(i + NSE, fe.s);
+                fe.next();
+            }
+            if (i + NSH <= x1 - 1) {
+                issue_h(i + NSH, fh.s);
+                fh.next();
+            }
+            if (i - 1 >= x0 && i - 1 + NSC <= x1 - 1) {
+                issue_c(i - 1 + NSC, fc.s);
+                fc.next();
+            }
         }
         if (own && eon) {
-            const size_t o = ((size_t)i * jny + j) * P + k;
             Hv e{0.f, 0.f, 0.f};
             if (ein) {
                 g.whx[o] = hx;
                 g.why[o] = hy;
                 g.whz[o] = hz;
-                const float *cs = sC + ((i - x0) % NSC) * 6 * CF;
                 const int ca = w * BK + lane;
+                const float *cs = sC + sc * 6 * CF + ca;
                 const bool iin = i >= 1 && i <= nx - 2;
                 const bool pec_i = (g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1);
                 float src = 0.f;
                 if (i == g.src.ix) src = (env * sinf(wt + s_ph1)) * s_amp;
                 else if (g.src.ix >= 0 && i == g.src.ix + 1) src = -((env * sinf(wt + s_ph2)) * s_amp);
-                PV xe{-1, 1.f, 0.f, 0.f};
-                size_t zb = 0, yb = 0, xb = 0;
+                const float hzj = shw[2 * SH_N + sa - SHK], hyk = shw[SH_N + sa - 1];
+                const float hxk = shw[sa - 1], hxj = shw[sa - SHK];
+                const float d1x = hz - hzj, d2x = hy - hyk;  // Ex
+                const float d1y = hx - hxk, d2y = hz - hzm;  // Ey
+                const float d1z = hy - hym, d2z = hx - hxj;  // Ez
+                float vx = ex, vy = ey, vz = ez;
+                if (iok) {
+                    if (lossy) vx = vx * cs[3 * CF];
+                    if (jin && kin) vx = vx + cs[0] * (d1x - d2x);
+                }
+                if (j < ny - 1) {
+                    if (lossy) vy = vy * cs[4 * CF];
+                    if (iin && kin) vy = vy + cs[CF] * (d1y - d2y);
+                }
+                if (k < nz - 1) {
+                    if (lossy) vz = vz * cs[5 * CF];
+                    if (iin && jin) vz = vz + cs[2 * CF] * (d1z - d2z);
+                }
                 if (ST) {
-                    xe = pv_at(g.ax.e, i);
-                    zb = ((size_t)i * jny + j) * wze + ze.s;
-                    yb = ((size_t)i * wye + ye.s) * P + k;
-                    xb = xoff + (size_t)xe.s * jny * P;
-                }
-                if (iok) {  // Ex
-                    const float cx = cs[ca];
-                    float v = lossy ? ex * cs[3 * CF + ca] : ex;
-                    if (jin && kin) {
-                        const float d1 = hz - shw[2 * SH_N + sa - SHK], d2 = hy - shw[SH_N + sa - 1];
-                        v = v + cx * (d1 - d2);
-                        if (ST) {
-                            if (ye.s >= 0) v = v + cx * psi_u(epv[0], ye, d1, g.pw[LENS_PSI_EX_Y], yb, true);
-                            if (ze.s >= 0) v = v + (-cx) * psi_u(epv[1], ze, d2, g.pw[LENS_PSI_EX_Z], zb, true);
-                        }
+                    const PV xe = pv_at(g.ax.e, i);
+                    const float *pp = sEP + sc * 6 * CF + ca;
+                    if (iok && jin && kin) {
+                        const float cx = cs[0];
+                        if (ye.s >= 0) vx = vx + cx * psi_u(pp[0], ye, d1x, g.pw[LENS_PSI_EX_Y], o, true);
+                        if (ze.s >= 0) vx = vx + (-cx) * psi_u(pp[CF], ze, d2x, g.pw[LENS_PSI_EX_Z], o, true);
                     }
-                    if (pec_j || pec_k) v = 0.f;
-                    if (g.src_comp == 0) v += src;
-                    e.x = v;
-                }
-                if (j < ny - 1) {  // Ey
-                    const float cy = cs[CF + ca];
-                    float v = lossy ? ey * cs[4 * CF + ca] : ey;
-                    if (iin && kin) {
-                        const float d1 = hx - shw[sa - 1], d2 = hz - hzm;
-                        v = v + cy * (d1 - d2);
-                        if (ST) {
-                            if (ze.s >= 0) v = v + cy * psi_u(epv[2], ze, d1, g.pw[LENS_PSI_EY_Z], zb, true);
-                            if (xe.s >= 0) v = v + (-cy) * psi_u(epv[3], xe, d2, g.pw[LENS_PSI_EY_X], xb, true);
-                        }
+                    if (j < ny - 1 && iin && kin) {
+                        const float cy = cs[CF];
+                        if (ze.s >= 0) vy = vy + cy * psi_u(pp[2 * CF], ze, d1y, g.pw[LENS_PSI_EY_Z], o, true);
+                        if (xe.s >= 0) vy = vy + (-cy) * psi_u(pp[3 * CF], xe, d2y, g.pw[LENS_PSI_EY_X], o, true);
                     }
-                    if (pec_i || pec_k) v = 0.f;
-                    if (g.src_comp == 1) v += src;
-                    e.y = v;
-                }
-                if (k < nz - 1) {  // Ez
-                    const float cz = cs[2 * CF + ca];
-                    float v = lossy ? ez * cs[5 * CF + ca] : ez;
-                    if (iin && jin) {
-                        const float d1 = hy - hym, d2 = hx - shw[sa - SHK];
-                        v = v + cz * (d1 - d2);
-                        if (ST) {
-                            if (xe.s >= 0) v = v + cz * psi_u(epv[4], xe, d1, g.pw[LENS_PSI_EZ_X], xb, true);
-                            if (ye.s >= 0) v = v + (-cz) * psi_u(epv[5], ye, d2, g.pw[LENS_PSI_EZ_Y], yb, true);
-                        }
+                    if (k < nz - 1 && iin && jin) {
+                        const float cz = cs[2 * CF];
+                        if (xe.s >= 0) vz = vz + cz * psi_u(pp[4 * CF], xe, d1z, g.pw[LENS_PSI_EZ_X], o, true);
+                        if (ye.s >= 0) vz = vz + (-cz) * psi_u(pp[5 * CF], ye, d2z, g.pw[LENS_PSI_EZ_Y], o, true);
                     }
-                    if (pec_i || pec_j) v = 0.f;
-                    if (g.src_comp == 2) v += src;
-                    e.z = v;
+                }
+                if (iok) {
+                    if (pec_j || pec_k) vx = 0.f;
+                    if (g.src_comp == 0) vx += src;
+                    e.x = vx;
+                }
+                if (j < ny - 1) {
+                    if (pec_i || pec_k) vy = 0.f;
+                    if (g.src_comp == 1) vy += src;
+                    e.y = vy;
+                }
+                if (k < nz - 1) {
+                    if (pec_i || pec_j) vz = 0.f;
+                    if (g.src_comp == 2) vz += src;
+                    e.z = vz;
                 }
                 g.wex[o] = e.x;
                 g.wey[o] = e.y;
                 g.wez[o] = e.z;
             }
-            if (epi) epi_cell(g, tab, ep, n, i, j, k, ein, e, hym, hzm, Hv{hx, hy, hz});
-            if (ST && i + 1 < x1) load_epsi(i + 1);
+            if (DF && dft_now) {
+                const float pr = tab.pe[2 * q0], pim = tab.pe[2 * q0 + 1];
+                const bool vx = iok, vy = j < ny - 1, vz = k < nz - 1;
+                if (ep.dft[0] && vx) {
+                    kahan_reg(acc[0], e.x * pr, e.x * pim);
+                    reinterpret_cast<float4 *>(ep.dft[0])[o] = acc[0];
+                }
+                if (ep.dft[1] && vy) {
+                    kahan_reg(acc[DF ? 1 : 0], e.y * pr, e.y * pim);
+                    reinterpret_cast<float4 *>(ep.dft[1])[o] = acc[DF ? 1 : 0];
+                }
+                if (ep.dft[2] && vz) {
+                    kahan_reg(acc[DF ? 2 : 0], e.z * pr, e.z * pim);
+                    reinterpret_cast<float4 *>(ep.dft[2])[o] = acc[DF ? 2 : 0];
+                }
+            }
+            if (epi) epi_cell(g, tab, ep, n, i, j, k, ein, e, hym, hzm, Hv{hx, hy, hz}, !DF);
         }
+        if (eon) sc = sc + 1 == NSC ? 0 : sc + 1;
+        se = se1;
+        sh = sh + 1 == NSH ? 0 : sh + 1;
         hym = hy;
         hzm = hz;
     }
-    if (!ok && g.flag) atomicExch(g.flag, 1);
+    if (prod && !ok && g.flag) atomicExch(g.flag, 1);
 }
 
 // ============================================================ Iavg
@@ -961,12 +1004,19 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
     const float *bases[6] = {g->ce_x, g->ce_y, g->ce_z, g->da_x, g->da_y, g->da_z};
     for (int q = 0; q < 6; ++q)
         if (reinterpret_cast<uintptr_t>(bases[q]) & 15) return LENS_ERR_ARG;
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < 2; ++b) {
         for (int c = 0; c < 6; ++c)
             if (reinterpret_cast<uintptr_t>(g->f[b][c]) & 15) return LENS_ERR_ARG;
-    if (cudaFuncSetAttribute(fused3d<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_FUSED) !=
+        for (int q = 0; q < LENS_NPSI; ++q)
+            if (!g->psi[b][q] || (reinterpret_cast<uintptr_t>(g->psi[b][q]) & 15)) return LENS_ERR_ARG;
+    }
+    if (cudaFuncSetAttribute(fused3d<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LEAN) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(fused3d<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_FUSED) !=
+        cudaFuncSetAttribute(fused3d<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LEAN) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(fused3d<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_STRIP) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(fused3d<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_STRIP) !=
             cudaSuccess)
         return LENS_ERR_CUDA;
     TMaps tm[2];
@@ -978,6 +1028,8 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
             ok = ok && encode(&tm[rb].c[c], bases[c], g, BK, BJ);
             ok = ok && encode(&tm[rb].c[3 + c], g->da_x ? bases[3 + c] : bases[c], g, BK, BJ);
         }
+        for (int q = 0; q < LENS_NPSI; ++q)  // H-psi tiles like H, E-psi tiles like the coefficients
+            ok = ok && encode(&tm[rb].p[q], g->psi[rb][q], g, q < 6 ? HK : BK, q < 6 ? HJ : BJ);
         if (!ok) return LENS_ERR_CUDA;
     }
     const Chunks chs = make_chunks(g, 40);
@@ -986,8 +1038,14 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
         const int rb = g->cur;
         const K3 k = view(g, rb, 1 - rb);
         const int ea = epi3d_active(&e, n);
-        fused3d<true><<<grd, dim3(BK, FW), SMEM_FUSED, s>>>(tm[rb], k, *tab, e, n, ea, chs);
-        fused3d<false><<<grd, dim3(BK, FW), SMEM_FUSED, s>>>(tm[rb], k, *tab, e, n, ea, chs);
+        const bool df = ea && n >= e.dft_n0 && n < e.dft_n1 && (e.dft[0] || e.dft[1] || e.dft[2]);
+        if (df) {
+            fused3d<true, true><<<grd, dim3(BK, FW), SMEM_STRIP, s>>>(tm[rb], k, *tab, e, n, ea, chs);
+            fused3d<false, true><<<grd, dim3(BK, FW), SMEM_LEAN, s>>>(tm[rb], k, *tab, e, n, ea, chs);
+        } else {
+            fused3d<true, false><<<grd, dim3(BK, FW), SMEM_STRIP, s>>>(tm[rb], k, *tab, e, n, ea, chs);
+            fused3d<false, false><<<grd, dim3(BK, FW), SMEM_LEAN, s>>>(tm[rb], k, *tab, e, n, ea, chs);
+        }
         g->cur = 1 - rb;
     }
     return lens_cuda_status();

@@ -14,6 +14,17 @@ LENS_HD int strip_of(int i, int lo, int hi, int n) {
 }
 
 // Compensated (Kahan) complex accumulation: a = (sum.re, sum.im, carry.re, carry.im).
+LENS_HD void kahan_reg(float4 &a, float re, float im) {
+    float y = re - a.z;
+    float t = a.x + y;
+    a.z = (t - a.x) - y;
+    a.x = t;
+    y = im - a.w;
+    t = a.y + y;
+    a.w = (t - a.y) - y;
+    a.y = t;
+}
+
 LENS_HD void kahan_add(float4 *p, float re, float im) {
     float4 a = *p;
     float y = re - a.z;

@@ -258,15 +258,8 @@ class Grid3D:
         X, Y, Zp = self.ax
         nbuf = 2 if fused else 1
         self.bufs = [{f: z() for f in self.FIELDS} for _ in range(nbuf)]
-        m1 = lambda w: max(1, w)
-        psi_shape = dict(
-            hx_z=(nx, ny, m1(Zp.w('h'))), hy_z=(nx, ny, m1(Zp.w('h'))),
-            ex_z=(nx, ny, m1(Zp.w('e'))), ey_z=(nx, ny, m1(Zp.w('e'))),
-            hx_y=(nx, m1(Y.w('h')), P), hz_y=(nx, m1(Y.w('h')), P),
-            ex_y=(nx, m1(Y.w('e')), P), ez_y=(nx, m1(Y.w('e')), P),
-            hy_x=(m1(X.w('h')), ny, P), hz_x=(m1(X.w('h')), ny, P),
-            ey_x=(m1(X.w('e')), ny, P), ez_x=(m1(X.w('e')), ny, P))
-        self.psi = [{q: z(*psi_shape[q]) for q in N.PSI_NAMES} for _ in range(nbuf)]
+        # psi volumes are full-domain (only their CPML strips are touched)
+        self.psi = [{q: z() for q in N.PSI_NAMES} for _ in range(nbuf)]
         self.ce = [_pad_upload(a, shp, dev) for a in ce]
         self.da = None if da is None else [_pad_upload(a, shp, dev) for a in da]
         amp = np.ascontiguousarray(src['amp'], F32)

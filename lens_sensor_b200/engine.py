@@ -222,6 +222,19 @@ class Epi2D:
         """Accumulated sum(F e^{-i w t}) on the nodes (nx, ny), complex128."""
         return _kahan_value(getattr(self, which))[:, :self.grid.ny]
 
+    def restart_dft(self, window):
+        """Open a new DFT window [n0, n1) after a failed CW convergence check
+        (fdtd2d_core.py:862-869): the finished window becomes the comparison
+        window; the DFT, the Ex DFT and the flux planes restart from zero."""
+        self.dft, self.prev = self.prev, self.dft
+        self.dft.zero_()
+        if self.dft_ex is not None:
+            self.dft_ex.zero_()
+        self.plane_acc.zero_()
+        self.s.dft, self.s.dft_prev = _ptr(self.dft), _ptr(self.prev)
+        self.s.dft_n0, self.s.dft_n1 = int(window[0]), int(window[1])
+        self.s.prev_n0 = self.s.prev_n1 = 0
+
     def flux(self, name, n_acc):
         """Net +x Poynting flux through plane `name` (flux.py:45-57)."""
         q = list(self.planes).index(name)

@@ -136,33 +136,52 @@ def _blend(eps, frac, n):
 class Stack:
     """Planar layer stack: a core of index wg_n and thickness t_wg_um on top of
     `layers` (from the core downward: (thickness_um, n), n complex = absorbing)
-    on a substrate n_sub, air above (common/layer_stack.py)."""
-    wg_n: float
+    on a substrate n_sub, air above (common/layer_stack.py).
+
+    n_sub may be a float or a depth profile with ``at_depth(d_um)`` (the layered
+    cornea).  thick_m, when given, are the layer thicknesses in metres used by
+    2D grids (the reference's legacy tear-film path computes them that way);
+    k_sub / force_lossy carry the legacy per-layer absorption switch."""
+    wg_n: complex
     t_wg_um: float
     layers: List[Tuple[float, complex]]
     n_sub: float
+    thick_m: Optional[List[float]] = None
+    k_sub: float = 0.0
+    force_lossy: bool = False
 
     @property
     def lossy(self):
-        return any(complex(n).imag > 0 for _, n in self.layers)
+        return self.force_lossy or any(complex(n).imag > 0 for _, n in self.layers)
 
     def eps_of_y(self, unit, core=True, n_core=None):
         """eps(y) in the given length unit (1.0 = metres, 1e-6 = micrometres)."""
         lossy = self.lossy
         bounds, yt = [], 0.0
-        for t, n in self.layers:
-            yb = yt - float(t) * (1e-6 / unit)
+        for q, (t, n) in enumerate(self.layers):
+            if unit == 1.0 and self.thick_m is not None:
+                yb = yt - self.thick_m[q]
+            else:
+                yb = yt - float(t) * (1e-6 / unit)
             nc = complex(n)
             bounds.append((yt, yb, nc if lossy else nc.real))
             yt = yb
         y_sub = yt
         top = self.t_wg_um * (1e-6 / unit)
-        wg = (complex(self.wg_n, 0.0) if lossy else self.wg_n) if n_core is None else n_core
+        wn = complex(self.wg_n) if lossy else complex(self.wg_n).real
+        wg = wn if n_core is None else n_core
         dt = np.complex128 if lossy else np.float64
+        sub, ks = self.n_sub, self.k_sub
+        depth_scale = 1e6 if unit == 1.0 else 1.0
 
         def f(y):
             e = np.full(y.shape, N_AIR ** 2, dtype=dt)
-            e[y < y_sub] = (float(self.n_sub) + 0j) ** 2 if lossy else self.n_sub ** 2
+            mc = y < y_sub
+            if hasattr(sub, 'at_depth'):
+                nd = sub.at_depth((y_sub - y[mc]) * depth_scale)
+                e[mc] = (nd + 1j * ks) ** 2 if lossy else nd ** 2
+            else:
+                e[mc] = (float(sub) + 1j * ks) ** 2 if lossy else sub ** 2
             for a, b, n in bounds:
                 e[(y >= b) & (y < a)] = n ** 2
             if core:
@@ -208,7 +227,7 @@ def air_path_um(distance_um, dx_um):
 class Bead2D:
     x_um: float
     d_um: float
-    n: float = 1.59
+    n: complex = 1.59
     y_um: Optional[float] = None      # centre; default -r (touching the core)
 
 
@@ -226,6 +245,11 @@ class Spec2D:
     lam_nm: float = 850.0
     waist_um: float = 3.0
     ramp_periods: Optional[float] = None
+    length_m: Optional[float] = None     # end of the core (default: the whole grid)
+    vcsel_distance_um: float = 0.0       # beam waist in front of the entry facet
+    vcsel_offset_um: float = 0.0
+    vcsel_tilt_deg: float = 0.0
+    src_core_only: bool = False
 
     @property
     def dt(self):
@@ -244,7 +268,7 @@ def build_2d(sp: Spec2D):
     """Coefficients, CPML profiles and source of a 2D solve (reference shapes)."""
     Nx, Ny, dx, dt = sp.nx, sp.ny, sp.dx, sp.dt
     lam_m = sp.lam_nm * 1e-9
-    air = air_path_um(0.0, dx * 1e6)
+    air = air_path_um(sp.vcsel_distance_um, dx * 1e6)
     x_facet_um = sp.src_ix * dx * 1e6 + air
     st = sp.stack
     lossy = st.lossy
@@ -252,7 +276,7 @@ def build_2d(sp: Spec2D):
     col = column_average(ys, dx, st.eps_of_y(1.0, core=False))
     col_core = column_average(ys, dx, st.eps_of_y(1.0, core=True))
     xs = np.arange(Nx) * dx
-    in_wg = (xs >= x_facet_um * 1e-6) & (xs <= Nx * dx * 1e6 * 1e-6)
+    in_wg = (xs >= x_facet_um * 1e-6) & (xs <= (sp.length_m if sp.length_m is not None else Nx * dx * 1e6 * 1e-6))
     eps = np.empty((Nx, Ny), dtype=np.complex128 if lossy else F32)
     eps[:, :] = col[None, :]
     eps[in_wg, :] = col_core[None, :]
@@ -267,9 +291,9 @@ def build_2d(sp: Spec2D):
             j0, j1 = max(0, int((yc - r - ys[0]) / dx) - 2), min(Ny, int((yc + r - ys[0]) / dx) + 3)
             if i1 > i0 and j1 > j0:
                 bead_patch = dict(bg=eps[i0:i1, j0:j1].real.astype(np.float64), i0=i0, j0=j0,
-                                  xs=xs[i0:i1], ys=ys[j0:j1], xc=xc, yc=yc, r=r, n=sp.bead.n)
+                                  xs=xs[i0:i1], ys=ys[j0:j1], xc=xc, yc=yc, r=r, n=complex(sp.bead.n).real)
                 _blend(eps[i0:i1, j0:j1], circle_fraction(xs[i0:i1], ys[j0:j1], xc, yc, r, dx),
-                       complex(sp.bead.n, 0.0) if lossy else sp.bead.n)
+                       complex(sp.bead.n) if lossy else complex(sp.bead.n).real)
     if lossy:
         sig = (2 * np.pi * C0 / lam_m * EPS0 * eps.imag).astype(F32)
         eps = eps.real.astype(F32)
@@ -282,17 +306,23 @@ def build_2d(sp: Spec2D):
     out['ce_h'] = (dt / (EPS0 * eps * dx) / cd).astype(F32)
     if tm:
         out.update(_tm_coefficients(sp, eps, sig, ys, in_wg, bead_patch))
-    # source: Gaussian line source on the Ez nodes (TM: averaged onto Ey)
-    yc_src = st.t_wg_um * 1e-6 / 2
-    y_um = (-sp.tear_m + np.arange(Ny) * dx) * 1e6 - yc_src * 1e6
-    w, R = beam(0.0 - air, sp.waist_um, sp.lam_nm, 1.0)
+    # source: Gaussian line source on the Ez nodes (TM: averaged onto Ey), in air
+    # in front of the entry facet (fdtd2d_core.py:378-397)
+    yc_src = st.t_wg_um * 1e-6 / 2 + sp.vcsel_offset_um * 1e-6
+    y_abs = (-sp.tear_m + np.arange(Ny) * dx) * 1e6
+    y_um = y_abs - yc_src * 1e6
+    w, R = beam(float(sp.vcsel_distance_um or 0.0) - air, sp.waist_um, sp.lam_nm, 1.0)
     amp = math.sqrt(sp.waist_um / w) * np.exp(-(y_um / w) ** 2)
-    kdx = huygens_kdx(sp.lam_nm, dx, C0 * dt, 1.0, 0.0)
-    a, p1, p2 = huygens_arrays(amp, _beam_phase(y_um, R, sp.lam_nm, 1.0, 0.0), kdx)
+    if sp.src_core_only:
+        from .physics import core_source_mask
+        amp = amp * core_source_mask(y_abs, st.t_wg_um)
+    kdx = huygens_kdx(sp.lam_nm, dx, C0 * dt, 1.0, sp.vcsel_tilt_deg)
+    a, p1, p2 = huygens_arrays(amp, _beam_phase(y_um, R, sp.lam_nm, 1.0, sp.vcsel_tilt_deg), kdx)
     if tm:
         h = F32(0.5)
         a, p1, p2 = h * (a[:-1] + a[1:]), h * (p1[:-1] + p1[1:]), h * (p2[:-1] + p2[1:])
-    out['src'] = dict(ix=sp.src_ix, amp=a, ph1=p1, ph2=p2, omega=2 * np.pi * sp.f0)
+    out['src'] = dict(ix=sp.src_ix, amp=a, ph1=p1, ph2=p2, omega=2 * np.pi * sp.f0, air_um=air,
+                      iy_src=int(round((yc_src + sp.tear_m) / dx)))
     out['cx'] = cpml_axis(Nx, sp.npml, sp.npml, dx, dt, lam_m)
     out['cy'] = cpml_axis(Ny, sp.npml, sp.npml, dx, dt, lam_m)
     return out

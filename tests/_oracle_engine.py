@@ -1,0 +1,105 @@
+"""Stand-in for lens_sensor_b200.engine built on the CPU oracle (TEST INFRASTRUCTURE).
+
+Implements the slice of the engine's 2D interface that the drop-in driver
+lens_sensor_b200.fdtd2d_core.run_beads calls (Grid2D, Epi2D, StepTable,
+cw_envelope), stepping with oracle.fdtd_oracle.Grid2D in FP32 and accumulating
+the epilogue exactly as the reference's loop does (fdtd2d_core.py:781-870).
+Tests patch it in to check the driver's schedule (step count, detector
+windows, DFT windows, CW convergence extension, snapshots, result keys) on the
+CPU against the reference's own known answers.  It is never used by the
+product.
+"""
+import numpy as np
+import torch
+
+from oracle import fdtd_oracle as O
+
+F32 = np.float32
+
+
+def cw_envelope(f0, ramp_periods=None):
+    return lambda t: O.cw_envelope(float(t), f0, ramp_periods)
+
+
+class StepTable:
+    def __init__(self, t0, n, dt, omega_src, omega_dft, envelope, device=None):
+        self.dt, self.envelope, self.omega = dt, envelope, omega_dft
+
+
+class Grid2D:
+    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None):
+        self.pol = 'p' if str(pol).lower() in ('p', 'tm') else 's'
+        self.nx, self.ny, self.dx, self.dt = nx, ny, dx, dt
+        h = O.Huygens.__new__(O.Huygens)
+        h.ix, h.omega = int(src['ix']), float(src['omega'])
+        h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
+        self.g = O.Grid2D(self.pol, nx, ny, dx, dt, cx, cy, h, coef, F32, pec)
+
+    def view(self, name):
+        return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
+
+    def step(self, table, n0, nsteps, epi=None, stream=None):
+        for n in range(n0, n0 + nsteps):
+            t = n * self.dt
+            self.g.step(n, float(table.envelope(t)))
+            if epi is not None:
+                epi.after(n, t, self.g)
+
+
+class Epi2D:
+    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=()):
+        nx, ny = grid.nx, grid.ny
+        self.grid = grid
+        self.boxes = [tuple(b) for b in boxes]
+        self.box = np.zeros(len(self.boxes), np.float64)
+        self.win, self.win_prev = tuple(dft), tuple(prev) if prev is not None else (0, 0)
+        self.acc = np.zeros((nx, ny), np.complex64)
+        self.acc_ex = np.zeros((nx, ny), np.complex64) if dft_ex else None
+        self.acc_prev = np.zeros((nx, ny), np.complex64)
+        self.iavg_n0 = iavg_n0
+        self.acc_I = np.zeros((nx, ny), F32)
+        self.planes = dict(planes)
+        self.flux_acc = None
+        self._omega = None
+
+    def after(self, n, t, g):
+        if self.flux_acc is None:
+            self._omega = float(g.src.omega)
+            self.flux_acc = O.PlaneFlux(self._omega, g.dt, F32)
+        field = g.field()
+        I_E = g.intensity(field)
+        for q, (x0, x1, y0, y1) in enumerate(self.boxes):
+            self.box[q] += np.sum(I_E[x0:x1, y0:y1], dtype=np.float64)
+        if self.win[0] <= n < self.win[1]:
+            ph = np.exp(-1j * self._omega * t)
+            self.acc += field.astype(np.complex64) * ph
+            if self.acc_ex is not None:
+                self.acc_ex += g.ex_node().astype(np.complex64) * ph
+            for k, il in self.planes.items():
+                self.flux_acc.add(k, t, g.flux_pairs(il))
+        elif self.win_prev[0] <= n < self.win_prev[1]:
+            self.acc_prev += field.astype(np.complex64) * np.exp(-1j * self._omega * t)
+        if self.iavg_n0 is not None and n >= self.iavg_n0:
+            self.acc_I += I_E
+
+    @property
+    def box_acc(self):
+        return torch.from_numpy(self.box.copy())
+
+    @property
+    def iavg(self):
+        return torch.from_numpy(self.acc_I.copy())
+
+    def phasor(self, which='dft'):
+        a = dict(dft=self.acc, prev=self.acc_prev, dft_ex=self.acc_ex)[which]
+        return torch.from_numpy(a.astype(np.complex128))
+
+    def restart_dft(self, window):
+        self.acc_prev, self.acc = self.acc, np.zeros_like(self.acc)
+        if self.acc_ex is not None:
+            self.acc_ex[...] = 0
+        self.flux_acc = O.PlaneFlux(self._omega, self.grid.dt, F32)
+        self.win, self.win_prev = tuple(window), (0, 0)
+
+    def flux(self, name, n_acc):
+        return self.flux_acc.flux(name)

@@ -15,6 +15,10 @@ Outputs:
   g2d_te.npz, g2d_tm.npz, g3d_tm.npz   setup arrays + fields/phasors after N steps
   characterization.json                run_beads / run_3d / run_3d_stitched known
                                        answers at the reference HEAD
+  dropin_2d.json                       run_beads + save_results outputs (NPZ / PKL
+                                       summaries) of three whole-driver cases
+
+`python tests/golden/make_golden.py dropin` stops after the two JSON files.
 """
 import json
 import os
@@ -248,11 +252,83 @@ def characterization():
     return dict(case_3d=r3, case_2d=r2)
 
 
+# ------------------------------------------------------------- drop-in run_beads
+# Whole-driver cases: fdtd2d_core.run_beads + save_results (method='full', CPML, CW).
+# 'te' is the reference's characterization case; 'tm_kappa' adds KAPPA losses on the
+# legacy aqueous layer and the core (TM loss split, Ex phasor); 'tm_stack' runs a
+# custom absorbing layer stack (auto tear buffer, stack keys in the output).
+DROPIN_2D = dict(
+    te=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.5, dx_nm=100.0,
+                    save_frames=True, n_snapshots=2, wg_thickness_um=1.0, lambda_nm=850.0,
+                    method='full', length_um=8.0, bead_x_um=4.0), kappa={}),
+    tm_kappa=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.6, dx_nm=80.0,
+                          save_frames=True, n_snapshots=3, wg_thickness_um=1.2, lambda_nm=850.0,
+                          method='full', length_um=7.0, bead_x_um=3.6, polarization='p',
+                          t_aqueous_um=1.5, t_lipid_um=0.1), kappa=dict(aq=0.002, wg=0.0005)),
+    tm_stack=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.5, dx_nm=100.0,
+                          save_frames=True, n_snapshots=2, wg_thickness_um=1.0, lambda_nm=850.0,
+                          method='full', length_um=8.0, bead_x_um=4.0, polarization='p',
+                          stack=[dict(name='Aqueous', t_um=6.0, n=complex(1.333, 0.001), kappa=0.001,
+                                      mat=None),
+                                 dict(name='Mucin', t_um=3.5, n=complex(1.342, 0.0), kappa=0.0,
+                                      mat=None)]), kappa={}),
+)
+
+
+def _summ(v):
+    """JSON summary of one NPZ / PKL value: strings verbatim, arrays reduced."""
+    a = np.asarray(v)
+    if a.dtype.kind in 'USO':
+        return dict(kind='str', value=[str(x) for x in a.ravel()])
+    d = dict(kind='num', dtype=str(a.dtype), shape=list(a.shape))
+    if a.size:
+        c = a.astype(np.complex128)
+        d.update(sum=[float(c.real.sum()), float(c.imag.sum())], abssum=float(np.abs(c).sum()),
+                 absmax=float(np.abs(c).max()))
+    return d
+
+
+def dropin_2d():
+    """Run the reference driver end to end for DROPIN_2D and summarise its outputs."""
+    import glob
+    import pickle
+    out = {}
+    for name, c in DROPIN_2D.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_dropin_')
+        old_k = d2.KAPPA
+        try:
+            os.chdir(tmp)
+            d2.KAPPA = dict(c['kappa'])
+            r = d2.run_beads(**c['kw'])
+            d2.save_results(r)
+            z = np.load(glob.glob('results/*_frames.npz')[0])
+            npz = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+        finally:
+            d2.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        out[name] = dict(kw={k: v for k, v in c['kw'].items() if k != 'stack'}, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         npz=npz, pkl=scal)
+    return out
+
+
 def main():
     ch = characterization()          # first: the cases below change module globals
     with open(os.path.join(OUT, 'characterization.json'), 'w') as f:
         json.dump(ch, f, indent=1)
     print('wrote characterization.json')
+    with open(os.path.join(OUT, 'dropin_2d.json'), 'w') as f:
+        json.dump(dropin_2d(), f, indent=1)
+    print('wrote dropin_2d.json')
+    if 'dropin' in sys.argv[1:]:
+        return
     for name, c in CASE_2D.items():
         o = run_2d(c)
         o = {k: (np.asarray(v) if not isinstance(v, (int, float)) else np.asarray(v)) for k, v in o.items()}

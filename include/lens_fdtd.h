@@ -167,7 +167,7 @@ typedef struct {
     int box[LENS_MAX_BOX][6];    /* [x0,x1) [y0,y1) [z0,z1), applied to Ex, Ey, Ez */
     double *box_acc;             /* nbox sums of Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481) */
     int dft_n0, dft_n1;
-    float *dft[3];               /* per component (or NULL): (nx,ny,pitch) x {re,im,c_re,c_im} */
+    float *dft[3];               /* per component (or NULL): (nx,ny,pitch) x {re,im} */
     int conv_k;                  /* z index of the convergence plane (driven component) */
     int prev_n0, prev_n1;        /* previous window for the convergence test */
     float *conv_prev, *conv_last;/* (nx, nj) x {re,im,c_re,c_im} planes or NULL */

@@ -20,6 +20,8 @@
 //  * h3d + e3d (in place, no buffer 1): two streaming passes.
 #include <cuda.h>
 
+#include <cmath>
+
 #include "lens_common.cuh"
 
 namespace {
@@ -203,14 +205,15 @@ __device__ __forceinline__ void plane3(const LensEpi3D &ep, const LensStepTable 
 
 // Epilogue of one cell after its E update.  All 32 lanes of a warp must call it.
 //   detector boxes: sum of Ex^2+Ey^2+Ez^2 in FP64 (fdtd3d_core.py:477-481)
-//   DFT windows:    compensated float32 (Kahan) complex sums of each selected component
+//   DFT windows:    complex float32 sums of each selected component (the
+//                   reference's complex64 accumulator, fdtd3d_core.py:1150-1158)
 //   flux planes:    FP64 DFT of E and of the x-averaged H (flux.py:28-41)
 __device__ __forceinline__ void epi_cell(const K3 &g, const LensStepTable &tab, const LensEpi3D &ep,
                                          int n, int i, int j, int k, bool in, Hv e, float hym,
-                                         float hzm, Hv h, bool vol_dft = true) {
+                                         float hzm, Hv h, bool vol_dft = true, bool boxes = true) {
     const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
     const bool vx = in && i < nx - 1, vy = in && j < ny - 1, vz = in && k < nz - 1;
-    if (ep.nbox > 0) {
+    if (boxes && ep.nbox > 0) {
         const int bk0 = blockIdx.x * BK, bj0 = blockIdx.y * BJ;
         for (int b = 0; b < ep.nbox; ++b) {
             const int *bx = ep.box[b];
@@ -239,9 +242,18 @@ __device__ __forceinline__ void epi_cell(const K3 &g, const LensStepTable &tab, 
         kahan_add(reinterpret_cast<float4 *>(ep.conv_prev) + (size_t)i * g.src.nj + j, f * pr, f * pim);
     if (!win) return;
     if (vol_dft) {
-        if (ep.dft[0] && vx) kahan_add(reinterpret_cast<float4 *>(ep.dft[0]) + o, e.x * pr, e.x * pim);
-        if (ep.dft[1] && vy) kahan_add(reinterpret_cast<float4 *>(ep.dft[1]) + o, e.y * pr, e.y * pim);
-        if (ep.dft[2] && vz) kahan_add(reinterpret_cast<float4 *>(ep.dft[2]) + o, e.z * pr, e.z * pim);
+        const float v[3] = {e.x, e.y, e.z};
+        const bool ok[3] = {vx, vy, vz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (ep.dft[c] && ok[c]) {
+                float2 *a = reinterpret_cast<float2 *>(ep.dft[c]) + o;
+                float2 s = *a;
+                s.x += v[c] * pr;
+                s.y += v[c] * pim;
+                *a = s;
+            }
+        }
     }
     if (ep.conv_last && vf && k == ep.conv_k)
         kahan_add(reinterpret_cast<float4 *>(ep.conv_last) + (size_t)i * g.src.nj + j, f * pr, f * pim);
@@ -354,38 +366,41 @@ __global__ void __launch_bounds__(NT)
 }
 
 // ============================================================ fused TMA pass
-// CTA = 10 warps: warps 0..7 own the tile rows j0..j0+7 (H and E), warp 8
-// computes H on the halo row j0-1, warp 9 (lanes 0..7) H on the halo column
-// k0-1, and lane 31 of warp 9 issues the TMA copies.  Every (j, k) dependent
-// quantity (validity, strip slot, CPML profile values, source profile) is
-// computed once per thread; i dependent ones once per plane.
-constexpr int FW = BJ + 2;
-constexpr int EK = BK + 8, EJ = BJ + 2;    // E box:   z k0-4..k0+35, y j0-1..j0+8
-constexpr int HK = BK + 4, HJ = BJ + 1;    // H box:   z k0-4..k0+31, y j0-1..j0+7
-constexpr int SHK = BK + 1, SHJ = BJ + 1;  // new H:   z k0-1..k0+31, y j0-1..j0+7
-constexpr int NSE = 4, NSH = 3, NSC = 3;   // ring depths (x-planes)
-constexpr int E_BYTES = EK * EJ * 4, E_SLOT = 1664;
-constexpr int H_BYTES = HK * HJ * 4, H_SLOT = 1408;
-constexpr int C_BYTES = BK * BJ * 4;
+// A CTA owns a tile of TJ = 14 rows (y) x TK = 32 lanes (z) and streams an
+// x-chunk.  Warps 0..6 own rows 2w and 2w+1 (H and E); warp 7 computes H on
+// the halo row j0-1 (all lanes) and the halo column k0-1 (lanes 0..13), and its
+// lane 0 drives the E ring.  Per x-plane, TMA stages E with a one-cell halo
+// (rows j0-1..j0+14, z k0-4..k0+35) into a 4-deep mbarrier ring and the old H
+// and coefficient tiles of the owner cells into a 3-deep ring; the halo cells'
+// old H and (in CPML tiles) psi are read with coalesced loads issued one phase
+// ahead.  One CTA barrier per plane publishes the new H tile (shared memory)
+// for the E update.  Reads buffer `cur`, writes the
+// other: 72 B per cell update (lossy), 60 B lossless, plus psi in the strips.
+constexpr int TJ = 14, TK = 32;             // 7 owner warps + 1 halo warp = 8 warps
+constexpr int NOW = TJ / 2;                  // owner warps (2 rows each)
+constexpr int NW3 = NOW + 1;                 // + halo warp
+constexpr int EK = TK + 8, EJ = TJ + 2;      // E box
+constexpr int E_BYTES = EK * EJ * 4;
+constexpr int E_SLOT = ((E_BYTES + 127) / 128) * 128;
+constexpr int NSE = 4;                       // E ring depth (x-planes)
+constexpr int SHK = TK + 1, SHJ = TJ + 1;    // new H tile: z k0-1..k0+31, y j0-1..j0+TJ-1
 constexpr int SH_N = SHK * SHJ;
-constexpr int OFF_H = NSE * 3 * E_SLOT;
-constexpr int OFF_C = OFF_H + NSH * 3 * H_SLOT;
-constexpr int OFF_SH = OFF_C + NSC * 6 * C_BYTES;
-constexpr int OFF_BAR = OFF_SH + ((2 * 3 * SH_N * 4 + 127) / 128) * 128;
-constexpr int SMEM_LEAN = OFF_BAR + (NSE + NSH + NSC) * 8;
-// strip CTAs also stage psi: 6 H-psi tiles per H stage, 6 E-psi tiles per C stage
-constexpr int OFF_HP = ((SMEM_LEAN + 127) / 128) * 128;
-constexpr int OFF_EP = OFF_HP + NSH * 6 * H_SLOT;
-constexpr int SMEM_STRIP = OFF_EP + NSC * 6 * C_BYTES;
-static_assert(E_SLOT % 128 == 0 && E_SLOT >= E_BYTES, "E slot");
-static_assert(H_SLOT % 128 == 0 && H_SLOT >= H_BYTES, "H slot");
-static_assert(OFF_H % 128 == 0 && OFF_C % 128 == 0 && OFF_SH % 128 == 0, "alignment");
+constexpr int EF = E_SLOT / 4;
+constexpr int HT = TK * TJ;                  // floats of one owner tile (z k0..k0+31, y j0..j0+TJ-1)
+constexpr int NHC = 3;                       // H + coefficient ring depth (x-planes)
+constexpr int HC_SLOT = 9 * HT * 4;          // Hx, Hy, Hz, ce_x, ce_y, ce_z, D_x, D_y, D_z
+constexpr int OFF_HC = NSE * 3 * E_SLOT;
+constexpr int OFF_SH = OFF_HC + NHC * HC_SLOT;
+constexpr int OFF_PT = OFF_SH + ((2 * 3 * SH_N * 4 + 127) / 128) * 128;
+constexpr int OFF_BAR = OFF_PT + (((6 * (TK + 1 + TJ + 1)) * 4 + 127) / 128) * 128;
+constexpr int SMEM3 = OFF_BAR + (NSE + NHC) * 8;
+static_assert(OFF_HC % 128 == 0 && HC_SLOT % 128 == 0 && (HT * 4) % 128 == 0, "TMA alignment");
+static_assert(OFF_SH % 128 == 0 && OFF_BAR % 8 == 0, "alignment");
 
-struct TMaps {
-    CUtensorMap e[3];  // E of the read buffer, box EK x EJ x 1
-    CUtensorMap h[3];  // H of the read buffer, box HK x HJ x 1
-    CUtensorMap c[6];  // ce_x, ce_y, ce_z, D_x, D_y, D_z, box BK x BJ x 1
-    CUtensorMap p[12]; // psi of the read buffer (LENS_PSI_* order): H-psi box HK x HJ, E-psi BK x BJ
+struct EMaps {
+    CUtensorMap e[3];  // Ex, Ey, Ez of the read buffer, box EK x EJ x 1
+    CUtensorMap h[3];  // Hx, Hy, Hz of the read buffer, box TK x TJ x 1
+    CUtensorMap c[6];  // ce_x, ce_y, ce_z, D_x, D_y, D_z, box TK x TJ x 1
 };
 
 __device__ __forceinline__ uint32_t s_addr(const void *p) {
@@ -426,358 +441,626 @@ __device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap *m, int c0,
         : "memory");
 }
 
-// CPML values of one coordinate: inside a psi strip?  and b, c, 1/kappa - 1.
-struct PV {
-    int s;
-    float b, c, km;
-};
-
-__device__ __forceinline__ PV pv_at(const LensProfile &p, int m) {
-    PV r{-1, 1.f, 0.f, 0.f};
-    if (m >= 0 && m < p.n) {
-        r.s = strip_of(m, p.lo, p.hi, p.n);
-        if (r.s >= 0) {
-            r.b = p.b[m];
-            r.c = p.c[m];
-            r.km = p.ik[m] - 1.0f;
-        }
-    }
-    return r;
-}
-
-// psi update: stores the new psi (owner only) and returns psi + (1/kappa - 1)*d.
-__device__ __forceinline__ float psi_u(float old, const PV &v, float d, float *pw, size_t idx, bool wr) {
-    const float p = v.b * old + v.c * d;
-    if (wr) pw[idx] = p;
-    return p + v.km * d;
-}
-
 // does [a, b] meet a psi strip of profile p?
-__device__ __forceinline__ bool meets(int a, int b, const LensProfile &p) {
+__host__ __device__ __forceinline__ bool meets(int a, int b, const LensProfile &p) {
     return (p.lo > 0 && a < p.lo) || (p.hi > 0 && b >= p.n - p.hi);
 }
 
-constexpr int MAXCH = 96;
-// x-decomposition: chunk c covers planes [x[c], x[c+1]); strip[c] != 0 when a
-// plane of the chunk (or the plane before it) lies in an x CPML strip.
-struct Chunks {
-    int n;
-    int x[MAXCH + 1];
-    int strip[MAXCH];
+__host__ __device__ __forceinline__ bool in_strip(const LensProfile &p, int m) {
+    return m >= 0 && m < p.n && (m < p.lo || m >= p.n - p.hi);
+}
+
+// psi = b*psi_old + c*d (stored when wr); returns psi + km*d, km = 1/kappa - 1.
+template <typename IX>
+__device__ __forceinline__ float psi_u(float b, float c, float km, float old, float d, float *pw, IX idx,
+                                       bool wr) {
+    const float v = b * old + c * d;
+    if (wr) pw[idx] = v;
+    return v + km * d;
+}
+
+// CPML profile tables of a CPML tile in shared memory: rows (b, c, 1/kappa-1) of
+// the half-node (H) then the integer-node (E) profile, for z = k0-1 .. k0+TK-1
+// (ZN entries) and y = j0-1 .. j0+TJ-1 (YN entries); zero outside the profile.
+constexpr int ZN = TK + 1, YN = TJ + 1;
+
+__device__ __forceinline__ void fill_row(float *t, int stride, const LensProfile &p, int m) {
+    const bool in = m >= 0 && m < p.n;
+    t[0] = in ? __ldg(p.b + m) : 0.f;
+    t[stride] = in ? __ldg(p.c + m) : 0.f;
+    t[2 * stride] = in ? __ldg(p.ik + m) - 1.0f : 0.f;
+}
+
+// Values of one x-plane (uniform): H profile at i (half node), E profile at i.
+struct PX {
+    float hb, hc, hk, eb, ec, ek;
 };
 
-// Ring slot (stage) and phase parity of the u-th use, tracked incrementally.
-struct Ring {
-    int s, ph;
-    int n;
-    __device__ __forceinline__ void next() {
-        if (++s == n) {
-            s = 0;
-            ph ^= 1;
+__device__ __forceinline__ PX px_at(const K3 &g, int i) {
+    PX v{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (in_strip(g.ax.h, i)) {
+        v.hb = __ldg(g.ax.h.b + i); v.hc = __ldg(g.ax.h.c + i); v.hk = __ldg(g.ax.h.ik + i) - 1.0f;
+    }
+    if (in_strip(g.ax.e, i)) {
+        v.eb = __ldg(g.ax.e.b + i); v.ec = __ldg(g.ax.e.c + i); v.ek = __ldg(g.ax.e.ik + i) - 1.0f;
+    }
+    return v;
+}
+
+constexpr int MAXCH = 96;
+// Work of one step: every (z-tile, y-tile, x-chunk).  The CPML tiles (outside
+// the lean core [lo, hi): CPML-free, interior) come first, the longer CTAs
+// starting early; within each group the order is chunk, y-tile, z-tile (z
+// fastest), so that CTAs sharing E halo lines run together.
+struct Work {
+    int ntz, nty, nc;
+    int lo[3], hi[3];  // lean core: z-tiles, y-tiles, chunks
+    int x[MAXCH + 1];  // chunk c covers planes [x[c], x[c+1])
+};
+
+// Tile of CTA `id` (see Work); returns true for a lean tile.
+__host__ __device__ __forceinline__ bool work_tile(const Work &wk, int id, int &tz, int &ty, int &c) {
+    const int ntz = wk.ntz, nty = wk.nty;
+    const int nlz = wk.hi[0] - wk.lo[0], nly = wk.hi[1] - wk.lo[1], nlc = wk.hi[2] - wk.lo[2];
+    const int full = nty * ntz;                  // CPML tiles of a CPML chunk
+    const int part = full - nly * nlz;           // CPML tiles of a lean chunk
+    const int nstrip = (wk.nc - nlc) * full + nlc * part;
+    if (id >= nstrip) {  // lean core, z fastest
+        int q = id - nstrip;
+        tz = wk.lo[0] + q % nlz;
+        q /= nlz;
+        ty = wk.lo[1] + q % nly;
+        c = wk.lo[2] + q / nly;
+        return true;
+    }
+    const int before = wk.lo[2] * full;          // CPML tiles of the chunks before the lean ones
+    int rem;
+    if (id < before) {
+        c = id / full;
+        rem = id % full;
+    } else if (id < before + nlc * part) {
+        c = wk.lo[2] + (id - before) / part;
+        rem = (id - before) % part;
+        // rows before the lean rows are whole, the lean rows lack their lean z-tiles
+        const int r0 = wk.lo[1] * ntz, rp = nly * (ntz - nlz);
+        if (rem >= r0 && rem < r0 + rp) {
+            const int q = rem - r0, w = ntz - nlz;
+            ty = wk.lo[1] + q / w;
+            const int t = q % w;
+            tz = t < wk.lo[0] ? t : t + nlz;
+            return false;
+        }
+        if (rem >= r0 + rp) rem -= rp - nly * ntz;  // map to whole-row numbering
+    } else {
+        const int q = id - before - nlc * part;
+        c = wk.hi[2] + q / full;
+        rem = q % full;
+    }
+    ty = rem / ntz;
+    tz = rem % ntz;
+    return false;
+}
+
+// Per-cell flags of an owner row.
+enum : unsigned {
+    F_IN = 1u, F_HX = 2u, F_HY = 4u, F_HZ = 8u,     // in the domain; H components that update
+    F_EXU = 16u, F_EYU = 32u, F_EZU = 64u,          // E components whose curl term applies (j,k part)
+    F_EYV = 128u, F_EZV = 256u,                     // Ey, Ez exist (j < ny-1, k < nz-1)
+    F_PJ = 512u, F_PK = 1024u,                      // on a PEC face in y / z
+    F_ZH = 2048u, F_YH = 4096u, F_ZE = 8192u, F_YE = 16384u,  // in a z / y psi strip (H / E)
+    F_BOX0 = 1u << 16                               // bit 16 + b: inside detector box b (y, z)
+};
+
+__device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep, int j, int k) {
+    const int ny = g.ny, nz = g.nz;
+    unsigned f = 0;
+    if (j < 0 || k < 0 || j >= ny || k >= nz) return 0;
+    f |= F_IN;
+    if (j < ny - 1 && k < nz - 1) f |= F_HX;
+    if (k < nz - 1) f |= F_HY | F_EZV;
+    if (j < ny - 1) f |= F_HZ | F_EYV;
+    const bool jin = j >= 1 && j <= ny - 2, kin = k >= 1 && k <= nz - 2;
+    if (jin && kin) f |= F_EXU;
+    if (kin && j < ny - 1) f |= F_EYU;
+    if (jin && k < nz - 1) f |= F_EZU;
+    if ((g.pec[2] && j == 0) || (g.pec[3] && j == ny - 1)) f |= F_PJ;
+    if ((g.pec[4] && k == 0) || (g.pec[5] && k == nz - 1)) f |= F_PK;
+    if (in_strip(g.az.h, k)) f |= F_ZH;
+    if (in_strip(g.ay.h, j)) f |= F_YH;
+    if (in_strip(g.az.e, k)) f |= F_ZE;
+    if (in_strip(g.ay.e, j)) f |= F_YE;
+    for (int b = 0; b < LENS_MAX_BOX; ++b)
+        if (b < ep.nbox && j >= ep.box[b][2] && j < ep.box[b][3] && k >= ep.box[b][4] && k < ep.box[b][5])
+            f |= F_BOX0 << b;
+    return f;
+}
+
+// H-psi values of one cell: hx_z, hx_y, hy_x, hy_z, hz_y, hz_x (LENS_PSI_* 0..5)
+struct P6 {
+    float v[6];
+};
+
+template <typename IX>
+__device__ __forceinline__ void load_hpsi(P6 &p, const K3 &g, IX o, unsigned f, bool xh) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) p.v[q] = 0.f;
+    if (f & F_ZH) {
+        p.v[0] = __ldg(g.pr[LENS_PSI_HX_Z] + o);
+        p.v[3] = __ldg(g.pr[LENS_PSI_HY_Z] + o);
+    }
+    if (f & F_YH) {
+        p.v[1] = __ldg(g.pr[LENS_PSI_HX_Y] + o);
+        p.v[4] = __ldg(g.pr[LENS_PSI_HZ_Y] + o);
+    }
+    if (xh) {
+        p.v[2] = __ldg(g.pr[LENS_PSI_HY_X] + o);
+        p.v[5] = __ldg(g.pr[LENS_PSI_HZ_X] + o);
+    }
+}
+
+// E-psi values of one cell: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y (LENS_PSI_* 6..11)
+template <typename IX>
+__device__ __forceinline__ void load_epsi(P6 &p, const K3 &g, IX o, unsigned f, bool xe) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) p.v[q] = 0.f;
+    if (f & F_YE) {
+        p.v[0] = __ldg(g.pr[LENS_PSI_EX_Y] + o);
+        p.v[5] = __ldg(g.pr[LENS_PSI_EZ_Y] + o);
+    }
+    if (f & F_ZE) {
+        p.v[1] = __ldg(g.pr[LENS_PSI_EX_Z] + o);
+        p.v[2] = __ldg(g.pr[LENS_PSI_EY_Z] + o);
+    }
+    if (xe) {
+        p.v[3] = __ldg(g.pr[LENS_PSI_EY_X] + o);
+        p.v[4] = __ldg(g.pr[LENS_PSI_EZ_X] + o);
+    }
+}
+
+struct F3 {
+    float x, y, z;
+};
+
+// New H of one cell from old H and E around it (boundaries3d.py:311-331):
+//   e = E(i,j,k); exk, eyk = E(i,j,k+1); exj, ezj = E(i,j+1,k); eyn, ezn = E(i+1,j,k).
+// iok: i < nx-1 (Hy, Hz exist).  ST: CPML tile (psi corrections in the strips).
+// zt / yt: the cell's entries of the z / y profile tables; x: this plane's x values.
+template <bool ST, typename IX>
+__device__ __forceinline__ F3 h_new(const K3 &g, F3 h, float ex, float ey, float ez, float exk, float eyk,
+                                    float exj, float ezj, float eyn, float ezn, unsigned f, bool iok,
+                                    const float *zt, const float *yt, const PX &x, const P6 &ps, IX o,
+                                    bool wr, bool xh) {
+    const float ch = g.ch;
+    const float d1x = eyk - ey, d2x = ezj - ez;
+    const float d1y = ezn - ez, d2y = exk - ex;
+    const float d1z = exj - ex, d2z = eyn - ey;
+    // !ST: a CPML-free interior tile (every component of every cell updates)
+    if (!ST || (f & F_HX)) {
+        float v = h.x + ch * (d1x - d2x);
+        if (ST) {
+            if (f & F_ZH) v = v + ch * psi_u(zt[0], zt[ZN], zt[2 * ZN], ps.v[0], d1x, g.pw[LENS_PSI_HX_Z], o, wr);
+            if (f & F_YH) v = v + (-ch) * psi_u(yt[0], yt[YN], yt[2 * YN], ps.v[1], d2x, g.pw[LENS_PSI_HX_Y], o, wr);
+        }
+        h.x = v;
+    }
+    if (!ST || (iok && (f & F_HY))) {
+        float v = h.y + ch * (d1y - d2y);
+        if (ST) {
+            if (xh) v = v + ch * psi_u(x.hb, x.hc, x.hk, ps.v[2], d1y, g.pw[LENS_PSI_HY_X], o, wr);
+            if (f & F_ZH) v = v + (-ch) * psi_u(zt[0], zt[ZN], zt[2 * ZN], ps.v[3], d2y, g.pw[LENS_PSI_HY_Z], o, wr);
+        }
+        h.y = v;
+    }
+    if (!ST || (iok && (f & F_HZ))) {
+        float v = h.z + ch * (d1z - d2z);
+        if (ST) {
+            if (f & F_YH) v = v + ch * psi_u(yt[0], yt[YN], yt[2 * YN], ps.v[4], d1z, g.pw[LENS_PSI_HZ_Y], o, wr);
+            if (xh) v = v + (-ch) * psi_u(x.hb, x.hc, x.hk, ps.v[5], d2z, g.pw[LENS_PSI_HZ_X], o, wr);
+        }
+        h.z = v;
+    }
+    return h;
+}
+
+// Coefficients of one cell: ce_x, ce_y, ce_z and (lossy) D_x, D_y, D_z.
+struct C6 {
+    float cx, cy, cz, dx, dy, dz;
+};
+
+template <typename IX>
+__device__ __forceinline__ void load_coef(C6 &c, const K3 &g, IX o, bool lossy) {
+    c.cx = __ldg(g.ce_x + o);
+    c.cy = __ldg(g.ce_y + o);
+    c.cz = __ldg(g.ce_z + o);
+    if (lossy) {
+        c.dx = __ldg(g.da_x + o);
+        c.dy = __ldg(g.da_y + o);
+        c.dz = __ldg(g.da_z + o);
+    } else {
+        c.dx = c.dy = c.dz = 1.f;
+    }
+}
+
+// Plane-uniform data of the E update.
+struct PlE {
+    bool iok, iin, pec_i, xe, src;
+    float sgn;  // +1 on plane src.ix, -1 on src.ix+1
+    float env, wt;
+};
+
+// New E of one cell (boundaries3d.py:333-362, fdtd3d_core.py:1116-1127):
+//   D*E, curl of the new H (h = H(i,j,k), hxk/hyk = H(i,j,k-1), hxj/hzj = H(i,j-1,k),
+//   hym/hzm = H(i-1,j,k)), psi in the strips, PEC on the absorbing faces, source.
+template <bool ST, typename IX>
+__device__ __forceinline__ F3 e_new(const K3 &g, F3 e, F3 h, float hxk, float hyk, float hxj, float hzj,
+                                    float hym, float hzm, const C6 &c, unsigned f, const PlE &pl, int j,
+                                    int k, const float *zt, const float *yt, const PX &x, const P6 &ps,
+                                    IX o) {
+    const float d1x = h.z - hzj, d2x = h.y - hyk;  // Ex
+    const float d1y = h.x - hxk, d2y = h.z - hzm;  // Ey
+    const float d1z = h.y - hym, d2z = h.x - hxj;  // Ez
+    float vx = e.x * c.dx, vy = e.y * c.dy, vz = e.z * c.dz;
+    // !ST: a CPML-free interior tile (all curl terms apply, no PEC, all components exist)
+    const bool ux = !ST || (pl.iok && (f & F_EXU)), uy = !ST || (pl.iin && (f & F_EYU)),
+               uz = !ST || (pl.iin && (f & F_EZU));
+    if (ux) vx = vx + c.cx * (d1x - d2x);
+    if (uy) vy = vy + c.cy * (d1y - d2y);
+    if (uz) vz = vz + c.cz * (d1z - d2z);
+    if (ST) {
+        if (ux) {
+            if (f & F_YE) vx = vx + c.cx * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[0], d1x, g.pw[LENS_PSI_EX_Y], o, true);
+            if (f & F_ZE) vx = vx + (-c.cx) * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[1], d2x, g.pw[LENS_PSI_EX_Z], o, true);
+        }
+        if (uy) {
+            if (f & F_ZE) vy = vy + c.cy * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[2], d1y, g.pw[LENS_PSI_EY_Z], o, true);
+            if (pl.xe) vy = vy + (-c.cy) * psi_u(x.eb, x.ec, x.ek, ps.v[3], d2y, g.pw[LENS_PSI_EY_X], o, true);
+        }
+        if (uz) {
+            if (pl.xe) vz = vz + c.cz * psi_u(x.eb, x.ec, x.ek, ps.v[4], d1z, g.pw[LENS_PSI_EZ_X], o, true);
+            if (f & F_YE) vz = vz + (-c.cz) * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[5], d2z, g.pw[LENS_PSI_EZ_Y], o, true);
         }
     }
-};
+    if (ST) {
+        if (!pl.iok || (f & (F_PJ | F_PK))) vx = 0.f;
+        if (!(f & F_EYV) || pl.pec_i || (f & F_PK)) vy = 0.f;
+        if (!(f & F_EZV) || pl.pec_i || (f & F_PJ)) vz = 0.f;
+    }
+    if (pl.src && j < g.src.nj && k < g.src.nk) {
+        const size_t m = (size_t)j * g.src.pitch_k + k;
+        const float *ph = pl.sgn > 0.f ? g.src.ph1 : g.src.ph2;
+        const float s = pl.sgn * ((pl.env * sinf(pl.wt + __ldg(ph + m))) * __ldg(g.src.amp + m));
+        if (g.src_comp == 0) vx += s;
+        else if (g.src_comp == 1) vy += s;
+        else vz += s;
+    }
+    return F3{vx, vy, vz};
+}
 
-// One launch per block category: ST = false runs only the blocks whose tile
-// and x-chunk meet no CPML strip (no psi at all), ST = true the others, whose
-// psi tiles are staged by TMA next to the field tiles.  Only the producer lane
-// waits on the mbarriers; the other warps sleep in the CTA barrier.
-template <bool ST, bool DF>
-__global__ void __launch_bounds__(FW * 32, ST ? 2 : 3)
-    fused3d(const __grid_constant__ TMaps tm, const K3 g, const LensStepTable tab,
-            const LensEpi3D ep, int n, int epi, const __grid_constant__ Chunks chs) {
+// IX: index type of the field volumes (32-bit when nx*ny*pitch < 2^31).
+template <bool ST, typename IX>
+__device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensStepTable &tab,
+                                       const LensEpi3D &ep, int n, int epi, int k0, int j0, int x0,
+                                       int x1, unsigned char *smem) {
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int k0 = blockIdx.x * BK, j0 = blockIdx.y * BJ;
-    const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
-    const int x0 = chs.x[blockIdx.z], x1 = chs.x[blockIdx.z + 1];
-    // block category (uniform); psi tiles this CTA needs
-    const bool nz_h = meets(k0 - 1, k0 + BK - 1, g.az.h), ny_h = meets(j0 - 1, j0 + BJ - 1, g.ay.h);
-    const bool nz_e = meets(k0, k0 + BK - 1, g.az.e), ny_e = meets(j0, j0 + BJ - 1, g.ay.e);
-    if ((nz_h || ny_h || nz_e || ny_e || chs.strip[blockIdx.z] != 0) != ST) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const float *sE = reinterpret_cast<const float *>(smem);
-    const float *sHo = reinterpret_cast<const float *>(smem + OFF_H);
-    const float *sC = reinterpret_cast<const float *>(smem + OFF_C);
-    float *sH = reinterpret_cast<float *>(smem + OFF_SH);
-    const float *sHP = reinterpret_cast<const float *>(smem + OFF_HP);
-    const float *sEP = reinterpret_cast<const float *>(smem + OFF_EP);
-    const uint32_t sbase = s_addr(smem);
-    const uint32_t bar0 = sbase + OFF_BAR;
+    const int nx = g.nx, ny = g.ny, P = g.P;
+    const IX S = (IX)ny * P;
     const int xs = x0 > 0 ? x0 - 1 : 0;  // plane x0-1: its H feeds E(x0)
+    const uint32_t sbase = s_addr(smem), bar0 = sbase + OFF_BAR, barh = bar0 + 8u * NSE;
+    const float *sE = reinterpret_cast<const float *>(smem);
+    const float *sHC = reinterpret_cast<const float *>(smem + OFF_HC);
+    float *sH = reinterpret_cast<float *>(smem + OFF_SH);
+    float *sZT = reinterpret_cast<float *>(smem + OFF_PT), *sYT = sZT + 6 * ZN;
     const bool lossy = g.da_x != nullptr;
     const int ncoef = lossy ? 6 : 3;
-    const bool prod = (w == FW - 1 && lane == 31);
-    const float ch = g.ch;
+    const bool owner = w < NOW;
+    const bool prod = (w == NOW && lane == 0);
+    const int q0 = n - tab.t0;
 
-    // ---- thread role: the cell (j, k) whose H this thread computes
-    const bool own = w < BJ;
-    int j, k, ej, ek, sa;
-    if (own) {
-        j = j0 + w; k = k0 + lane; ej = w + 1; ek = lane + 4; sa = (w + 1) * SHK + lane + 1;
-    } else if (w == BJ) {
-        j = j0 - 1; k = k0 + lane; ej = 0; ek = lane + 4; sa = lane + 1;
-    } else {
-        j = j0 + lane; k = k0 - 1; ej = lane + 1; ek = 3; sa = (lane + 1) * SHK;
-    }
-    const bool hrole = own || w == BJ || lane < BJ;
-    const bool hact = hrole && j >= 0 && j < ny && k >= 0 && k < nz;
-    const int ea = ej * EK + ek, ha = ej * HK + ek;
-    const bool hx_ok = hact && j < ny - 1 && k < nz - 1, hy_k = hact && k < nz - 1, hz_j = hact && j < ny - 1;
-    const bool ein = own && j < ny && k < nz;
-    const bool jin = j >= 1 && j <= ny - 2, kin = k >= 1 && k <= nz - 2;
-    const bool pec_j = (g.pec[2] && j == 0) || (g.pec[3] && j == ny - 1);
-    const bool pec_k = (g.pec[4] && k == 0) || (g.pec[5] && k == nz - 1);
-    float s_amp = 0.f, s_ph1 = 0.f, s_ph2 = 0.f;
-    if (ein && g.src.ix >= 0 && j < g.src.nj && k < g.src.nk) {
-        const size_t m = (size_t)j * g.src.pitch_k + k;
-        s_amp = g.src.amp[m];
-        s_ph1 = g.src.ph1[m];
-        s_ph2 = g.src.ph2[m];
-    }
-    PV zh{-1, 1.f, 0.f, 0.f}, yh = zh, ze = zh, ye = zh;
-    if (ST) {
-        zh = pv_at(g.az.h, k); yh = pv_at(g.ay.h, j);
-        ze = pv_at(g.az.e, k); ye = pv_at(g.ay.e, j);
-    }
-    const size_t S = (size_t)ny * P;
-    size_t o = ((size_t)xs * ny + j) * P + k;  // field / psi index of (xs, j, k)
-
-    auto issue_e = [&](int p, int s) {
+    // ---- producer (lane 0 of the halo warp): E ring and H/coefficient ring.
+    // E(p) sits in slot (p-xs) % NSE, HC(p) in slot (p-xs) % NHC; the u-th fill of a
+    // slot completes mbarrier phase u.  Planes (issued] are in flight, (waited] ready.
+    // After a wait gives up nothing new is issued or awaited (the flag reports it)
+    // and the copies in flight are drained (bounded) before the CTA exits.
+    bool ok = true;
+    int ie = xs - 1, we = xs - 1, ih = xs - 1, wh = xs - 1;
+    auto issue_e = [&](int p) {
+        const int s = (p - xs) % NSE;
         const uint32_t bar = bar0 + 8u * s;
         mbar_expect(bar, 3 * E_BYTES);
-        for (int c = 0; c < 3; ++c) tma3(sbase + (s * 3 + c) * E_SLOT, &tm.e[c], k0 - 4, j0 - 1, p, bar);
-    };
-    auto issue_h = [&](int p, int s) {
-        const uint32_t bar = bar0 + 8u * (NSE + s);
-        int np = 0;
-        bool pn[6] = {false, false, false, false, false, false};
-        if (ST) {
-            const bool xh = meets(p, p, g.ax.h);
-            pn[0] = nz_h; pn[1] = ny_h; pn[2] = xh; pn[3] = nz_h; pn[4] = ny_h; pn[5] = xh;
-            for (int q = 0; q < 6; ++q) np += pn[q];
-        }
-        mbar_expect(bar, (3 + np) * H_BYTES);
-        for (int c = 0; c < 3; ++c) tma3(sbase + OFF_H + (s * 3 + c) * H_SLOT, &tm.h[c], k0 - 4, j0 - 1, p, bar);
-        if (ST)
-            for (int q = 0; q < 6; ++q)
-                if (pn[q]) tma3(sbase + OFF_HP + (s * 6 + q) * H_SLOT, &tm.p[q], k0 - 4, j0 - 1, p, bar);
-    };
-    auto issue_c = [&](int p, int s) {
-        const uint32_t bar = bar0 + 8u * (NSE + NSH + s);
-        int np = 0;
-        bool pn[6] = {false, false, false, false, false, false};
-        if (ST) {
-            const bool xe = meets(p, p, g.ax.e);
-            pn[0] = ny_e; pn[1] = nz_e; pn[2] = nz_e; pn[3] = xe; pn[4] = xe; pn[5] = ny_e;
-            for (int q = 0; q < 6; ++q) np += pn[q];
-        }
-        mbar_expect(bar, (ncoef + np) * C_BYTES);
-        for (int c = 0; c < ncoef; ++c) tma3(sbase + OFF_C + (s * 6 + c) * C_BYTES, &tm.c[c], k0, j0, p, bar);
-        if (ST)
-            for (int q = 0; q < 6; ++q)
-                if (pn[q]) tma3(sbase + OFF_EP + (s * 6 + q) * C_BYTES, &tm.p[6 + q], k0, j0, p, bar);
-    };
-    // rings: E holds planes xs.., H planes xs.., C planes x0..; the producer lane
-    // issues and waits, everybody else only uses __syncthreads
-    Ring we{0, 0, NSE}, wh{0, 0, NSH}, wc{0, 0, NSC};  // waiter cursors
-    Ring fe{0, 0, NSE}, fh{0, 0, NSH}, fc{0, 0, NSC};  // fill cursors
-    bool ok = true;
-    if (prod) {
-        for (int q = 0; q < NSE + NSH + NSC; ++q) mbar_init(bar0 + 8u * q, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (int p = xs; p <= min(x1, xs + NSE - 1); ++p, fe.next()) issue_e(p, fe.s);
-        for (int p = xs; p <= min(x1 - 1, xs + NSH - 1); ++p, fh.next()) issue_h(p, fh.s);
-        for (int p = x0; p <= min(x1 - 1, x0 + NSC - 1); ++p, fc.next()) issue_c(p, fc.s);
-        ok &= mbar_wait(bar0 + 8u * we.s, we.ph);  // E(xs)
-        we.next();
-        ok &= mbar_wait(bar0 + 8u * we.s, we.ph);  // E(xs+1)
-        ok &= mbar_wait(bar0 + 8u * (NSE + wh.s), wh.ph);  // H(xs)
-        wh.next();
-    }
-    __syncthreads();
-    const int EF = E_SLOT / 4, HF = H_SLOT / 4, CF = C_BYTES / 4;
-    const int q0 = n - tab.t0;
-    const float env = tab.env[q0], wt = tab.wt[q0];
-    const bool win = DF && epi && n >= ep.dft_n0 && n < ep.dft_n1;
-    float hym = 0.f, hzm = 0.f;  // own H(i-1), new
-    int se = 0, sh = 0, sc = 0;  // stage of E(i), H(i), C(i)
-    for (int i = xs; i < x1; ++i, o += S) {
-        const bool eon = i >= x0;
-        const int se1 = se + 1 == NSE ? 0 : se + 1;
-        const float *eC = sE + se * 3 * EF;
-        const float *eN = sE + se1 * 3 * EF;
-        const float *hO = sHo + sh * 3 * HF;
-        float *shw = sH + ((i - xs) & 1) * 3 * SH_N;
-        const bool iok = i < nx - 1;
-
-        // DFT accumulators of this plane: loaded now, used after the H phase
-        float4 acc[DF ? 3 : 1];
-        const bool dft_now = DF && win && ein && eon;
-        if (DF && dft_now) {
 #pragma unroll
-            for (int c = 0; c < (DF ? 3 : 1); ++c)
-                if (ep.dft[c]) acc[c] = reinterpret_cast<const float4 *>(ep.dft[c])[o];
+        for (int q = 0; q < 3; ++q) tma3(sbase + (s * 3 + q) * E_SLOT, &tm.e[q], k0 - 4, j0 - 1, p, bar);
+        ie = p;
+    };
+    auto issue_hc = [&](int p) {
+        const int s = (p - xs) % NHC;
+        const uint32_t bar = barh + 8u * s, dst = sbase + OFF_HC + s * HC_SLOT;
+        mbar_expect(bar, (3 + ncoef) * HT * 4);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) tma3(dst + q * HT * 4, &tm.h[q], k0, j0, p, bar);
+        for (int q = 0; q < ncoef; ++q) tma3(dst + (3 + q) * HT * 4, &tm.c[q], k0, j0, p, bar);
+        ih = p;
+    };
+    auto wait_e = [&](int p) {
+        if (ok) ok = mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1);
+        if (ok) we = p;
+    };
+    auto wait_hc = [&](int p) {
+        if (ok) ok = mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1);
+        if (ok) wh = p;
+    };
+    if (prod) {
+        for (int q = 0; q < NSE + NHC; ++q) mbar_init(bar0 + 8u * q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int p = xs; p <= min(x1, xs + NSE - 1); ++p) issue_e(p);
+        for (int p = xs; p <= min(x1 - 1, xs + NHC - 1); ++p) issue_hc(p);
+        wait_e(xs);
+        if (xs + 1 <= x1) wait_e(xs + 1);
+        wait_hc(xs);
+    }
+
+    // ---- per-thread cells.  Owners: rows a = j0+2w, b = a+1 at k = k0+lane.
+    // Halo warp: A = (j0-1, k0+lane), B = (j0+lane, k0-1) for lane < TJ.
+    const int k = owner ? k0 + lane : 0;
+    const int ja = owner ? j0 + 2 * w : 0, jb = ja + 1;
+    const int kA = k0 + lane, jA = j0 - 1, kB = k0 - 1, jB = j0 + lane;
+    unsigned fa, fb;
+    int ea, sa;            // E-box / new-H tile index of the first cell
+    IX oa, ob;             // in-plane offsets
+    if (owner) {
+        fa = cell_flags(g, ep, ja, k);
+        fb = cell_flags(g, ep, jb, k);
+        ea = (2 * w + 1) * EK + lane + 4;
+        sa = (2 * w + 1) * SHK + lane + 1;
+        oa = (IX)ja * P + k;
+        ob = oa + P;
+    } else {
+        fa = cell_flags(g, ep, jA, kA);
+        fb = lane < TJ ? cell_flags(g, ep, jB, kB) : 0u;
+        ea = lane + 4;
+        sa = lane + 1;
+        oa = (fa & F_IN) ? (IX)jA * P + kA : 0;
+        ob = (fb & F_IN) ? (IX)jB * P + kB : 0;
+    }
+    const int hl = lane < TJ ? lane : TJ - 1;  // lanes >= TJ of the halo warp compute a discarded copy
+    const int eb = owner ? ea + EK : (hl + 1) * EK + 3;
+    const int sb = owner ? sa + SHK : (hl + 1) * SHK;
+    const int ta = 2 * w * TK + lane;          // owner tile index of row a (row b: ta + TK)
+    // profile-table entries of the two cells
+    const float *zta = sZT + lane + 1, *ztb = owner ? zta : sZT;
+    const float *yta = sYT + (owner ? 2 * w + 1 : 0), *ytb = owner ? yta + 1 : sYT + hl + 1;
+    if (ST) {
+        const int t = w * TK + lane;
+        if (t < ZN) {
+            fill_row(sZT + t, ZN, g.az.h, k0 - 1 + t);
+            fill_row(sZT + 3 * ZN + t, ZN, g.az.e, k0 - 1 + t);
+        } else if (t < ZN + YN) {
+            fill_row(sYT + (t - ZN), YN, g.ay.h, j0 - 1 + (t - ZN));
+            fill_row(sYT + 3 * YN + (t - ZN), YN, g.ay.e, j0 - 1 + (t - ZN));
         }
-        // ---- H(i) at (j, k)
-        const float ex = eC[ea], ey = eC[EF + ea], ez = eC[2 * EF + ea];
-        float hx = 0.f, hy = 0.f, hz = 0.f;
-        if (hact) {
-            hx = hO[ha];
-            hy = hO[HF + ha];
-            hz = hO[2 * HF + ha];
-            const float dxz = eC[EF + ea + 1] - ey, dxy = eC[2 * EF + ea + EK] - ez;  // Hx terms
-            const float dyx = eN[2 * EF + ea] - ez, dyz = eC[ea + 1] - ex;          // Hy terms
-            const float dzy = eC[ea + EK] - ex, dzx = eN[EF + ea] - ey;             // Hz terms
-            if (hx_ok) hx = hx + ch * (dxz - dxy);
-            if (iok && hy_k) hy = hy + ch * (dyx - dyz);
-            if (iok && hz_j) hz = hz + ch * (dzy - dzx);
-            if (ST) {
-                const bool wr = own && eon;  // psi of this plane is written by its owner only
-                const PV xh = pv_at(g.ax.h, i);
-                const float *hp = sHP + sh * 6 * HF + ha;
-                if (hx_ok) {
-                    if (zh.s >= 0) hx = hx + ch * psi_u(hp[0], zh, dxz, g.pw[LENS_PSI_HX_Z], o, wr);
-                    if (yh.s >= 0) hx = hx + (-ch) * psi_u(hp[HF], yh, dxy, g.pw[LENS_PSI_HX_Y], o, wr);
-                }
-                if (iok && hy_k) {
-                    if (xh.s >= 0) hy = hy + ch * psi_u(hp[2 * HF], xh, dyx, g.pw[LENS_PSI_HY_X], o, wr);
-                    if (zh.s >= 0) hy = hy + (-ch) * psi_u(hp[3 * HF], zh, dyz, g.pw[LENS_PSI_HY_Z], o, wr);
-                }
-                if (iok && hz_j) {
-                    if (yh.s >= 0) hz = hz + ch * psi_u(hp[4 * HF], yh, dzy, g.pw[LENS_PSI_HZ_Y], o, wr);
-                    if (xh.s >= 0) hz = hz + (-ch) * psi_u(hp[5 * HF], xh, dzx, g.pw[LENS_PSI_HZ_X], o, wr);
-                }
+    }
+
+    // halo warp: old H by loads one plane ahead; CPML tiles: psi one phase ahead
+    //   after the H phase of plane i: halo old H of plane i+1, E-psi of plane i;
+    //   after the E phase of plane i: H-psi of plane i+1.
+    F3 hoa{0.f, 0.f, 0.f}, hob{0.f, 0.f, 0.f};
+    P6 hpa, hpb, epa, epb;
+    auto load_hold = [&](int p) {
+        const IX base = (IX)p * S;
+        if (fa & F_IN) hoa = F3{__ldg(g.hx + base + oa), __ldg(g.hy + base + oa), __ldg(g.hz + base + oa)};
+        if (fb & F_IN) hob = F3{__ldg(g.hx + base + ob), __ldg(g.hy + base + ob), __ldg(g.hz + base + ob)};
+    };
+    auto load_hp = [&](int p) {
+        const IX base = (IX)p * S;
+        const bool xh = in_strip(g.ax.h, p);
+        if (fa & F_IN) load_hpsi(hpa, g, base + oa, fa, xh);
+        if (fb & F_IN) load_hpsi(hpb, g, base + ob, fb, xh);
+    };
+    auto load_ep = [&](int p) {
+        const IX base = (IX)p * S;
+        const bool xe = in_strip(g.ax.e, p);
+        if (fa & F_IN) load_epsi(epa, g, base + oa, fa, xe);
+        if (fb & F_IN) load_epsi(epb, g, base + ob, fb, xe);
+    };
+    if (!owner) load_hold(xs);
+    if (ST) load_hp(xs);
+
+    // detector boxes: per-thread float sums over the chunk, added to the FP64 totals at the end
+    float bacc[LENS_MAX_BOX];
+#pragma unroll
+    for (int b = 0; b < LENS_MAX_BOX; ++b) bacc[b] = 0.f;
+    const bool boxes = epi && ep.nbox > 0;
+    const float env = tab.env[q0], wt = tab.wt[q0];
+
+    // E(i) of the owner cells at (j, k): Ey, Ez carried from the previous plane's "next" reads
+    float cya = 0.f, cza = 0.f, cyb = 0.f, czb = 0.f;
+    float hyma = 0.f, hzma = 0.f, hymb = 0.f, hzmb = 0.f;  // new H(i-1)
+    __syncthreads();  // E(xs), E(xs+1), HC(xs) visible (waited by the producer)
+    if (owner) {  // plane xs sits in slot 0
+        cya = sE[EF + ea];
+        cza = sE[2 * EF + ea];
+        cyb = sE[EF + eb];
+        czb = sE[2 * EF + eb];
+    }
+
+    for (int i = xs; i < x1; ++i) {
+        const bool eon = i >= x0;
+        const unsigned u = i - xs;
+        const unsigned sc = u % NSE, sn = (u + 1) % NSE;
+        const float *eC = sE + sc * 3 * EF, *eN = sE + sn * 3 * EF;
+        const float *hc = sHC + (u % NHC) * (HC_SLOT / 4);
+        float *shw = sH + (u & 1) * 3 * SH_N;
+        const bool iok = i < nx - 1;
+        const bool xh = ST && in_strip(g.ax.h, i);
+        const PX px = ST ? px_at(g, i) : PX{};
+        const IX base = (IX)i * S;
+        F3 ha{0.f, 0.f, 0.f}, hb{0.f, 0.f, 0.f};
+        float exa = 0.f, exb = 0.f, nya = 0.f, nza = 0.f, nyb = 0.f, nzb = 0.f;
+        // ---------------- H(i)
+        if (owner) {
+            exa = eC[ea];
+            const float exa1 = eC[ea + 1], eya1 = eC[EF + ea + 1];
+            exb = eC[eb];
+            const float exb1 = eC[eb + 1], eyb1 = eC[EF + eb + 1];
+            const float exc = eC[eb + EK], ezc = eC[2 * EF + eb + EK];
+            nya = eN[EF + ea];
+            nza = eN[2 * EF + ea];
+            nyb = eN[EF + eb];
+            nzb = eN[2 * EF + eb];
+            const F3 h0a{hc[ta], hc[HT + ta], hc[2 * HT + ta]};
+            const F3 h0b{hc[ta + TK], hc[HT + ta + TK], hc[2 * HT + ta + TK]};
+            const bool wr = eon;
+            ha = h_new<ST, IX>(g, h0a, exa, cya, cza, exa1, eya1, exb, czb, nya, nza, fa, iok, zta, yta, px,
+                               hpa, base + oa, wr, xh);
+            hb = h_new<ST, IX>(g, h0b, exb, cyb, czb, exb1, eyb1, exc, ezc, nyb, nzb, fb, iok, ztb, ytb, px,
+                               hpb, base + ob, wr, xh);
+        } else if (eon) {
+            // halo cells: A on row 0 of the boxes, B on column 0 (read-only psi)
+            const float *c = eC + ea;
+            ha = h_new<ST, IX>(g, hoa, c[0], c[EF], c[2 * EF], c[1], c[EF + 1], c[EK], c[2 * EF + EK],
+                               eN[EF + ea], eN[2 * EF + ea], fa, iok, zta, yta, px, hpa, base + oa, false, xh);
+            const float *d = eC + eb;
+            hb = h_new<ST, IX>(g, hob, d[0], d[EF], d[2 * EF], d[1], d[EF + 1], d[EK], d[2 * EF + EK],
+                               eN[EF + eb], eN[2 * EF + eb], fb, iok, ztb, ytb, px, hpb, base + ob, false, xh);
+        }
+        if (owner || eon) {
+            shw[sa] = ha.x;
+            shw[SH_N + sa] = ha.y;
+            shw[2 * SH_N + sa] = ha.z;
+            if (owner || lane < TJ) {
+                shw[sb] = hb.x;
+                shw[SH_N + sb] = hb.y;
+                shw[2 * SH_N + sb] = hb.z;
             }
         }
-        if (hrole) {
-            shw[sa] = hx;
-            shw[SH_N + sa] = hy;
-            shw[2 * SH_N + sa] = hz;
-        }
-        if (prod) {  // data of this plane's E phase and of the next plane's H phase
-            if (eon) {
-                ok &= mbar_wait(bar0 + 8u * (NSE + NSH + wc.s), wc.ph);
-                wc.next();
-            }
-            if (i + 2 <= x1) {
-                we.next();
-                ok &= mbar_wait(bar0 + 8u * we.s, we.ph);
-            }
-            if (i + 1 <= x1 - 1) {
-                ok &= mbar_wait(bar0 + 8u * (NSE + wh.s), wh.ph);
-                wh.next();
-            }
+        if (!owner && i + 1 < x1) load_hold(i + 1);
+        if (ST && owner && eon) load_ep(i);
+        if (prod) {
+            if (i + 2 <= x1) wait_e(i + 2);
+            if (i + 1 < x1) wait_hc(i + 1);
         }
         __syncthreads();
-        // E(i) and H(i) stages are free now, and the coefficients of plane i-1
-        if (prod) {
-            if (i + NSE <= x1) {
-                issue_e(i + NSE, fe.s);
-                fe.next();
+        if (prod && ok) {
+            if (i + NSE <= x1) issue_e(i + NSE);                        // E(i)'s slot is free
+            if (i - 1 >= xs && i - 1 + NHC <= x1 - 1) issue_hc(i - 1 + NHC);  // HC(i-1)'s slot is free
+        }
+
+        // ---------------- E(i)
+        if (owner && eon) {
+            PlE pl;
+            pl.iok = iok;
+            pl.iin = i >= 1 && i <= nx - 2;
+            pl.pec_i = (g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1);
+            pl.xe = ST && in_strip(g.ax.e, i);
+            pl.src = g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1);
+            pl.sgn = i == g.src.ix ? 1.f : -1.f;
+            pl.env = env;
+            pl.wt = wt;
+            const float hxja = shw[sa - SHK], hzja = shw[2 * SH_N + sa - SHK];
+            const float hxka = shw[sa - 1], hyka = shw[SH_N + sa - 1];
+            const float hxkb = shw[sb - 1], hykb = shw[SH_N + sb - 1];
+            const float *cs = hc + 3 * HT + ta;
+            const C6 ca{cs[0], cs[HT], cs[2 * HT], lossy ? cs[3 * HT] : 1.f, lossy ? cs[4 * HT] : 1.f,
+                        lossy ? cs[5 * HT] : 1.f};
+            cs += TK;
+            const C6 cb{cs[0], cs[HT], cs[2 * HT], lossy ? cs[3 * HT] : 1.f, lossy ? cs[4 * HT] : 1.f,
+                        lossy ? cs[5 * HT] : 1.f};
+            const F3 Ea = e_new<ST, IX>(g, F3{exa, cya, cza}, ha, hxka, hyka, hxja, hzja, hyma, hzma, ca, fa,
+                                        pl, ja, k, zta, yta, px, epa, base + oa);
+            const F3 Eb = e_new<ST, IX>(g, F3{exb, cyb, czb}, hb, hxkb, hykb, ha.x, ha.z, hymb, hzmb, cb, fb,
+                                        pl, jb, k, ztb, ytb, px, epb, base + ob);
+            if (!ST || (fa & F_IN)) {
+                const IX o = base + oa;
+                g.whx[o] = ha.x; g.why[o] = ha.y; g.whz[o] = ha.z;
+                g.wex[o] = Ea.x; g.wey[o] = Ea.y; g.wez[o] = Ea.z;
             }
-            if (i + NSH <= x1 - 1) {
-                issue_h(i + NSH, fh.s);
-                fh.next();
+            if (!ST || (fb & F_IN)) {
+                const IX o = base + ob;
+                g.whx[o] = hb.x; g.why[o] = hb.y; g.whz[o] = hb.z;
+                g.wex[o] = Eb.x; g.wey[o] = Eb.y; g.wez[o] = Eb.z;
             }
-            if (i - 1 >= x0 && i - 1 + NSC <= x1 - 1) {
-                issue_c(i - 1 + NSC, fc.s);
-                fc.next();
+            if (boxes) {
+                // detector boxes: Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481; invalid components are zero)
+#pragma unroll
+                for (int b = 0; b < LENS_MAX_BOX; ++b) {
+                    if (b < ep.nbox && i >= ep.box[b][0] && i < ep.box[b][1]) {
+                        if (fa & (F_BOX0 << b)) bacc[b] += (Ea.x * Ea.x + Ea.y * Ea.y) + Ea.z * Ea.z;
+                        if (fb & (F_BOX0 << b)) bacc[b] += (Eb.x * Eb.x + Eb.y * Eb.y) + Eb.z * Eb.z;
+                    }
+                }
             }
         }
-        if (own && eon) {
-            Hv e{0.f, 0.f, 0.f};
-            if (ein) {
-                g.whx[o] = hx;
-                g.why[o] = hy;
-                g.whz[o] = hz;
-                const int ca = w * BK + lane;
-                const float *cs = sC + sc * 6 * CF + ca;
-                const bool iin = i >= 1 && i <= nx - 2;
-                const bool pec_i = (g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1);
-                float src = 0.f;
-                if (i == g.src.ix) src = (env * sinf(wt + s_ph1)) * s_amp;
-                else if (g.src.ix >= 0 && i == g.src.ix + 1) src = -((env * sinf(wt + s_ph2)) * s_amp);
-                const float hzj = shw[2 * SH_N + sa - SHK], hyk = shw[SH_N + sa - 1];
-                const float hxk = shw[sa - 1], hxj = shw[sa - SHK];
-                const float d1x = hz - hzj, d2x = hy - hyk;  // Ex
-                const float d1y = hx - hxk, d2y = hz - hzm;  // Ey
-                const float d1z = hy - hym, d2z = hx - hxj;  // Ez
-                float vx = ex, vy = ey, vz = ez;
-                if (iok) {
-                    if (lossy) vx = vx * cs[3 * CF];
-                    if (jin && kin) vx = vx + cs[0] * (d1x - d2x);
-                }
-                if (j < ny - 1) {
-                    if (lossy) vy = vy * cs[4 * CF];
-                    if (iin && kin) vy = vy + cs[CF] * (d1y - d2y);
-                }
-                if (k < nz - 1) {
-                    if (lossy) vz = vz * cs[5 * CF];
-                    if (iin && jin) vz = vz + cs[2 * CF] * (d1z - d2z);
-                }
-                if (ST) {
-                    const PV xe = pv_at(g.ax.e, i);
-                    const float *pp = sEP + sc * 6 * CF + ca;
-                    if (iok && jin && kin) {
-                        const float cx = cs[0];
-                        if (ye.s >= 0) vx = vx + cx * psi_u(pp[0], ye, d1x, g.pw[LENS_PSI_EX_Y], o, true);
-                        if (ze.s >= 0) vx = vx + (-cx) * psi_u(pp[CF], ze, d2x, g.pw[LENS_PSI_EX_Z], o, true);
-                    }
-                    if (j < ny - 1 && iin && kin) {
-                        const float cy = cs[CF];
-                        if (ze.s >= 0) vy = vy + cy * psi_u(pp[2 * CF], ze, d1y, g.pw[LENS_PSI_EY_Z], o, true);
-                        if (xe.s >= 0) vy = vy + (-cy) * psi_u(pp[3 * CF], xe, d2y, g.pw[LENS_PSI_EY_X], o, true);
-                    }
-                    if (k < nz - 1 && iin && jin) {
-                        const float cz = cs[2 * CF];
-                        if (xe.s >= 0) vz = vz + cz * psi_u(pp[4 * CF], xe, d1z, g.pw[LENS_PSI_EZ_X], o, true);
-                        if (ye.s >= 0) vz = vz + (-cz) * psi_u(pp[5 * CF], ye, d2z, g.pw[LENS_PSI_EZ_Y], o, true);
-                    }
-                }
-                if (iok) {
-                    if (pec_j || pec_k) vx = 0.f;
-                    if (g.src_comp == 0) vx += src;
-                    e.x = vx;
-                }
-                if (j < ny - 1) {
-                    if (pec_i || pec_k) vy = 0.f;
-                    if (g.src_comp == 1) vy += src;
-                    e.y = vy;
-                }
-                if (k < nz - 1) {
-                    if (pec_i || pec_j) vz = 0.f;
-                    if (g.src_comp == 2) vz += src;
-                    e.z = vz;
-                }
-                g.wex[o] = e.x;
-                g.wey[o] = e.y;
-                g.wez[o] = e.z;
-            }
-            if (DF && dft_now) {
-                const float pr = tab.pe[2 * q0], pim = tab.pe[2 * q0 + 1];
-                const bool vx = iok, vy = j < ny - 1, vz = k < nz - 1;
-                if (ep.dft[0] && vx) {
-                    kahan_reg(acc[0], e.x * pr, e.x * pim);
-                    reinterpret_cast<float4 *>(ep.dft[0])[o] = acc[0];
-                }
-                if (ep.dft[1] && vy) {
-                    kahan_reg(acc[DF ? 1 : 0], e.y * pr, e.y * pim);
-                    reinterpret_cast<float4 *>(ep.dft[1])[o] = acc[DF ? 1 : 0];
-                }
-                if (ep.dft[2] && vz) {
-                    kahan_reg(acc[DF ? 2 : 0], e.z * pr, e.z * pim);
-                    reinterpret_cast<float4 *>(ep.dft[2])[o] = acc[DF ? 2 : 0];
-                }
-            }
-            if (epi) epi_cell(g, tab, ep, n, i, j, k, ein, e, hym, hzm, Hv{hx, hy, hz}, !DF);
-        }
-        if (eon) sc = sc + 1 == NSC ? 0 : sc + 1;
-        se = se1;
-        sh = sh + 1 == NSH ? 0 : sh + 1;
-        hym = hy;
-        hzm = hz;
+        if (ST && i + 1 < x1) load_hp(i + 1);
+        // carry
+        cya = nya; cza = nza; cyb = nyb; czb = nzb;
+        hyma = ha.y; hzma = ha.z; hymb = hb.y; hzmb = hb.z;
     }
-    if (prod && !ok && g.flag) atomicExch(g.flag, 1);
+    if (owner && boxes) {
+#pragma unroll
+        for (int b = 0; b < LENS_MAX_BOX; ++b)
+            if (b < ep.nbox) warp_atomic_add(ep.box_acc + b, (double)bacc[b]);
+    }
+    if (prod && !ok) {
+        for (int p = we + 1; p <= ie; ++p) mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1);
+        for (int p = wh + 1; p <= ih; ++p) mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1);
+        if (g.flag) atomicExch(g.flag, 1);
+    }
+}
+
+template <typename IX>
+__global__ void __launch_bounds__(NW3 * 32, 2)
+    yee3d(const __grid_constant__ EMaps tm, const K3 g, const LensStepTable tab, const LensEpi3D ep, int n,
+          int epi, const __grid_constant__ Work wk) {
+    int tz, ty, c;
+    const bool lean = work_tile(wk, blockIdx.x, tz, ty, c);
+    extern __shared__ __align__(128) unsigned char smem[];
+    if (!lean)
+        tile3d<true, IX>(tm, g, tab, ep, n, epi, tz * TK, ty * TJ, wk.x[c], wk.x[c + 1], smem);
+    else
+        tile3d<false, IX>(tm, g, tab, ep, n, epi, tz * TK, ty * TJ, wk.x[c], wk.x[c + 1], smem);
+}
+
+// Window epilogue after a fused step (DFT / convergence windows): volume DFTs,
+// convergence planes and flux planes of the NEW fields (g reads the buffer the
+// step wrote).  A separate streaming pass keeps the step kernel's registers for
+// its pipeline: it reads E once (12 B per cell) and updates the complex
+// accumulators (16 B per component and cell) on window steps only.
+__global__ void __launch_bounds__(NT) win3d(const K3 g, const LensStepTable tab, const LensEpi3D ep, int n) {
+    const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y, i = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (k >= nz || j >= ny) return;  // no warp-collective operations below
+    const size_t S = (size_t)ny * g.P, o = i * S + (size_t)j * g.P + k;
+    const bool vx = i < nx - 1, vy = j < ny - 1, vz = k < nz - 1;
+    const bool win = n >= ep.dft_n0 && n < ep.dft_n1;
+    const int q = n - tab.t0;
+    const float pr = tab.pe[2 * q], pim = tab.pe[2 * q + 1];
+    const float ex = vx ? g.ex[o] : 0.f, ey = vy ? g.ey[o] : 0.f, ez = vz ? g.ez[o] : 0.f;
+    if (win) {
+        const float v[3] = {ex, ey, ez};
+        const bool ok[3] = {vx, vy, vz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (ep.dft[c] && ok[c]) {
+                float2 *a = reinterpret_cast<float2 *>(ep.dft[c]) + o;
+                float2 s = *a;
+                s.x += v[c] * pr;
+                s.y += v[c] * pim;
+                *a = s;
+            }
+        }
+    }
+    const bool conv = (win && ep.conv_last) || (ep.conv_prev && n >= ep.prev_n0 && n < ep.prev_n1);
+    bool fl = false;
+    for (int p = 0; p < ep.nplane; ++p) fl |= (i == ep.plane[p]);
+    if ((conv && k == ep.conv_k) || (win && fl)) {
+        Hv h{0.f, 0.f, 0.f};
+        float hym = 0.f, hzm = 0.f;
+        if (fl) {
+            h = Hv{g.hx[o], g.hy[o], g.hz[o]};
+            hym = g.hy[o - S];
+            hzm = g.hz[o - S];
+        }
+        epi_cell(g, tab, ep, n, i, j, k, true, Hv{ex, ey, ez}, hym, hzm, h, false, false);
+    }
 }
 
 // ============================================================ Iavg
@@ -915,20 +1198,21 @@ K3 view(const LensGrid3D *g, int rb, int wb) {
 }
 
 // x-chunks of the fused pass: the planes that carry x CPML psi get chunks of
-// their own, the rest is cut into pieces of about `target` planes.
-Chunks make_chunks(const LensGrid3D *g, int target) {
-    Chunks c{};
+// their own, the rest is cut into pieces of about `target` planes.  Returns the
+// chunk count; x[c] is the first plane of chunk c, strip[c] != 0 for CPML chunks.
+int make_chunks(const LensGrid3D *g, int target, int *x, int *strip) {
     const int nx = g->nx;
+    int n = 0;
     int lo = g->ax.h.lo > g->ax.e.lo ? g->ax.h.lo : g->ax.e.lo;
     int hi = nx - 1 - g->ax.h.hi;
     if (nx - g->ax.e.hi < hi) hi = nx - g->ax.e.hi;
     lo = lo > 0 ? lo + 1 : 0;  // the next chunk's warm-up plane lo must be strip-free too
     if (hi < lo) hi = lo;
-    auto add = [&](int a, int b, int strip) {
-        if (b <= a || c.n >= MAXCH) return;
-        c.x[c.n] = a;
-        c.strip[c.n] = strip;
-        c.x[++c.n] = b;
+    auto add = [&](int a, int b, int s) {
+        if (b <= a || n >= MAXCH) return;
+        x[n] = a;
+        strip[n] = s;
+        x[++n] = b;
     };
     if (lo > 0) add(0, lo, 1);
     const int mid = hi - lo;
@@ -936,10 +1220,64 @@ Chunks make_chunks(const LensGrid3D *g, int target) {
         int pieces = (mid + target / 2) / target;
         if (pieces < 1) pieces = 1;
         if (pieces > MAXCH - 4) pieces = MAXCH - 4;
-        for (int q = 0; q < pieces; ++q) add(lo + (int)((long)mid * q / pieces), lo + (int)((long)mid * (q + 1) / pieces), 0);
+        for (int q = 0; q < pieces; ++q)
+            add(lo + (int)((long)mid * q / pieces), lo + (int)((long)mid * (q + 1) / pieces), 0);
     }
     if (hi < nx) add(hi, nx, 1);
-    return c;
+    return n;
+}
+
+// Lean (CPML-free) range [l0, l1) of a sequence of tiles; empty when the lean
+// tiles are not one contiguous run.
+template <class F>
+void lean_range(int count, F is_strip, int &l0, int &l1) {
+    l0 = 0;
+    while (l0 < count && is_strip(l0)) ++l0;
+    l1 = l0;
+    while (l1 < count && !is_strip(l1)) ++l1;
+    for (int q = l1; q < count; ++q)
+        if (!is_strip(q)) l0 = l1 = 0;
+}
+
+// Work of the fused pass: all tiles, and the CPML-free interior core.  The chunk length is chosen so that the CTAs
+// fill whole waves of `slots` resident CTAs: estimated time = waves x (planes
+// per chunk + 1 warm-up plane).
+Work make_work(const LensGrid3D *g, int slots) {
+    Work wk{};
+    int cstrip[MAXCH];
+    const int ntz = g->pitch / TK, nty = (g->ny + TJ - 1) / TJ;
+    int target = 32;
+    double best = 1e300;
+    for (int t = 12; t <= 96; t += 2) {
+        const int nc = make_chunks(g, t, wk.x, cstrip);
+        const double waves = std::ceil((double)ntz * nty * nc / (slots > 0 ? slots : 1));
+        const double cost = waves * ((double)g->nx / nc + 1.0);
+        if (cost < best - 1e-9) {
+            best = cost;
+            target = t;
+        }
+    }
+    const int nc = make_chunks(g, target, wk.x, cstrip);
+    int z0, z1, y0, y1, c0, c1;
+    // a lean tile has no psi strip cell (owners and halo) and lies inside the
+    // domain's interior: every component of every cell exists and updates
+    lean_range(ntz, [&](int t) {
+        const int k0 = t * TK;
+        return meets(k0 - 1, k0 + TK - 1, g->az.h) || meets(k0, k0 + TK - 1, g->az.e) || k0 < 1 ||
+               k0 + TK - 1 > g->nz - 2;
+    }, z0, z1);
+    lean_range(nty, [&](int t) {
+        const int j0 = t * TJ;
+        return meets(j0 - 1, j0 + TJ - 1, g->ay.h) || meets(j0, j0 + TJ - 1, g->ay.e) || j0 < 1 ||
+               j0 + TJ - 1 > g->ny - 2;
+    }, y0, y1);
+    lean_range(nc, [&](int c) { return cstrip[c] != 0 || wk.x[c] < 1 || wk.x[c + 1] > g->nx - 1; }, c0, c1);
+    if (z1 == z0 || y1 == y0 || c1 == c0) z0 = z1 = y0 = y1 = c0 = c1 = 0;
+    wk.ntz = ntz; wk.nty = nty; wk.nc = nc;
+    wk.lo[0] = z0; wk.hi[0] = z1;
+    wk.lo[1] = y0; wk.hi[1] = y1;
+    wk.lo[2] = c0; wk.hi[2] = c1;
+    return wk;
 }
 
 // x-chunk length: about `target` planes, enough CTAs that the last wave's tail is short.
@@ -1010,42 +1348,35 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
         for (int q = 0; q < LENS_NPSI; ++q)
             if (!g->psi[b][q] || (reinterpret_cast<uintptr_t>(g->psi[b][q]) & 15)) return LENS_ERR_ARG;
     }
-    if (cudaFuncSetAttribute(fused3d<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LEAN) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(fused3d<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LEAN) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(fused3d<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_STRIP) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(fused3d<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_STRIP) !=
-            cudaSuccess)
+    const bool ix32 = (double)g->nx * g->ny * g->pitch < 2147483647.0;
+    if (cudaFuncSetAttribute(yee3d<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM3) != cudaSuccess ||
+        cudaFuncSetAttribute(yee3d<size_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM3) != cudaSuccess)
         return LENS_ERR_CUDA;
-    TMaps tm[2];
+    EMaps tm[2];
     for (int rb = 0; rb < 2; ++rb) {
-        bool ok = true;
-        for (int c = 0; c < 3; ++c) {
-            ok = ok && encode(&tm[rb].e[c], g->f[rb][c], g, EK, EJ);
-            ok = ok && encode(&tm[rb].h[c], g->f[rb][3 + c], g, HK, HJ);
-            ok = ok && encode(&tm[rb].c[c], bases[c], g, BK, BJ);
-            ok = ok && encode(&tm[rb].c[3 + c], g->da_x ? bases[3 + c] : bases[c], g, BK, BJ);
-        }
-        for (int q = 0; q < LENS_NPSI; ++q)  // H-psi tiles like H, E-psi tiles like the coefficients
-            ok = ok && encode(&tm[rb].p[q], g->psi[rb][q], g, q < 6 ? HK : BK, q < 6 ? HJ : BJ);
-        if (!ok) return LENS_ERR_CUDA;
+        for (int c = 0; c < 3; ++c)
+            if (!encode(&tm[rb].e[c], g->f[rb][c], g, EK, EJ) || !encode(&tm[rb].h[c], g->f[rb][3 + c], g, TK, TJ))
+                return LENS_ERR_CUDA;
+        for (int c = 0; c < 6; ++c)
+            if (!encode(&tm[rb].c[c], c < 3 ? bases[c] : (g->da_x ? bases[c] : bases[c - 3]), g, TK, TJ))
+                return LENS_ERR_CUDA;
     }
-    const Chunks chs = make_chunks(g, 40);
-    const dim3 grd(g->pitch / BK, (g->ny + BJ - 1) / BJ, chs.n);
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return LENS_ERR_CUDA;
+    const Work wk = make_work(g, 2 * nsm);
+    const int nblk = wk.ntz * wk.nty * wk.nc;
+    const dim3 grd_w(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx);
     for (int n = n0; n < n0 + nsteps; ++n) {
         const int rb = g->cur;
         const K3 k = view(g, rb, 1 - rb);
         const int ea = epi3d_active(&e, n);
-        const bool df = ea && n >= e.dft_n0 && n < e.dft_n1 && (e.dft[0] || e.dft[1] || e.dft[2]);
-        if (df) {
-            fused3d<true, true><<<grd, dim3(BK, FW), SMEM_STRIP, s>>>(tm[rb], k, *tab, e, n, ea, chs);
-            fused3d<false, true><<<grd, dim3(BK, FW), SMEM_LEAN, s>>>(tm[rb], k, *tab, e, n, ea, chs);
-        } else {
-            fused3d<true, false><<<grd, dim3(BK, FW), SMEM_STRIP, s>>>(tm[rb], k, *tab, e, n, ea, chs);
-            fused3d<false, false><<<grd, dim3(BK, FW), SMEM_LEAN, s>>>(tm[rb], k, *tab, e, n, ea, chs);
-        }
+        if (ix32)
+            yee3d<uint32_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
+        else
+            yee3d<size_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
+        if (ea && ((n >= e.dft_n0 && n < e.dft_n1) || (e.conv_prev && n >= e.prev_n0 && n < e.prev_n1)))
+            win3d<<<grd_w, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, e, n);
         g->cur = 1 - rb;
     }
     return lens_cuda_status();

@@ -270,6 +270,7 @@ class Grid3D:
         self.ax = [_Axis(cpml[a], n, dev) for a, n in enumerate((nx, ny, nz))]
         X, Y, Zp = self.ax
         nbuf = 2 if fused else 1
+
         self.bufs = [{f: z() for f in self.FIELDS} for _ in range(nbuf)]
         # psi volumes are full-domain (only their CPML strips are touched)
         self.psi = [{q: z() for q in N.PSI_NAMES} for _ in range(nbuf)]
@@ -342,7 +343,7 @@ class Epi3D:
         self.dft = [None, None, None]
         if dft is not None:
             for c in comps:
-                self.dft[c] = torch.zeros((nx, ny, P, 4), dtype=torch.float32, device=dev)
+                self.dft[c] = torch.zeros((nx, ny, P, 2), dtype=torch.float32, device=dev)
         self.planes = dict(planes)
         self.plane_acc = torch.zeros((max(1, len(self.planes)), 2, 4, ny, P), dtype=torch.float64,
                                      device=dev)
@@ -373,7 +374,8 @@ class Epi3D:
         g = self.grid
         nx, ny, nz = g.nx, g.ny, g.nz
         shape = {0: (nx - 1, ny, nz), 1: (nx, ny - 1, nz), 2: (nx, ny, nz - 1)}[comp]
-        return _kahan_value(self.dft[comp])[:shape[0], :shape[1], :shape[2]]
+        a = self.dft[comp].double()
+        return torch.complex(a[..., 0], a[..., 1])[:shape[0], :shape[1], :shape[2]]
 
     def flux(self, name, n_acc):
         """Net +x Poynting flux (pairs_3d, flux.py:84-90 and :45-57)."""

@@ -92,18 +92,26 @@ class Solve3D:
         """Advance from the current step to n1 (default: the end of the schedule)."""
         n1 = self.steps_total if n1 is None else min(int(n1), self.steps_total)
         n = self.n
-        per_step = 2                      # two launches per step (strip + lean blocks, or H + E)
+        fused = self.grid.s.f[1][0] is not None
         for m in self.iavg_steps(n, n1) + [None]:
             stop = n1 if m is None else m + 1
             if stop > n:
                 self.grid.step(self.table, n, stop - n, self.epi, stream)
-                self.launches += per_step * (stop - n)
+                self.launches += self._launches(n, stop, fused)
                 n = stop
             if m is not None:
                 self.grid.accum_e2(self.epi.iavg, stream=stream)
                 self.launches += 1
         self.n = n
         return self
+
+    def _launches(self, n0, n1, fused):
+        """Kernel launches of steps [n0, n1): fused, one step kernel plus the window
+        epilogue on DFT / convergence-window steps; two passes otherwise."""
+        if not fused:
+            return 2 * (n1 - n0)
+        w0, w1 = self.prev[0], self.dft[1]
+        return (n1 - n0) + max(0, min(n1, w1) - max(n0, w0))
 
     # ---------------------------------------------------------------- results
     def phasor(self, comp=None):

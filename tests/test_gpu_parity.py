@@ -179,3 +179,18 @@ def test_3d_uneven_tiles_and_chunks():
     o = H.run_3d(c, setup=s, n_dft=15, box=(slice(36, 44), slice(20, 34), slice(8, 37)))
     check_fields_3d(r, o)
     assert rel_l2(r['acc'], o['acc']) < TOL_FIELD
+
+
+def test_3d_lean_interior_tiles():
+    """A grid large enough that the fused pass has CPML-free interior tiles (the
+    specialised path without per-cell masks) next to CPML tiles in z, y and x."""
+    c = dict(CASES['d3'], Nx=96, Ny=60, Nz=100, steps=40, tear_um=1.6,
+             bead=dict(x_um=2.4, d_um=0.6, n=1.59, z_um=0.3))
+    s = H.setup_3d(c)
+    r = run_engine_3d(c, setup=s, n_dft=15)
+    o = H.run_3d(c, setup=s, n_dft=15, box=(slice(36, 44), slice(20, 34), slice(10, 90)))
+    check_fields_3d(r, o)
+    assert rel_l2(r['acc'], o['acc']) < TOL_FIELD
+    assert abs(r['P_box'] - o['P_box']) <= TOL_SCALAR * abs(o['P_box'])
+    t = run_engine_3d(c, setup=s, n_dft=15, fused=False)
+    check_fields_3d(r, t)

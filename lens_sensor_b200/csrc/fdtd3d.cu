@@ -382,7 +382,7 @@ constexpr int NW3 = NOW + 1;                 // + halo warp
 constexpr int EK = TK + 8, EJ = TJ + 2;      // E box
 constexpr int E_BYTES = EK * EJ * 4;
 constexpr int E_SLOT = ((E_BYTES + 127) / 128) * 128;
-constexpr int NSE = 4;                       // E ring depth (x-planes)
+constexpr int NSE = 3;                       // E ring depth (x-planes)
 constexpr int SHK = TK + 1, SHJ = TJ + 1;    // new H tile: z k0-1..k0+31, y j0-1..j0+TJ-1
 constexpr int SH_N = SHK * SHJ;
 constexpr int EF = E_SLOT / 4;
@@ -392,7 +392,10 @@ constexpr int HC_SLOT = 9 * HT * 4;          // Hx, Hy, Hz, ce_x, ce_y, ce_z, D_
 constexpr int OFF_HC = NSE * 3 * E_SLOT;
 constexpr int OFF_SH = OFF_HC + NHC * HC_SLOT;
 constexpr int OFF_PT = OFF_SH + ((2 * 3 * SH_N * 4 + 127) / 128) * 128;
-constexpr int OFF_BAR = OFF_PT + (((6 * (TK + 1 + TJ + 1)) * 4 + 127) / 128) * 128;
+constexpr int NT3 = NW3 * 32;                // threads of a CTA
+constexpr int OFF_HS = OFF_PT + (((6 * (TK + 1 + TJ + 1)) * 4 + 127) / 128) * 128;
+constexpr int HS_STAGE = 12 * NT3;           // H-psi of a thread's two cells, 6 components each
+constexpr int OFF_BAR = OFF_HS + 2 * HS_STAGE * 4;
 constexpr int SMEM3 = OFF_BAR + (NSE + NHC) * 8;
 static_assert(OFF_HC % 128 == 0 && HC_SLOT % 128 == 0 && (HT * 4) % 128 == 0, "TMA alignment");
 static_assert(OFF_SH % 128 == 0 && OFF_BAR % 8 == 0, "alignment");
@@ -575,28 +578,38 @@ __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep,
     return f;
 }
 
-// H-psi values of one cell: hx_z, hx_y, hy_x, hy_z, hz_y, hz_x (LENS_PSI_* 0..5)
+// Read-only global load issued where it is written: the volatile asm keeps the
+// compiler from sinking a prefetch toward its first use (the scoreboard then
+// waits at the use, after the work placed in between).
+__device__ __forceinline__ float ldg_early(const float *p) {
+    float v;
+    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+// 4-byte asynchronous global -> shared copy (zero fill when !pred: nothing is read).
+__device__ __forceinline__ void cp_async4(uint32_t dst, const float *src, bool pred) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(pred ? 4 : 0)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Stage the H-psi of one cell (hx_z, hx_y, hy_x, hy_z, hz_y, hz_x) into dst + q*NT3*4.
+template <typename IX>
+__device__ __forceinline__ void stage_hpsi(uint32_t dst, const K3 &g, IX o, unsigned f, bool xh) {
+    const bool in = f & F_IN, z = in && (f & F_ZH), y = in && (f & F_YH), x = in && xh;
+    const bool on[6] = {z, y, x, z, y, x};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) cp_async4(dst + q * NT3 * 4, on[q] ? g.pr[q] + o : g.pr[q], on[q]);
+}
+
+// psi values of one cell (E-psi: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y)
 struct P6 {
     float v[6];
 };
-
-template <typename IX>
-__device__ __forceinline__ void load_hpsi(P6 &p, const K3 &g, IX o, unsigned f, bool xh) {
-#pragma unroll
-    for (int q = 0; q < 6; ++q) p.v[q] = 0.f;
-    if (f & F_ZH) {
-        p.v[0] = __ldg(g.pr[LENS_PSI_HX_Z] + o);
-        p.v[3] = __ldg(g.pr[LENS_PSI_HY_Z] + o);
-    }
-    if (f & F_YH) {
-        p.v[1] = __ldg(g.pr[LENS_PSI_HX_Y] + o);
-        p.v[4] = __ldg(g.pr[LENS_PSI_HZ_Y] + o);
-    }
-    if (xh) {
-        p.v[2] = __ldg(g.pr[LENS_PSI_HY_X] + o);
-        p.v[5] = __ldg(g.pr[LENS_PSI_HZ_X] + o);
-    }
-}
 
 // E-psi values of one cell: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y (LENS_PSI_* 6..11)
 template <typename IX>
@@ -604,16 +617,16 @@ __device__ __forceinline__ void load_epsi(P6 &p, const K3 &g, IX o, unsigned f, 
 #pragma unroll
     for (int q = 0; q < 6; ++q) p.v[q] = 0.f;
     if (f & F_YE) {
-        p.v[0] = __ldg(g.pr[LENS_PSI_EX_Y] + o);
-        p.v[5] = __ldg(g.pr[LENS_PSI_EZ_Y] + o);
+        p.v[0] = ldg_early(g.pr[LENS_PSI_EX_Y] + o);
+        p.v[5] = ldg_early(g.pr[LENS_PSI_EZ_Y] + o);
     }
     if (f & F_ZE) {
-        p.v[1] = __ldg(g.pr[LENS_PSI_EX_Z] + o);
-        p.v[2] = __ldg(g.pr[LENS_PSI_EY_Z] + o);
+        p.v[1] = ldg_early(g.pr[LENS_PSI_EX_Z] + o);
+        p.v[2] = ldg_early(g.pr[LENS_PSI_EY_Z] + o);
     }
     if (xe) {
-        p.v[3] = __ldg(g.pr[LENS_PSI_EY_X] + o);
-        p.v[4] = __ldg(g.pr[LENS_PSI_EZ_X] + o);
+        p.v[3] = ldg_early(g.pr[LENS_PSI_EY_X] + o);
+        p.v[4] = ldg_early(g.pr[LENS_PSI_EZ_X] + o);
     }
 }
 
@@ -628,8 +641,9 @@ struct F3 {
 template <bool ST, typename IX>
 __device__ __forceinline__ F3 h_new(const K3 &g, F3 h, float ex, float ey, float ez, float exk, float eyk,
                                     float exj, float ezj, float eyn, float ezn, unsigned f, bool iok,
-                                    const float *zt, const float *yt, const PX &x, const P6 &ps, IX o,
+                                    const float *zt, const float *yt, const PX &x, const float *hs, IX o,
                                     bool wr, bool xh) {
+    // hs: this cell's staged H-psi, component q at hs[q * NT3]
     const float ch = g.ch;
     const float d1x = eyk - ey, d2x = ezj - ez;
     const float d1y = ezn - ez, d2y = exk - ex;
@@ -638,24 +652,24 @@ __device__ __forceinline__ F3 h_new(const K3 &g, F3 h, float ex, float ey, float
     if (!ST || (f & F_HX)) {
         float v = h.x + ch * (d1x - d2x);
         if (ST) {
-            if (f & F_ZH) v = v + ch * psi_u(zt[0], zt[ZN], zt[2 * ZN], ps.v[0], d1x, g.pw[LENS_PSI_HX_Z], o, wr);
-            if (f & F_YH) v = v + (-ch) * psi_u(yt[0], yt[YN], yt[2 * YN], ps.v[1], d2x, g.pw[LENS_PSI_HX_Y], o, wr);
+            if (f & F_ZH) v = v + ch * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[0 * NT3], d1x, g.pw[LENS_PSI_HX_Z], o, wr);
+            if (f & F_YH) v = v + (-ch) * psi_u(yt[0], yt[YN], yt[2 * YN], hs[1 * NT3], d2x, g.pw[LENS_PSI_HX_Y], o, wr);
         }
         h.x = v;
     }
     if (!ST || (iok && (f & F_HY))) {
         float v = h.y + ch * (d1y - d2y);
         if (ST) {
-            if (xh) v = v + ch * psi_u(x.hb, x.hc, x.hk, ps.v[2], d1y, g.pw[LENS_PSI_HY_X], o, wr);
-            if (f & F_ZH) v = v + (-ch) * psi_u(zt[0], zt[ZN], zt[2 * ZN], ps.v[3], d2y, g.pw[LENS_PSI_HY_Z], o, wr);
+            if (xh) v = v + ch * psi_u(x.hb, x.hc, x.hk, hs[2 * NT3], d1y, g.pw[LENS_PSI_HY_X], o, wr);
+            if (f & F_ZH) v = v + (-ch) * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[3 * NT3], d2y, g.pw[LENS_PSI_HY_Z], o, wr);
         }
         h.y = v;
     }
     if (!ST || (iok && (f & F_HZ))) {
         float v = h.z + ch * (d1z - d2z);
         if (ST) {
-            if (f & F_YH) v = v + ch * psi_u(yt[0], yt[YN], yt[2 * YN], ps.v[4], d1z, g.pw[LENS_PSI_HZ_Y], o, wr);
-            if (xh) v = v + (-ch) * psi_u(x.hb, x.hc, x.hk, ps.v[5], d2z, g.pw[LENS_PSI_HZ_X], o, wr);
+            if (f & F_YH) v = v + ch * psi_u(yt[0], yt[YN], yt[2 * YN], hs[4 * NT3], d1z, g.pw[LENS_PSI_HZ_Y], o, wr);
+            if (xh) v = v + (-ch) * psi_u(x.hb, x.hc, x.hk, hs[5 * NT3], d2z, g.pw[LENS_PSI_HZ_X], o, wr);
         }
         h.z = v;
     }
@@ -843,17 +857,23 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     //   after the H phase of plane i: halo old H of plane i+1, E-psi of plane i;
     //   after the E phase of plane i: H-psi of plane i+1.
     F3 hoa{0.f, 0.f, 0.f}, hob{0.f, 0.f, 0.f};
-    P6 hpa, hpb, epa, epb;
+    P6 epa, epb;
+    const int tid = w * 32 + lane;
+    const uint32_t hs_s = sbase + OFF_HS + tid * 4;  // this thread's H-psi staging slot
+    const float *hs_p = reinterpret_cast<const float *>(smem + OFF_HS) + tid;
     auto load_hold = [&](int p) {
         const IX base = (IX)p * S;
-        if (fa & F_IN) hoa = F3{__ldg(g.hx + base + oa), __ldg(g.hy + base + oa), __ldg(g.hz + base + oa)};
-        if (fb & F_IN) hob = F3{__ldg(g.hx + base + ob), __ldg(g.hy + base + ob), __ldg(g.hz + base + ob)};
+        if (fa & F_IN) hoa = F3{ldg_early(g.hx + base + oa), ldg_early(g.hy + base + oa), ldg_early(g.hz + base + oa)};
+        if (fb & F_IN) hob = F3{ldg_early(g.hx + base + ob), ldg_early(g.hy + base + ob), ldg_early(g.hz + base + ob)};
     };
-    auto load_hp = [&](int p) {
+    // H-psi of plane p into staging buffer (p - xs) & 1 (cp.async, one plane ahead)
+    auto stage_hp = [&](int p) {
         const IX base = (IX)p * S;
         const bool xh = in_strip(g.ax.h, p);
-        if (fa & F_IN) load_hpsi(hpa, g, base + oa, fa, xh);
-        if (fb & F_IN) load_hpsi(hpb, g, base + ob, fb, xh);
+        const uint32_t d = hs_s + (((unsigned)(p - xs) & 1u) * HS_STAGE) * 4;
+        stage_hpsi(d, g, base + oa, fa, xh);
+        stage_hpsi(d + 6 * NT3 * 4, g, base + ob, fb, xh);
+        cp_async_commit();
     };
     auto load_ep = [&](int p) {
         const IX base = (IX)p * S;
@@ -862,7 +882,8 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         if (fb & F_IN) load_epsi(epb, g, base + ob, fb, xe);
     };
     if (!owner) load_hold(xs);
-    if (ST) load_hp(xs);
+    if (ST) stage_hp(xs);
+    if (ST && owner) load_ep(x0);
 
     // detector boxes: per-thread float sums over the chunk, added to the FP64 totals at the end
     float bacc[LENS_MAX_BOX];
@@ -895,6 +916,8 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         const IX base = (IX)i * S;
         F3 ha{0.f, 0.f, 0.f}, hb{0.f, 0.f, 0.f};
         float exa = 0.f, exb = 0.f, nya = 0.f, nza = 0.f, nyb = 0.f, nzb = 0.f;
+        const float *hs = hs_p + (u & 1u) * HS_STAGE;  // staged H-psi of plane i (own slots)
+        if (ST) cp_async_wait_all();
         // ---------------- H(i)
         if (owner) {
             exa = eC[ea];
@@ -910,17 +933,17 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             const F3 h0b{hc[ta + TK], hc[HT + ta + TK], hc[2 * HT + ta + TK]};
             const bool wr = eon;
             ha = h_new<ST, IX>(g, h0a, exa, cya, cza, exa1, eya1, exb, czb, nya, nza, fa, iok, zta, yta, px,
-                               hpa, base + oa, wr, xh);
+                               hs, base + oa, wr, xh);
             hb = h_new<ST, IX>(g, h0b, exb, cyb, czb, exb1, eyb1, exc, ezc, nyb, nzb, fb, iok, ztb, ytb, px,
-                               hpb, base + ob, wr, xh);
+                               hs + 6 * NT3, base + ob, wr, xh);
         } else if (eon) {
             // halo cells: A on row 0 of the boxes, B on column 0 (read-only psi)
             const float *c = eC + ea;
             ha = h_new<ST, IX>(g, hoa, c[0], c[EF], c[2 * EF], c[1], c[EF + 1], c[EK], c[2 * EF + EK],
-                               eN[EF + ea], eN[2 * EF + ea], fa, iok, zta, yta, px, hpa, base + oa, false, xh);
+                               eN[EF + ea], eN[2 * EF + ea], fa, iok, zta, yta, px, hs, base + oa, false, xh);
             const float *d = eC + eb;
             hb = h_new<ST, IX>(g, hob, d[0], d[EF], d[2 * EF], d[1], d[EF + 1], d[EK], d[2 * EF + EK],
-                               eN[EF + eb], eN[2 * EF + eb], fb, iok, ztb, ytb, px, hpb, base + ob, false, xh);
+                               eN[EF + eb], eN[2 * EF + eb], fb, iok, ztb, ytb, px, hs + 6 * NT3, base + ob, false, xh);
         }
         if (owner || eon) {
             shw[sa] = ha.x;
@@ -933,7 +956,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             }
         }
         if (!owner && i + 1 < x1) load_hold(i + 1);
-        if (ST && owner && eon) load_ep(i);
+        if (ST && i + 1 < x1) stage_hp(i + 1);
         if (prod) {
             if (i + 2 <= x1) wait_e(i + 2);
             if (i + 1 < x1) wait_hc(i + 1);
@@ -989,7 +1012,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
                 }
             }
         }
-        if (ST && i + 1 < x1) load_hp(i + 1);
+        if (ST && owner && i + 1 < x1) load_ep(i + 1);
         // carry
         cya = nya; cza = nza; cyb = nyb; czb = nzb;
         hyma = ha.y; hzma = ha.z; hymb = hb.y; hzmb = hb.z;

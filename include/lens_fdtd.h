@@ -164,7 +164,9 @@ typedef struct {
 
 typedef struct {
     int nbox;
-    int box[LENS_MAX_BOX][6];    /* [x0,x1) [y0,y1) [z0,z1), applied to Ex, Ey, Ez */
+    int box[LENS_MAX_BOX][6];    /* [x0,x1) [y0,y1) [z0,z1), applied to Ex, Ey, Ez; an end
+                                    < 0 counts from each component's own end (numpy
+                                    slice(a, -b), fdtd3d_core.py:1139-1142)           */
     double *box_acc;             /* nbox sums of Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481) */
     int dft_n0, dft_n1;
     float *dft[3];               /* per component (or NULL): (nx,ny,pitch) x {re,im} */

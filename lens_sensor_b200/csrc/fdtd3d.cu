@@ -203,6 +203,17 @@ __device__ __forceinline__ void plane3(const LensEpi3D &ep, const LensStepTable 
     a[3 * vol] += (double)h * (double)tab.ph[2 * q + 1];
 }
 
+// End of a detector-box range on an axis of extent `ext` with numpy slice
+// semantics: a negative end counts from that component's own end
+// (fdtd3d_core.py:1139-1142 uses slice(n_sp, -n_sp) on Ex, Ey and Ez alike).
+__host__ __device__ __forceinline__ int box_end(int e, int ext) { return e < 0 ? ext + e : (e < ext ? e : ext); }
+
+// Is (i, j, k) of component c (0 Ex, 1 Ey, 2 Ez) inside box bx?
+__device__ __forceinline__ bool in_box(const int *bx, int c, int i, int j, int k, int nx, int ny, int nz) {
+    return i >= bx[0] && i < box_end(bx[1], nx - (c == 0)) && j >= bx[2] && j < box_end(bx[3], ny - (c == 1)) &&
+           k >= bx[4] && k < box_end(bx[5], nz - (c == 2));
+}
+
 // Epilogue of one cell after its E update.  All 32 lanes of a warp must call it.
 //   detector boxes: sum of Ex^2+Ey^2+Ez^2 in FP64 (fdtd3d_core.py:477-481)
 //   DFT windows:    complex float32 sums of each selected component (the
@@ -217,16 +228,13 @@ __device__ __forceinline__ void epi_cell(const K3 &g, const LensStepTable &tab, 
         const int bk0 = blockIdx.x * BK, bj0 = blockIdx.y * BJ;
         for (int b = 0; b < ep.nbox; ++b) {
             const int *bx = ep.box[b];
-            if (i < bx[0] || i >= bx[1] || bx[3] <= bj0 || bx[2] >= bj0 + BJ || bx[5] <= bk0 ||
-                bx[4] >= bk0 + BK)
+            if (i < bx[0] || i >= box_end(bx[1], nx) || box_end(bx[3], ny) <= bj0 || bx[2] >= bj0 + BJ ||
+                box_end(bx[5], nz) <= bk0 || bx[4] >= bk0 + BK)
                 continue;  // block-uniform
-            const bool inb = j >= bx[2] && j < bx[3] && k >= bx[4] && k < bx[5];
             double v = 0.0;
-            if (inb) {
-                if (vx) v += (double)(e.x * e.x);
-                if (vy) v += (double)(e.y * e.y);
-                if (vz) v += (double)(e.z * e.z);
-            }
+            if (vx && in_box(bx, 0, i, j, k, nx, ny, nz)) v += (double)(e.x * e.x);
+            if (vy && in_box(bx, 1, i, j, k, nx, ny, nz)) v += (double)(e.y * e.y);
+            if (vz && in_box(bx, 2, i, j, k, nx, ny, nz)) v += (double)(e.z * e.z);
             warp_atomic_add(ep.box_acc + b, v);
         }
     }
@@ -551,7 +559,7 @@ enum : unsigned {
     F_EYV = 128u, F_EZV = 256u,                     // Ey, Ez exist (j < ny-1, k < nz-1)
     F_PJ = 512u, F_PK = 1024u,                      // on a PEC face in y / z
     F_ZH = 2048u, F_YH = 4096u, F_ZE = 8192u, F_YE = 16384u,  // in a z / y psi strip (H / E)
-    F_BOX0 = 1u << 16                               // bit 16 + b: inside detector box b (y, z)
+    F_BOX0 = 1u << 16                               // bit 16 + 3b + c: component c inside box b (y, z)
 };
 
 __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep, int j, int k) {
@@ -573,8 +581,10 @@ __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep,
     if (in_strip(g.az.e, k)) f |= F_ZE;
     if (in_strip(g.ay.e, j)) f |= F_YE;
     for (int b = 0; b < LENS_MAX_BOX; ++b)
-        if (b < ep.nbox && j >= ep.box[b][2] && j < ep.box[b][3] && k >= ep.box[b][4] && k < ep.box[b][5])
-            f |= F_BOX0 << b;
+        for (int c = 0; c < 3; ++c)
+            if (b < ep.nbox && j >= ep.box[b][2] && j < box_end(ep.box[b][3], ny - (c == 1)) &&
+                k >= ep.box[b][4] && k < box_end(ep.box[b][5], nz - (c == 2)))
+                f |= F_BOX0 << (3 * b + c);
     return f;
 }
 
@@ -1005,9 +1015,13 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
                 // detector boxes: Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481; invalid components are zero)
 #pragma unroll
                 for (int b = 0; b < LENS_MAX_BOX; ++b) {
-                    if (b < ep.nbox && i >= ep.box[b][0] && i < ep.box[b][1]) {
-                        if (fa & (F_BOX0 << b)) bacc[b] += (Ea.x * Ea.x + Ea.y * Ea.y) + Ea.z * Ea.z;
-                        if (fb & (F_BOX0 << b)) bacc[b] += (Eb.x * Eb.x + Eb.y * Eb.y) + Eb.z * Eb.z;
+                    if (b < ep.nbox && i >= ep.box[b][0] && i < box_end(ep.box[b][1], nx)) {
+                        const bool ix = i < box_end(ep.box[b][1], nx - 1);  // Ex is one plane shorter
+                        const unsigned m = F_BOX0 << (3 * b);
+                        bacc[b] += ((ix && (fa & m) ? Ea.x * Ea.x : 0.f) + ((fa & (m << 1)) ? Ea.y * Ea.y : 0.f)) +
+                                   ((fa & (m << 2)) ? Ea.z * Ea.z : 0.f);
+                        bacc[b] += ((ix && (fb & m) ? Eb.x * Eb.x : 0.f) + ((fb & (m << 1)) ? Eb.y * Eb.y : 0.f)) +
+                                   ((fb & (m << 2)) ? Eb.z * Eb.z : 0.f);
                     }
                 }
             }

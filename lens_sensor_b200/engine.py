@@ -388,3 +388,26 @@ class Epi3D:
             aH = torch.complex(a[2, :nj, :nk], a[3, :nj, :nk])
             tot += sign * 0.5 * float(torch.real(torch.sum(aE * torch.conj(aH))))
         return tot * (2.0 / n_acc) ** 2
+
+    def conv_change(self, n_last, n_prev):
+        """||a - b|| / ||a|| of the convergence planes a = last / n_last, b = prev / n_prev
+        (fdtd3d_core.py:1159-1162); nan without a previous window."""
+        if self.conv_last is None or n_prev <= 0 or n_last <= 0:
+            return float('nan')
+        a = _kahan_value(self.conv_last) / n_last
+        b = _kahan_value(self.conv_prev) / n_prev
+        return float(torch.linalg.norm(a - b)) / max(float(torch.linalg.norm(a)), 1e-30)
+
+    def restart_dft(self, window):
+        """Open a new DFT window [n0, n1) after a failed convergence check
+        (fdtd3d_core.py:1162-1170): the last convergence plane becomes the previous
+        one; the volume DFTs, the flux planes and the last plane restart from zero."""
+        self.conv_prev, self.conv_last = self.conv_last, self.conv_prev
+        self.conv_last.zero_()
+        for d in self.dft:
+            if d is not None:
+                d.zero_()
+        self.plane_acc.zero_()
+        self.s.conv_prev, self.s.conv_last = _ptr(self.conv_prev), _ptr(self.conv_last)
+        self.s.dft_n0, self.s.dft_n1 = int(window[0]), int(window[1])
+        self.s.prev_n0 = self.s.prev_n1 = 0

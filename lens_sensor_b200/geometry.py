@@ -386,7 +386,7 @@ def _tm_coefficients(sp, eps, sig, ys, in_wg, bp):
 class Sphere:
     x_um: float
     d_um: float
-    n: float = 1.59
+    n: complex = 1.59                  # complex: absorbing bead (lossy stacks)
     y_um: Optional[float] = None       # default -r: resting on the core bottom
     z_um: float = 0.0
 
@@ -406,6 +406,18 @@ class Spec3D:
     lam_nm: float = 850.0
     waist_um: float = 3.0
     ramp_periods: Optional[float] = None
+    # run_3d options (fdtd3d_core.py:793-807)
+    waist_z_um: Optional[float] = None   # default: waist_um
+    offset_y_um: float = 0.0             # source centre offsets from (t_wg/2, 0)
+    offset_z_um: float = 0.0
+    tilt_deg: float = 0.0                # beam tilt in the x-y plane
+    vcsel_distance_um: float = 0.0       # beam waist in front of the entry facet
+    n_sponge: Optional[int] = None       # absorber/source offset cells (default from sponge_um)
+    sponge_um: float = 1.2
+    end_facet_um: float = 0.0            # air over the last end_facet_um of the length
+    wg_width_um: Optional[float] = None  # rectangular channel: core only for |z| < width/2
+    n_clad_side: float = 1.0             # index beside the channel core
+    pec_faces: Tuple[str, ...] = ()      # faces without CPML (PEC mirrors)
 
     @property
     def dx(self):
@@ -417,9 +429,10 @@ class Spec3D:
 
     @property
     def n_sp(self):
-        """Sponge thickness in cells (fdtd3d_core.py:262-275), which fixes the source plane."""
+        """Sponge thickness in cells (fdtd3d_core.py:381-396), which fixes the source plane."""
         dx_um = self.dx_nm / 1000.0
-        n = max(8, int(np.ceil(1.2 / dx_um)))
+        n = int(self.n_sponge) if self.n_sponge else int(np.ceil(float(self.sponge_um) / dx_um))
+        n = max(8, n)
         return min(n, max(8, min(self.nx, self.ny, self.nz) // 6))
 
     @property
@@ -456,17 +469,27 @@ def build_3d(sp: Spec3D):
     ys = y0_um + np.arange(Ny) * dx_um
     zs = z0_um + np.arange(Nz) * dx_um
     xs = np.arange(Nx) * dx_um
-    air = air_path_um(0.0, dx_um)
+    air = air_path_um(sp.vcsel_distance_um, dx_um)
     x_facet_um = sp.src_ix * dx_um + air
-    # column types: 1 = core stack, 3 = air in front of the entry facet
+    # column types (fdtd3d_core.py:248-261): 1 core stack, 2 channel cladding beside
+    # the core, 3 air (in front of the entry facet, over the end facet)
     T = np.full((Nx, Nz), 1, dtype=np.int8)
+    channel = sp.wg_width_um is not None and 0 < sp.wg_width_um < Nz * dx_um
+    if channel:
+        T[:, np.abs(zs) > sp.wg_width_um / 2.0] = 2
+    if sp.end_facet_um and sp.end_facet_um > 0:
+        T[xs >= (Nx * dx_um - sp.end_facet_um), :] = 3
     T[xs < x_facet_um, :] = 3
     col = column_average(ys, dx_um, st.eps_of_y(1e-6, core=True))
     cols_node = {1: col, 3: np.full(Ny, N_AIR ** 2, dtype=col.dtype)}
+    if channel:   # core rows (0 <= y <= t_wg) set to the cladding index at the nodes
+        c2 = col.copy()
+        c2[(ys >= 0.0) & (ys <= st.t_wg_um)] = sp.n_clad_side ** 2
+        cols_node[2] = c2
     # harmonic Ey columns for the four column types (fdtd3d_core.py:239-261)
     hcol = lambda core, nc=None: column_average(ys[:-1], dx_um, lambda y: np.real(st.eps_of_y(1e-6, core, nc)(y)),
                                                 harmonic=True, shift=0.5 * dx_um).astype(np.float64)
-    hcols = np.stack([hcol(False), hcol(True), hcol(True, N_AIR), np.full(Ny - 1, N_AIR ** 2)])
+    hcols = np.stack([hcol(False), hcol(True), hcol(True, sp.n_clad_side), np.full(Ny - 1, N_AIR ** 2)])
     c0f, c1f = F32(dt / (EPS0 * dx)), F32(np.pi * C0 / lam_m * dt)
 
     def inv_damp(e_complex_or_real):
@@ -506,9 +529,9 @@ def build_3d(sp: Spec3D):
             box[np.broadcast_to((tb == t)[:, None, :], box.shape)] = np.broadcast_to(
                 cv[None, j0:j1, None], box.shape)[np.broadcast_to((tb == t)[:, None, :], box.shape)]
         patches.append(dict(bg=box.real.astype(np.float64), i0=i0, j0=j0, k0=k0, xs=xs[i0:i1],
-                            ys=ys[j0:j1], zs=zs[k0:k1], xc=xc, yc=yc, zc=zc, r=r, n=bd.n))
+                            ys=ys[j0:j1], zs=zs[k0:k1], xc=xc, yc=yc, zc=zc, r=r, n=complex(bd.n).real))
         _blend(box, sphere_fraction(xs[i0:i1], ys[j0:j1], zs[k0:k1], xc, yc, zc, r, dx_um),
-               complex(bd.n, 0.0) if lossy else bd.n)
+               complex(bd.n) if lossy else complex(bd.n).real)
         iv, dv = inv_damp(box)
         inv[i0:i1, j0:j1, k0:k1] = iv
         if lossy:
@@ -559,20 +582,31 @@ def build_3d(sp: Spec3D):
             blk[sel] = val[sel]
             tgt[sl] = blk.astype(F32)
     da = None if not lossy else tuple(_stagger(D, ax) for ax in range(3))
-    # source on the driven component (fdtd3d_core.py:375-411)
+    # source on the driven component (fdtd3d_core.py:494-530, vcsel.py:110-123): a
+    # Gaussian spot in air (n = 1) in front of the facet, waist vcsel_distance_um
+    # before the facet, centred at (t_wg/2 + offset_y, offset_z), tilted in x-y
     pol = sp.pol
     Nj, Nk = (Ny - 1, Nz) if pol == 'p' else (Ny, Nz - 1)
-    yv = y0_um + (np.arange(Nj) + (0.5 if pol == 'p' else 0.0)) * dx_um - st.t_wg_um / 2
-    zv = z0_um + (np.arange(Nk) + (0.5 if pol == 's' else 0.0)) * dx_um
-    zprop = 0.0 - air
-    wy, Ry = beam(zprop, sp.waist_um, sp.lam_nm, 1.0)
-    wz, Rz = beam(zprop, sp.waist_um, sp.lam_nm, 1.0)
-    amp = math.sqrt((sp.waist_um / wy) * (sp.waist_um / wz)) * np.exp(-(yv[:, None] / wy) ** 2 - (zv[None, :] / wz) ** 2)
-    ph = _beam_phase(yv[:, None], Ry, sp.lam_nm, 1.0, 0.0) + np.zeros((1, Nk))
+    wy0 = sp.waist_um
+    wz0 = sp.waist_um if sp.waist_z_um is None else sp.waist_z_um
+    yc = st.t_wg_um / 2 + sp.offset_y_um
+    zc = sp.offset_z_um
+    yv = y0_um + (np.arange(Nj) + (0.5 if pol == 'p' else 0.0)) * dx_um - yc
+    zv = z0_um + (np.arange(Nk) + (0.5 if pol == 's' else 0.0)) * dx_um - zc
+    zprop = float(sp.vcsel_distance_um or 0.0) - air
+    wy, Ry = beam(zprop, wy0, sp.lam_nm, 1.0)
+    wz, Rz = beam(zprop, wz0, sp.lam_nm, 1.0)
+    amp = math.sqrt((wy0 / wy) * (wz0 / wz)) * np.exp(-(yv[:, None] / wy) ** 2 - (zv[None, :] / wz) ** 2)
+    ph = _beam_phase(yv[:, None], Ry, sp.lam_nm, 1.0, sp.tilt_deg) + np.zeros((1, Nk))
     if math.isfinite(Rz):
         ph = ph - (2 * math.pi / (sp.lam_nm * 1e-3)) * zv[None, :] ** 2 / (2.0 * Rz)
-    kdx = huygens_kdx(sp.lam_nm, dx, C0 * dt, 1.0, 0.0)
+    kdx = huygens_kdx(sp.lam_nm, dx, C0 * dt, 1.0, sp.tilt_deg)
     a, p1, p2 = huygens_arrays(amp, ph, kdx)
-    src = dict(ix=sp.src_ix, amp=a, ph1=p1, ph2=p2, omega=2 * np.pi * C0 / lam_m)
-    cpml = [cpml_axis(N, sp.npml, sp.npml, dx, dt, lam_m) for N in (Nx, Ny, Nz)]
+    src = dict(ix=sp.src_ix, amp=a, ph1=p1, ph2=p2, omega=2 * np.pi * C0 / lam_m, air_um=air,
+               j_src=min(max(int(round((yc - y0_um) / dx_um)), 0), Nj - 1),
+               k_src=min(max(int(round((zc - z0_um) / dx_um)), 0), Nk - 1))
+    # CPML on the absorbing faces, none on the PEC mirrors (boundaries3d.py:262-302)
+    pf = set(sp.pec_faces or ())
+    cpml = [cpml_axis(N, 0 if lo in pf else sp.npml, 0 if hi in pf else sp.npml, dx, dt, lam_m)
+            for N, lo, hi in ((Nx, 'xmin', 'xmax'), (Ny, 'ymin', 'ymax'), (Nz, 'zmin', 'zmax'))]
     return dict(ce=tuple(ce), da=da, src=src, cpml=cpml, x_facet_um=x_facet_um, T=T)

@@ -69,7 +69,8 @@ class Solve3D:
         sh = guard_in_plane(ci, max(sp.src_ix, int(round(g['x_facet_um'] / dx_um))), Nx) - ci
         iin0, iin1 = iin0 + sh, min(Nx, iin1 + sh)
         nsp = sp.n_sp
-        self.boxes = [(iin0, iin1, j_wg0, j_wg1, nsp, Nz - nsp), (iout0, iout1, j_wg0, j_wg1, nsp, Nz - nsp)]
+        # z range slice(n_sp, -n_sp) of each component (fdtd3d_core.py:1139-1142)
+        self.boxes = [(iin0, iin1, j_wg0, j_wg1, nsp, -nsp), (iout0, iout1, j_wg0, j_wg1, nsp, -nsp)]
         self.planes = {'in': max(1, (iin0 + iin1) // 2), 'out': max(1, (iout0 + iout1) // 2),
                        'src_up': sp.src_ix - 1, 'src_dn': sp.src_ix + 3}
         self.comps = tuple(comps) if comps is not None else (sp.src_comp,)

@@ -103,3 +103,107 @@ class Epi2D:
 
     def flux(self, name, n_acc):
         return self.flux_acc.flux(name)
+
+
+# ----------------------------------------------------------------------------- 3D
+_COMP = {0: 'Ex', 1: 'Ey', 2: 'Ez'}
+_FACES = ('xmin', 'xmax', 'ymin', 'ymax', 'zmin', 'zmax')
+
+
+class Grid3D:
+    """3D stand-in: oracle FP32 stepping in the reference loop order
+    (fdtd3d_core.py:1106-1127; CPML step, PEC, source)."""
+
+    def __init__(self, nx, ny, nz, dx, dt, ce, da, cpml, src, src_comp=1, pec=(1,) * 6, device=None,
+                 fused=True):
+        self.nx, self.ny, self.nz, self.dx, self.dt = nx, ny, nz, dx, dt
+        h = O.Huygens.__new__(O.Huygens)
+        h.ix, h.omega = int(src['ix']), float(src['omega'])
+        h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
+        self.src_comp = src_comp
+        faces = tuple(f for f, on in zip(_FACES, pec) if on)
+        self.g = O.Grid3D(nx, ny, nz, dx, dt, cpml, ce, da, h, _COMP[src_comp], F32, faces=faces)
+
+    def view(self, name):
+        return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
+
+    def step(self, table, n0, nsteps, epi=None, stream=None):
+        for n in range(n0, n0 + nsteps):
+            t = n * self.dt
+            self.g.step(n, float(table.envelope(t)))
+            if epi is not None:
+                epi.after(n, t, self.g)
+
+    def accum_e2(self, iavg, target=None, stream=None):
+        O.accum_e2(iavg.numpy(), self.g.Ex, self.g.Ey, self.g.Ez)
+
+    def check_flag(self):
+        pass
+
+
+class Epi3D:
+    """3D stand-in: the reference's per-step epilogue (fdtd3d_core.py:1139-1175):
+    detector boxes, complex64 DFT of the driven component, plane-flux DFT and the
+    convergence planes at z index kc."""
+
+    def __init__(self, grid, boxes=(), dft=None, comps=(1,), planes=(), conv=None, iavg=False):
+        self.grid = grid
+        cshape = getattr(grid.g, _COMP[grid.src_comp]).shape
+
+        def sl(a, b):
+            return slice(a, b if b != 0 else None)
+        self.boxes = [(sl(b[0], b[1]), sl(b[2], b[3]), sl(b[4], b[5])) for b in boxes]
+        self.box = np.zeros(len(self.boxes), np.float64)
+        self.win = tuple(dft)
+        self.comps = tuple(comps)
+        self.acc = {c: np.zeros(getattr(grid.g, _COMP[c]).shape, np.complex64) for c in comps}
+        self.planes = dict(planes)
+        self.kc, self.prev_win = (conv[0], tuple(conv[1])) if conv is not None else (None, (0, 0))
+        self.pl_a = np.zeros(cshape[:2], np.complex64)
+        self.pl_b = np.zeros(cshape[:2], np.complex64)
+        self._iavg = np.zeros(cshape, F32)
+        self.iavg = torch.from_numpy(self._iavg)
+        self.flux_acc = None
+        self._omega = None
+
+    def after(self, n, t, g):
+        if self._omega is None:
+            self._omega = float(g.src.omega)
+            self.flux_acc = O.PlaneFlux(self._omega, g.dt, F32)
+        for q, bx in enumerate(self.boxes):
+            self.box[q] += g.box_e2(*bx)
+        F = getattr(g, _COMP[self.grid.src_comp])
+        if self.win[0] <= n < self.win[1]:
+            ph = np.exp(-1j * self._omega * t)
+            for c in self.comps:
+                self.acc[c] += getattr(g, _COMP[c]).astype(np.complex64) * ph
+            for k, il in self.planes.items():
+                self.flux_acc.add(k, t, g.flux_pairs(il))
+            if self.kc is not None:
+                self.pl_b += F[:, :, self.kc].astype(np.complex64) * ph
+        elif self.kc is not None and self.prev_win[0] <= n < self.prev_win[1]:
+            self.pl_a += F[:, :, self.kc].astype(np.complex64) * np.exp(-1j * self._omega * t)
+
+    @property
+    def box_acc(self):
+        return torch.from_numpy(self.box.copy())
+
+    def phasor(self, comp=1):
+        return torch.from_numpy(self.acc[comp].astype(np.complex128))
+
+    def flux(self, name, n_acc):
+        return self.flux_acc.flux(name)
+
+    def conv_change(self, n_last, n_prev):
+        if n_prev <= 0 or n_last <= 0:
+            return float('nan')
+        a = self.pl_b / n_last
+        b = self.pl_a / n_prev
+        return float(np.linalg.norm(a - b) / max(float(np.linalg.norm(a)), 1e-30))
+
+    def restart_dft(self, window):
+        self.pl_a, self.pl_b = self.pl_b, np.zeros_like(self.pl_b)
+        for c in self.acc:
+            self.acc[c][...] = 0
+        self.flux_acc = O.PlaneFlux(self._omega, self.grid.dt, F32)
+        self.win, self.prev_win = tuple(window), (0, 0)

@@ -17,6 +17,7 @@ Outputs:
                                        answers at the reference HEAD
   dropin_2d.json                       run_beads + save_results outputs (NPZ / PKL
                                        summaries) of three whole-driver cases
+  dropin_3d.json                       the same for run_3d + save_results_3d
 
 `python tests/golden/make_golden.py dropin` stops after the two JSON files.
 """
@@ -319,6 +320,66 @@ def dropin_2d():
     return out
 
 
+# ------------------------------------------------------------- drop-in run_3d
+# Whole-driver cases: fdtd3d_core.run_3d + save_results_3d (CPML, CW).  'golden3d' is
+# the reference's characterization case (TE, legacy tear film); 'tm_stack' a TM run on
+# a custom absorbing stack with a displaced bead; 'te_kappa' KAPPA losses with a lipid
+# layer, astigmatic tilted offset source, input gap and end facet.
+DROPIN_3D = dict(
+    golden3d=dict(kw=dict(label='golden3d', wg_n=1.491, lx_um=4.0, air_um=1.0, tear_um=2.0, lz_um=2.0,
+                          dx_nm=100.0, t_wg_um=1.0, t_aq_um=1.0, t_mu_um=0.5, lam_nm=850.0, n_snapshots=2,
+                          steps_factor=1.0, vcsel_waist_um=1.0, vcsel_waist_z_um=1.0,
+                          bead=dict(x_um=2.0, d_um=0.5, n=1.59), n_sponge=8), kappa={}),
+    tm_stack=dict(kw=dict(label='tm_stack', wg_n=1.49, lx_um=4.2, air_um=0.8, lz_um=2.4, dx_nm=100.0,
+                          t_wg_um=0.9, lam_nm=850.0, n_snapshots=3, steps_factor=1.0, vcsel_waist_um=1.2,
+                          vcsel_waist_z_um=0.9, bead=dict(x_um=2.3, d_um=0.6, n=1.59, z_um=0.2),
+                          n_sponge=8, polarization='p',
+                          stack=[dict(name='Aqueous', t_um=1.2, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                                 dict(name='Mucin', t_um=0.4, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+                  kappa={}),
+    te_kappa=dict(kw=dict(label='te_kappa', wg_n=1.49, lx_um=4.0, air_um=0.8, tear_um=2.2, lz_um=2.0,
+                          dx_nm=100.0, t_wg_um=1.0, t_lip_um=0.2, t_aq_um=0.9, t_mu_um=0.4, lam_nm=850.0,
+                          n_snapshots=2, steps_factor=1.0, vcsel_waist_um=1.1, vcsel_waist_z_um=0.8,
+                          vcsel_tilt_deg=3.0, vcsel_offset_y_um=0.1, vcsel_offset_z_um=-0.1,
+                          input_gap_um=1.5, end_facet_um=0.5, bead=dict(x_um=2.1, d_um=0.5, n=1.59),
+                          n_sponge=8), kappa=dict(aq=0.003, wg=0.0005)),
+)
+
+
+def dropin_3d():
+    """Run the reference 3D driver end to end for DROPIN_3D and summarise its outputs."""
+    import glob
+    import pickle
+    out = {}
+    for name, c in DROPIN_3D.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_dropin3d_')
+        old_k = d3.KAPPA
+        try:
+            os.chdir(tmp)
+            d3.KAPPA = dict(c['kappa'])
+            r = d3.run_3d(**c['kw'])
+            d3.save_results_3d(r)
+            files = {}
+            for f in sorted(glob.glob('results/*.npz')):
+                z = np.load(f)
+                files[os.path.basename(f).replace(c['kw']['label'], '{label}')] = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+        finally:
+            d3.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        kw = {k: v for k, v in c['kw'].items() if k != 'stack'}
+        out[name] = dict(kw=kw, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         npz=files, pkl=scal)
+    return out
+
+
 def main():
     ch = characterization()          # first: the cases below change module globals
     with open(os.path.join(OUT, 'characterization.json'), 'w') as f:
@@ -327,6 +388,9 @@ def main():
     with open(os.path.join(OUT, 'dropin_2d.json'), 'w') as f:
         json.dump(dropin_2d(), f, indent=1)
     print('wrote dropin_2d.json')
+    with open(os.path.join(OUT, 'dropin_3d.json'), 'w') as f:
+        json.dump(dropin_3d(), f, indent=1)
+    print('wrote dropin_3d.json')
     if 'dropin' in sys.argv[1:]:
         return
     for name, c in CASE_2D.items():

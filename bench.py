@@ -170,6 +170,77 @@ def run_e2e(spec, steps_total, cells, ws, pg):
     return out
 
 
+def run_batched(plain_sample=16):
+    """Config 2: the 256-instance uneven 2D TE/TM sweep (4000 steps each).
+
+    plain   instances one at a time through the single-grid engine (the drop-in
+            run_beads path, lens_te2d_step / lens_tm2d_step), on a seeded sample of
+            `plain_sample` instances spread over the sweep;
+    batched the whole sweep through batch2d.Sweep (autotuned tile and group
+            budget, one CUDA graph per group), FP32 storage, then FP16 storage
+            with each instance's phasor error against the FP32 run.
+    Throughput is cell-updates/s over the whole timed region (device events)."""
+    import torch
+    from lens_sensor_b200 import batch2d as B
+    from lens_sensor_b200 import engine as E
+    from lens_sensor_b200.workloads import config2
+    specs, steps = config2()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    sw = B.Sweep(specs, steps, 'f32')
+    tuned = sw.autotune()
+    for g in sw.groups:
+        g.capture(sw.table)
+    e0, e1 = ev(), ev()
+    e0.record()
+    launches = sw.run()
+    e1.record()
+    torch.cuda.synchronize()
+    t_b = e0.elapsed_time(e1) * 1e-3
+    cells = sw.cells()
+    ref = [r['phasor'] for r in sw.results()]
+    K = [r['K'] for r in sw.results()]
+    idx = list(range(0, len(specs), max(1, len(specs) // plain_sample)))[:plain_sample]
+    pc = 0
+    e0.record()
+    for q in idx:
+        sp, geo = specs[q], sw.insts[q].geo
+        coef = {k: geo[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if k in geo}
+        g = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, geo['cx'], geo['cy'], geo['src'])
+        epi = E.Epi2D(g, dft=sw.insts[q].window)
+        g.step(sw.table, 0, steps, epi)
+        pc += sp.nx * sp.ny
+    e1.record()
+    torch.cuda.synchronize()
+    t_p = e0.elapsed_time(e1) * 1e-3
+    geos = [q.geo for q in sw.insts]
+    by, budget = sw.by, sw.budget
+    del sw
+    torch.cuda.empty_cache()
+    sh = B.Sweep(specs, steps, 'f16', by=by, budget=budget, geos=geos)
+    for g in sh.groups:
+        g.capture(sh.table)
+    e0.record()
+    sh.run()
+    e1.record()
+    torch.cuda.synchronize()
+    t_h = e0.elapsed_time(e1) * 1e-3
+    err = [float((r['phasor'] - ref[q]).abs().norm() / max(float(ref[q].abs().norm()), 1e-300))
+           for q, r in enumerate(sh.results())]
+    del sh
+    torch.cuda.empty_cache()
+    plain = pc * steps / t_p
+    f32 = cells * steps / t_b
+    f16 = cells * steps / t_h
+    return dict(workload='config2: 256 uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
+                         '12-cell CPML, 4000 steps, seeded tear-film / lipid / bead sweep',
+                unit=UNIT, cells_total=cells, steps=steps, plain=plain,
+                plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time',
+                batched_f32=f32, batched_f16=f16, batched_vs_plain=f32 / plain, f16_vs_plain=f16 / plain,
+                tile_rows=4 * by, group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
+                f16_phasor_err_vs_f32_max=max(err), f16_phasor_err_vs_f32_median=float(np.median(err)),
+                K_median=float(np.median(K)))
+
+
 def ours_arm(args):
     import torch
     ws, rank, local = dist_env()
@@ -248,6 +319,7 @@ def ours_arm(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(spec, steps_total, cells, ws, pg)
+    batched = run_batched() if (ws == 1 and not args.no_batch) else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, info = cpu_baseline(spec)
@@ -266,7 +338,7 @@ def ours_arm(args):
                                   launch_ms=t_launch * 1e3,
                                   mix_alg_bytes_per_cell_update=alg / (cells * K),
                                   mix_achieved=alg / (ms * 1e-3) / 1e9),
-                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches)
+                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches, batched=batched)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -281,6 +353,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
+    ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (config 2)')
     args = ap.parse_args()
     if args.impl == 'reference':
         reference_arm(args)

@@ -129,6 +129,46 @@ int lens_te2d_step(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D 
 int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
                    int n0, int nsteps, void *stream);
 
+/* ------------------------------------------------------- batched 2D solves
+ * Many independent 2D solves of uneven sizes (TE and TM mixed) advanced together:
+ * one launch per half step covers every tile of every instance, so a sweep of
+ * small grids runs at the memory rate instead of the launch rate, and a span of
+ * steps can be captured into one CUDA graph by the caller.  Field storage is
+ * FP32, FP16 or BF16 for the whole batch (arithmetic is FP32 throughout);
+ * coefficients, CPML psi and the DFT stay FP32.  The per-cell update is the one
+ * of lens_te2d_step / lens_tm2d_step; the epilogue is the node-field DFT
+ * (Ez for TE, Ey averaged onto the nodes for TM) over [dft_n0, dft_n1).    */
+#define LENS_F32 0
+#define LENS_F16 1
+#define LENS_BF16 2
+
+typedef struct {
+    int pol;                     /* 0 TE (Ez, Hx, Hy), 1 TM (Ex, Ey, Hz)       */
+    int nx, ny, pitch;
+    void *f[3];                  /* TE ez, hx, hy / TM ex, ey, hz (storage type) */
+    const float *c[4];           /* TE ce_e, ce_h / TM ca_x, ca_y, da_x, da_y   */
+    float ch;
+    LensAxis ax, ay;
+    float *psi[4];               /* TE hxy, hyx, ezx, ezy / TM hzx, hzy, exy, eyx
+                                    (shapes as in LensTE2D / LensTM2D)          */
+    int pec[4];
+    LensSource src;              /* drives Ez (TE) or Ey (TM)                   */
+    int dft_n0, dft_n1;
+    float *dft;                  /* (nx, pitch) x {re, im} or NULL              */
+} LensInst2D;
+
+/* Block plan of a batch for tiles of 32 columns x 4*by rows: writes blk[0..ninst]
+ * (first block of each instance) and, when owner is not NULL, owner[b] (the
+ * instance of block b, one entry per block); returns the block count, or < 0. */
+int lens_batch2d_plan(const LensInst2D *inst, int ninst, int by, int *blk, int *owner);
+
+/* Advance every instance by nsteps from step n0.  inst_host / inst_dev: the
+ * same instance array in host and device memory; blk_dev / owner_dev: the
+ * plan's tables in device memory; storage: LENS_F32 / LENS_F16 / LENS_BF16. */
+int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
+                      const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
+                      int n0, int nsteps, void *stream);
+
 /* ---------------------------------------------------------------- 3D grid */
 /* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
  * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same
@@ -191,8 +231,8 @@ int lens_version(void);
 const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
- * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D.
- * Writes min(n, 9) entries and returns 9 (bindings check their mirrors). */
+ * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D.
+ * Writes min(n, 10) entries and returns 10 (bindings check their mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

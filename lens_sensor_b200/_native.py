@@ -82,7 +82,17 @@ class Epi3D(ctypes.Structure):
                 ('nplane', c_int), ('plane', c_int * MAX_PLANE), ('plane_acc', c_void_p)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D)
+F32, F16, BF16 = 0, 1, 2   # LENS_F32 / LENS_F16 / LENS_BF16 field storage
+
+
+class Inst2D(ctypes.Structure):
+    _fields_ = [('pol', c_int), ('nx', c_int), ('ny', c_int), ('pitch', c_int),
+                ('f', c_void_p * 3), ('c', c_void_p * 4), ('ch', c_float),
+                ('ax', Axis), ('ay', Axis), ('psi', c_void_p * 4), ('pec', c_int * 4),
+                ('src', Source), ('dft_n0', c_int), ('dft_n1', c_int), ('dft', c_void_p)]
+
+
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
@@ -91,6 +101,9 @@ SIGNATURES = {
     'lens_tm2d_step': (c_int, [POINTER(TM2D), POINTER(StepTable), POINTER(Epi2D), c_int, c_int, c_void_p]),
     'lens_fdtd3d_step': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), c_int, c_int, c_void_p]),
     'lens_fdtd3d_accum_e2': (c_int, [POINTER(Grid3D), c_int, c_void_p, c_void_p]),
+    'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
+    'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                  POINTER(StepTable), c_int, c_int, c_void_p]),
     'lens_version': (c_int, []),
     'lens_status_string': (ctypes.c_char_p, [c_int]),
     'lens_abi_sizes': (c_int, [POINTER(c_int), c_int]),
@@ -116,8 +129,8 @@ def load(path=LIB_PATH):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    sizes = (c_int * 9)()
-    lib.lens_abi_sizes(sizes, 9)
+    sizes = (c_int * len(MIRRORS))()
+    lib.lens_abi_sizes(sizes, len(MIRRORS))
     mine = [ctypes.sizeof(m) for m in MIRRORS]
     if list(sizes) != mine:
         raise LensError(f'ABI mismatch between liblens_fdtd.so {list(sizes)} and bindings {mine}')

@@ -1,0 +1,249 @@
+"""Batched 2D solves: many uneven TE/TM instances advanced together.
+
+A sweep (tear-film thickness, bead size and position, polarisation) is a list
+of geometry.Spec2D.  Instances are packed into groups whose resident state
+fits a working-set budget (so a group's fields can stay in the 126 MB L2 across
+steps); each group runs its whole schedule as ONE CUDA graph of batched
+launches (lens_batch2d_step: one launch per half step for every tile of every
+instance in the group).  Field storage is FP32, FP16 or BF16 (arithmetic is
+FP32 throughout; coefficients, CPML psi and the DFT stay FP32).
+
+Per instance the output is the CW phasor of the node field (Ez for TE, Ey on
+the nodes for TM) over the last 8 periods (fdtd2d_core.py:757-758, 838-847)
+and the evanescent overlap K = I_tear / I_guided of the time-averaged
+intensity |E|^2/2 at the output window (fdtd_analyzer.py:2842-2935).
+
+The tile shape (rows per block) and the group budget are chosen by a small
+autotuner that times candidate configurations on the sweep itself and then
+restores the initial state.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import engine as E
+from .geometry import build_2d
+
+DTYPES = {'f32': (N.F32, torch.float32), 'f16': (N.F16, torch.float16), 'bf16': (N.BF16, torch.bfloat16)}
+
+
+class Instance:
+    """Device state of one 2D solve in a batch."""
+
+    def __init__(self, sp, steps, dtype, dev, geo=None):
+        self.spec, self.steps = sp, int(steps)
+        geo = build_2d(sp) if geo is None else geo
+        self.geo = geo
+        nx, ny = sp.nx, sp.ny
+        P = self.pitch = E.pitch_of(ny)
+        shp = (nx, P)
+        self.pol = 0 if sp.pol == 's' else 1
+        self.f = [torch.zeros(shp, dtype=dtype, device=dev) for _ in range(3)]
+        if self.pol == 0:
+            cn = ['ce_e', 'ce_h']
+        else:
+            cn = ['ca_x', 'ca_y'] + (['da_x', 'da_y'] if geo.get('da_x') is not None else [])
+        self.c = [E._pad_upload(geo[k], shp, dev) for k in cn]
+        self.axx, self.axy = E._Axis(geo['cx'], nx, dev), E._Axis(geo['cy'], ny, dev)
+        wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
+        z = lambda a, b: torch.zeros((a, b), dtype=torch.float32, device=dev)
+        if self.pol == 0:   # hxy (nx, wyh), hyx (wxh, P), ezx (wxe, P), ezy (nx, wye)
+            self.psi = [z(nx, max(1, wyh)), z(max(1, wxh), P), z(max(1, wxe), P), z(nx, max(1, wye))]
+        else:               # hzx (wxh, P), hzy (nx, wyh), exy (nx, wye), eyx (wxe, P)
+            self.psi = [z(max(1, wxh), P), z(nx, max(1, wyh)), z(nx, max(1, wye)), z(max(1, wxe), P)]
+        src = geo['src']
+        self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], np.float32)).to(dev)
+                      for k in ('amp', 'ph1', 'ph2')}
+        self.omega = src['omega']
+        f0 = sp.f0
+        self.steps_per_T = max(4, int(round((1.0 / f0) / sp.dt)))
+        self.n_acc = min(self.steps, 8 * self.steps_per_T)
+        self.window = (self.steps - self.n_acc, self.steps)
+        self.dft = torch.zeros((nx, P, 2), dtype=torch.float32, device=dev)
+        s = N.Inst2D()
+        s.pol, s.nx, s.ny, s.pitch = self.pol, nx, ny, P
+        for q in range(3):
+            s.f[q] = self.f[q].data_ptr()
+        for q, t in enumerate(self.c):
+            s.c[q] = t.data_ptr()
+        s.ch = float(np.float32(sp.dt / (E.MU0 * sp.dx)))
+        s.ax, s.ay = self.axx.ax, self.axy.ax
+        for q in range(4):
+            s.psi[q] = self.psi[q].data_ptr()
+        s.pec = (ctypes.c_int * 4)(1, 1, 1, 1)
+        s.src = N.Source(int(src['ix']), E._ptr(self.src_t['amp']), E._ptr(self.src_t['ph1']),
+                         E._ptr(self.src_t['ph2']), len(src['amp']), 1, len(src['amp']))
+        s.dft_n0, s.dft_n1 = self.window
+        s.dft = self.dft.data_ptr()
+        self.s = s
+
+    def nbytes(self):
+        t = self.f + self.c + self.psi + [self.dft]
+        return sum(x.numel() * x.element_size() for x in t)
+
+    def reset(self):
+        for t in self.f + self.psi + [self.dft]:
+            t.zero_()
+
+    def phasor(self):
+        """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 (fdtd2d_core.py:879)."""
+        a = self.dft[:, :self.spec.ny].double()
+        return (2.0 / self.n_acc) * torch.complex(a[..., 0], a[..., 1])
+
+    def overlap(self, ph=None):
+        """Evanescent overlap K = I_tear / I_guided at the output window (0.8 of the
+        length, 10 % wide) from <E^2> = |E|^2 / 2 (fdtd_analyzer.py:2880-2935)."""
+        sp = self.spec
+        ph = self.phasor() if ph is None else ph
+        I = 0.5 * (ph.real ** 2 + ph.imag ** 2)
+        dx, nx = sp.dx, sp.nx
+        c, w = 0.8 * nx, 0.1 * nx
+        lo, hi = max(0, int(round(c - w / 2))), min(nx, int(round(c + w / 2)))
+        j0 = int(round(sp.tear_m / dx))                            # y = 0: core bottom
+        j1 = int(round((sp.tear_m + sp.stack.t_wg_um * 1e-6) / dx))
+        tear = sum(t for t, _ in sp.stack.layers) * 1e-6
+        jt = max(0, int(round((sp.tear_m - tear) / dx)))
+        band = lambda a, b: float(torch.mean(torch.sum(I[lo:hi, a:b], dim=1))) if b > a else 0.0
+        g = band(j0, j1)
+        return band(jt, j0) / g if g > 0 else 0.0
+
+
+class Group:
+    """Instances advanced by the same batched launches."""
+
+    def __init__(self, insts, storage, by, dev):
+        self.insts, self.storage, self.by, self.dev = insts, storage, by, dev
+        n = len(insts)
+        self.host = (N.Inst2D * n)(*[q.s for q in insts])
+        self.lib = N.load()
+        blk = (ctypes.c_int * (n + 1))()
+        nblk = self.lib.lens_batch2d_plan(self.host, n, int(by), blk, None)
+        N.check(min(0, nblk))
+        owner = (ctypes.c_int * max(1, nblk))()
+        N.check(min(0, self.lib.lens_batch2d_plan(self.host, n, int(by), blk, owner)))
+        self.nblk = nblk
+        raw = ctypes.string_at(ctypes.addressof(self.host), ctypes.sizeof(self.host))
+        self.dev_desc = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
+        self.dev_blk = torch.tensor(list(blk), dtype=torch.int32, device=dev)
+        self.dev_owner = torch.frombuffer(bytearray(owner), dtype=torch.int32).to(dev)
+        self.steps = max(q.steps for q in insts)
+        self.graph = None
+
+    def step(self, tab, n0, nsteps, stream=None):
+        N.check(self.lib.lens_batch2d_step(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()),
+                                           ctypes.c_void_p(self.dev_blk.data_ptr()),
+                                           ctypes.c_void_p(self.dev_owner.data_ptr()), len(self.insts),
+                                           self.storage, int(self.by), ctypes.byref(tab.s), int(n0), int(nsteps),
+                                           E._stream_ptr(stream)))
+
+    def launches(self, n0, n1):
+        """Kernel launches of steps [n0, n1): H and E, plus the TM node DFT on window steps."""
+        tm = [q.window for q in self.insts if q.pol == 1]
+        extra = sum(1 for n in range(n0, n1) if any(a <= n < b for a, b in tm))
+        return 2 * (n1 - n0) + extra
+
+    def capture(self, tab):
+        """Record the whole schedule [0, steps) as one CUDA graph."""
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.dev)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.step(tab, 0, self.steps)
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+        return g
+
+
+class Sweep:
+    """A batched sweep of 2D solves (one shared time step and wavelength).
+
+    storage: 'f32' | 'f16' | 'bf16'.  by: rows per 32-lane tile; budget: bytes of
+    resident state per group (None: one group).  autotune() chooses both."""
+
+    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None):
+        dev = self.dev = E._device(device)
+        if storage not in DTYPES:
+            raise ValueError(f'storage {storage!r}: one of {sorted(DTYPES)}')
+        self.storage_name = storage
+        self.storage, dtype = DTYPES[storage]
+        dts = {round(sp.dt * 1e30) for sp in specs}
+        lams = {sp.lam_nm for sp in specs}
+        if len(dts) != 1 or len(lams) != 1:
+            raise ValueError('a batched sweep shares one time step and one wavelength')
+        self.steps = int(steps)
+        geos = geos if geos is not None else [None] * len(specs)
+        self.insts = [Instance(sp, steps, dtype, dev, geo) for sp, geo in zip(specs, geos)]
+        sp0 = specs[0]
+        self.table = E.StepTable(0, self.steps, sp0.dt, self.insts[0].omega, 2 * np.pi * sp0.f0,
+                                 E.cw_envelope(sp0.f0, sp0.ramp_periods), device=dev)
+        self.by, self.budget = by, budget
+        self.groups = self._groups(by, budget)
+        self.tuned = None
+
+    def _groups(self, by, budget):
+        order = sorted(range(len(self.insts)), key=lambda q: -self.insts[q].nbytes())
+        groups, cur, size = [], [], 0
+        for q in order:
+            b = self.insts[q].nbytes()
+            if cur and budget is not None and size + b > budget:
+                groups.append(cur)
+                cur, size = [], 0
+            cur.append(self.insts[q])
+            size += b
+        if cur:
+            groups.append(cur)
+        return [Group(g, self.storage, by, self.dev) for g in groups]
+
+    def cells(self):
+        return sum(q.spec.nx * q.spec.ny for q in self.insts)
+
+    def reset(self):
+        for q in self.insts:
+            q.reset()
+
+    def autotune(self, candidates=((8, None), (4, None), (8, 96 << 20), (4, 96 << 20), (8, 48 << 20), (2, 96 << 20)),
+                 probe_steps=24):
+        """Time `probe_steps` batched steps of every (rows per tile, group budget)
+        candidate on this sweep, keep the fastest, reset the fields."""
+        res = []
+        for by, budget in candidates:
+            groups = self._groups(by, budget)
+            for g in groups:              # warm-up
+                g.step(self.table, 0, 2)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for g in groups:
+                g.step(self.table, 2, probe_steps)
+            torch.cuda.synchronize()
+            res.append(((time.perf_counter() - t0) / probe_steps, by, budget))
+        self.reset()
+        best = min(res, key=lambda r: r[0])
+        self.by, self.budget = best[1], best[2]
+        self.groups = self._groups(self.by, self.budget)
+        self.tuned = [dict(by=b, budget=u, s_per_step=t) for t, b, u in res]
+        return self.tuned
+
+    def run(self, graphs=True):
+        """Run every group's whole schedule (one CUDA graph per group); returns
+        the number of kernel launches the graphs hold."""
+        launches = 0
+        for g in self.groups:
+            if graphs:
+                if g.graph is None:
+                    g.capture(self.table)
+                g.graph.replay()
+            else:
+                g.step(self.table, 0, g.steps)
+            launches += g.launches(0, g.steps)
+        return launches
+
+    def results(self):
+        out = []
+        for q in self.insts:
+            ph = q.phasor()
+            out.append(dict(pol=q.spec.pol, nx=q.spec.nx, ny=q.spec.ny, phasor=ph, K=q.overlap(ph)))
+        return out

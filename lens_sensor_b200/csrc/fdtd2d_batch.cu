@@ -1,0 +1,420 @@
+// Batched 2D TE/TM steps for sm_100a: many independent solves of uneven sizes
+// advanced together (tear-film / bead sweeps).
+//
+// One launch per half step covers every tile of every instance (32 columns x
+// 4 * blockDim.y rows, four rows per thread); block b reads its instance from
+// the plan's owner table (lens_batch2d_plan).  The per-cell arithmetic is term for
+// term the single-grid kernels' (fdtd2d.cu, after planar_beads/boundaries.py:
+// 164-274, source vcsel.py:151-156, loss fdtd2d_core.py:796-797), with the
+// fields read and written in the batch's storage type (FP32, FP16 or BF16) and
+// all arithmetic in FP32.
+//
+// Launches per step: H, E (TE: + node DFT), and on DFT-window steps a TM node
+// epilogue (Ey averaged onto the nodes, fdtd2d_core.py:458-465).  A span of
+// steps is graph-capturable: the host issues only kernel launches.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "lens_common.cuh"
+
+namespace {
+
+constexpr int BXB = 32;  // lanes along y (contiguous)
+
+template <typename T>
+struct St;
+template <>
+struct St<float> {
+    static __device__ __forceinline__ float ld(const void *p, size_t o) { return static_cast<const float *>(p)[o]; }
+    static __device__ __forceinline__ void st(void *p, size_t o, float v) { static_cast<float *>(p)[o] = v; }
+};
+template <>
+struct St<__half> {
+    static __device__ __forceinline__ float ld(const void *p, size_t o) {
+        return __half2float(static_cast<const __half *>(p)[o]);
+    }
+    static __device__ __forceinline__ void st(void *p, size_t o, float v) {
+        static_cast<__half *>(p)[o] = __float2half_rn(v);
+    }
+};
+template <>
+struct St<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const void *p, size_t o) {
+        return __bfloat162float(static_cast<const __nv_bfloat16 *>(p)[o]);
+    }
+    static __device__ __forceinline__ void st(void *p, size_t o, float v) {
+        static_cast<__nv_bfloat16 *>(p)[o] = __float2bfloat16_rn(v);
+    }
+};
+
+// A block covers a tile of 32 columns (lanes, contiguous y) x blockDim.y * RB
+// rows of one instance; each thread updates RB consecutive rows of its column,
+// issuing all of their loads before the arithmetic (the rows share the
+// x-neighbour loads).  owner[b] is the instance of block b and blk[q] its first
+// block; the descriptor fields are read through the read-only cache (every
+// thread of the block reads the same words).
+constexpr int RB = 4;
+
+struct Tile {
+    const LensInst2D *g;
+    int i, j;  // first row of this thread, column
+};
+
+__device__ __forceinline__ Tile tile_of(const LensInst2D *inst, const int *blk, const int *owner) {
+    const int b = blockIdx.x;
+    const int q = __ldg(owner + b);
+    const LensInst2D *g = inst + q;
+    const int t = b - __ldg(blk + q);
+    const int ntj = (__ldg(&g->ny) + BXB - 1) / BXB;
+    return Tile{g, (t / ntj) * (int)blockDim.y * RB + (int)threadIdx.y * RB, (t % ntj) * BXB + (int)threadIdx.x};
+}
+
+// Read-only view of one instance descriptor (loads through the non-coherent cache).
+struct V {
+    const LensInst2D *p;
+    __device__ __forceinline__ int pol() const { return __ldg(&p->pol); }
+    __device__ __forceinline__ int nx() const { return __ldg(&p->nx); }
+    __device__ __forceinline__ int ny() const { return __ldg(&p->ny); }
+    __device__ __forceinline__ int pitch() const { return __ldg(&p->pitch); }
+    __device__ __forceinline__ void *f(int q) const {
+        return reinterpret_cast<void *>(__ldg(reinterpret_cast<const unsigned long long *>(&p->f[q])));
+    }
+    __device__ __forceinline__ const float *c(int q) const {
+        return reinterpret_cast<const float *>(__ldg(reinterpret_cast<const unsigned long long *>(&p->c[q])));
+    }
+    __device__ __forceinline__ float *psi(int q) const {
+        return reinterpret_cast<float *>(__ldg(reinterpret_cast<const unsigned long long *>(&p->psi[q])));
+    }
+    __device__ __forceinline__ float ch() const { return __ldg(&p->ch); }
+    __device__ __forceinline__ const LensProfile &prof(bool x, bool e) const {
+        return x ? (e ? p->ax.e : p->ax.h) : (e ? p->ay.e : p->ay.h);
+    }
+};
+
+__device__ __forceinline__ float src_b(const LensSource &s, const LensStepTable &tab, int n, int i, int j) {
+    const int k = n - tab.t0;
+    if (i == s.ix) return (tab.env[k] * sinf(tab.wt[k] + s.ph1[j])) * s.amp[j];
+    return -((tab.env[k] * sinf(tab.wt[k] + s.ph2[j])) * s.amp[j]);
+}
+
+__device__ __forceinline__ void dft_node(const LensInst2D *g, const LensStepTable &tab, int n, size_t o, float v) {
+    float *d = reinterpret_cast<float *>(__ldg(reinterpret_cast<const unsigned long long *>(&g->dft)));
+    if (d && n >= __ldg(&g->dft_n0) && n < __ldg(&g->dft_n1)) {
+        const int k = n - tab.t0;
+        float2 *a = reinterpret_cast<float2 *>(d) + o;
+        float2 s = *a;
+        s.x += v * tab.pe[2 * k];
+        s.y += v * tab.pe[2 * k + 1];
+        *a = s;
+    }
+}
+
+// psi update at profile entry m: psi = b*psi + c*d, stored; returns the new psi.
+__device__ __forceinline__ float psi_step(const LensProfile &pf, int m, float *q, float d) {
+    const float p = __ldg(pf.b + m) * (*q) + __ldg(pf.c + m) * d;
+    *q = p;
+    return p;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
+    const Tile tl = tile_of(inst, blk, owner);
+    const V g{tl.g};
+    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    const float ch = g.ch();
+    using S = St<T>;
+    const LensProfile &xh = g.prof(true, false), &yh = g.prof(false, false);
+    if (g.pol() == 0) {  // TE: Hx, Hy from Ez (boundaries.py:186-194)
+        if (i0 >= nx || j >= ny) return;
+        const void *ezp = g.f(0);
+        void *hxp = g.f(1), *hyp = g.f(2);
+        float ez[RB + 1], ezj[RB], hx[RB], hy[RB];
+#pragma unroll
+        for (int r = 0; r <= RB; ++r) ez[r] = (i0 + r < nx) ? S::ld(ezp, (size_t)(i0 + r) * P + j) : 0.f;
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const size_t o = (size_t)(i0 + r) * P + j;
+            const bool in = i0 + r < nx;
+            ezj[r] = (in && j < ny - 1) ? S::ld(ezp, o + 1) : 0.f;
+            hx[r] = in ? S::ld(hxp, o) : 0.f;
+            hy[r] = in ? S::ld(hyp, o) : 0.f;
+        }
+        const int sj = j < ny - 1 ? strip_of(j, yh.lo, yh.hi, yh.n) : -1;
+        const float kj = j < ny - 1 ? __ldg(yh.ik + j) : 0.f;
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            if (i >= nx) break;
+            const size_t o = (size_t)i * P + j;
+            if (j < ny - 1) {
+                const float d = ezj[r] - ez[r];
+                float p = 0.f;
+                if (sj >= 0) p = psi_step(yh, j, g.psi(0) + (size_t)i * (yh.lo + yh.hi) + sj, d);
+                S::st(hxp, o, hx[r] - ch * (d * kj + p));
+            }
+            if (i < nx - 1) {
+                const float d = ez[r + 1] - ez[r];
+                float p = 0.f;
+                const int s = strip_of(i, xh.lo, xh.hi, xh.n);
+                if (s >= 0) p = psi_step(xh, i, g.psi(1) + (size_t)s * P + j, d);
+                S::st(hyp, o, hy[r] + ch * (d * __ldg(xh.ik + i) + p));
+            }
+        }
+        return;
+    }
+    // TM: Hz from Ex, Ey (boundaries.py:240-247)
+    if (i0 >= nx - 1 || j >= ny - 1) return;
+    const void *exp_ = g.f(0), *eyp = g.f(1);
+    void *hzp = g.f(2);
+    float ey[RB + 1], ex[RB], exj[RB], hz[RB];
+#pragma unroll
+    for (int r = 0; r <= RB; ++r) ey[r] = (i0 + r < nx) ? S::ld(eyp, (size_t)(i0 + r) * P + j) : 0.f;
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const size_t o = (size_t)(i0 + r) * P + j;
+        const bool in = i0 + r < nx - 1;
+        ex[r] = in ? S::ld(exp_, o) : 0.f;
+        exj[r] = in ? S::ld(exp_, o + 1) : 0.f;
+        hz[r] = in ? S::ld(hzp, o) : 0.f;
+    }
+    const int sj = strip_of(j, yh.lo, yh.hi, yh.n);
+    const float kj = __ldg(yh.ik + j);
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r;
+        if (i >= nx - 1) break;
+        const size_t o = (size_t)i * P + j;
+        const float dyx = ey[r + 1] - ey[r], dxy = exj[r] - ex[r];
+        float px = 0.f, py = 0.f;
+        const int s = strip_of(i, xh.lo, xh.hi, xh.n);
+        if (s >= 0) px = psi_step(xh, i, g.psi(0) + (size_t)s * P + j, dyx);
+        if (sj >= 0) py = psi_step(yh, j, g.psi(1) + (size_t)i * (yh.lo + yh.hi) + sj, dxy);
+        S::st(hzp, o, hz[r] - ch * ((dyx * __ldg(xh.ik + i) + px) - (dxy * kj + py)));
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    b2d_e(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
+    const Tile tl = tile_of(inst, blk, owner);
+    const V g{tl.g};
+    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    using S = St<T>;
+    const LensProfile &xe = g.prof(true, true), &ye = g.prof(false, true);
+    const LensSource &src = tl.g->src;
+    const int *pec = tl.g->pec;
+    const int six = __ldg(&src.ix), snj = __ldg(&src.nj);
+    const int pec0 = __ldg(pec), pec1 = __ldg(pec + 1), pec2 = __ldg(pec + 2), pec3 = __ldg(pec + 3);
+    if (g.pol() == 0) {  // TE: Ez (boundaries.py:196-215), source, PEC, node DFT
+        if (i0 >= nx || j >= ny) return;
+        void *ezp = g.f(0);
+        const void *hxp = g.f(1), *hyp = g.f(2);
+        const float *ce = g.c(0), *chh = g.c(1);
+        const bool jin = j > 0 && j < ny - 1;
+        float hy[RB + 1], hx[RB], hxm[RB], ez[RB], c0[RB], c1[RB];
+#pragma unroll
+        for (int r = 0; r <= RB; ++r) {  // hy[r] = Hy(i0 + r - 1)
+            const int i = i0 + r - 1;
+            hy[r] = (i >= 0 && i < nx && jin) ? S::ld(hyp, (size_t)i * P + j) : 0.f;
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            const size_t o = (size_t)i * P + j;
+            const bool in = i < nx;
+            const bool upd = in && jin && i > 0 && i < nx - 1;
+            hx[r] = upd ? S::ld(hxp, o) : 0.f;
+            hxm[r] = upd ? S::ld(hxp, o - 1) : 0.f;
+            ez[r] = in ? S::ld(ezp, o) : 0.f;
+            c0[r] = upd ? __ldg(ce + o) : 0.f;
+            c1[r] = upd ? __ldg(chh + o) : 0.f;
+        }
+        const int sj = jin ? strip_of(j, ye.lo, ye.hi, ye.n) : -1;
+        const float kj = __ldg(ye.ik + j);
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            if (i >= nx) break;
+            const size_t o = (size_t)i * P + j;
+            float v = ez[r];
+            if (jin && i > 0 && i < nx - 1) {
+                const float dhy = hy[r + 1] - hy[r], dhx = hx[r] - hxm[r];
+                float qx = 0.f, qy = 0.f;
+                const int s = strip_of(i, xe.lo, xe.hi, xe.n);
+                if (s >= 0) qx = psi_step(xe, i, g.psi(2) + (size_t)s * P + j, dhy);
+                if (sj >= 0) qy = psi_step(ye, j, g.psi(3) + (size_t)i * (ye.lo + ye.hi) + sj, dhx);
+                v = c0[r] * v + c1[r] * (dhy * __ldg(xe.ik + i) + qx - dhx * kj - qy);
+            }
+            if ((i == six || i == six + 1) && j < snj) v += src_b(src, tab, n, i, j);
+            if ((pec0 && i == 0) || (pec1 && i == nx - 1) || (pec2 && j == 0) || (pec3 && j == ny - 1)) v = 0.f;
+            S::st(ezp, o, v);
+            dft_node(tl.g, tab, n, o, v);
+        }
+        return;
+    }
+    // TM: loss damping, Ex / Ey (boundaries.py:249-268), source, PEC
+    if (i0 >= nx || j >= ny) return;
+    void *exp_ = g.f(0), *eyp = g.f(1);
+    const void *hzp = g.f(2);
+    const float *cax = g.c(0), *cay = g.c(1), *dax = g.c(2), *day = g.c(3);
+    const bool jin = j > 0 && j < ny - 1;
+    float hz[RB + 1], hzj[RB], ex[RB], ey[RB], ax_[RB], ay_[RB], dx_[RB], dy_[RB];
+#pragma unroll
+    for (int r = 0; r <= RB; ++r) {  // hz[r] = Hz(i0 + r - 1)
+        const int i = i0 + r - 1;
+        hz[r] = (i >= 0 && i < nx - 1 && j < ny - 1) ? S::ld(hzp, (size_t)i * P + j) : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r;
+        const size_t o = (size_t)i * P + j;
+        const bool exv = i < nx - 1, eyv = i < nx && j < ny - 1;
+        hzj[r] = (exv && jin) ? S::ld(hzp, o - 1) : 0.f;
+        ex[r] = exv ? S::ld(exp_, o) : 0.f;
+        ey[r] = eyv ? S::ld(eyp, o) : 0.f;
+        ax_[r] = (exv && jin) ? __ldg(cax + o) : 0.f;
+        ay_[r] = (eyv && i > 0 && i < nx - 1) ? __ldg(cay + o) : 0.f;
+        dx_[r] = (exv && dax) ? __ldg(dax + o) : 1.f;
+        dy_[r] = (eyv && day) ? __ldg(day + o) : 1.f;
+    }
+    const int sj = jin ? strip_of(j, ye.lo, ye.hi, ye.n) : -1;
+    const float kj = __ldg(ye.ik + j);
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r;
+        if (i >= nx) break;
+        const size_t o = (size_t)i * P + j;
+        if (i < nx - 1) {  // Ex at (i+1/2, j)
+            float e = ex[r];
+            if (dax) e = e * dx_[r];
+            if (jin) {
+                const float d = hz[r + 1] - hzj[r];
+                float p = 0.f;
+                if (sj >= 0) p = psi_step(ye, j, g.psi(2) + (size_t)i * (ye.lo + ye.hi) + sj, d);
+                e = e + ax_[r] * (d * kj + p);
+            }
+            if ((pec2 && j == 0) || (pec3 && j == ny - 1)) e = 0.f;
+            S::st(exp_, o, e);
+        }
+        if (j < ny - 1) {  // Ey at (i, j+1/2)
+            float e = ey[r];
+            if (day) e = e * dy_[r];
+            if (i > 0 && i < nx - 1) {
+                const float d = hz[r + 1] - hz[r];
+                float p = 0.f;
+                const int s = strip_of(i, xe.lo, xe.hi, xe.n);
+                if (s >= 0) p = psi_step(xe, i, g.psi(3) + (size_t)s * P + j, d);
+                e = e + (-ay_[r]) * (d * __ldg(xe.ik + i) + p);
+            }
+            if ((i == six || i == six + 1) && j < snj) e += src_b(src, tab, n, i, j);
+            if ((pec0 && i == 0) || (pec1 && i == nx - 1)) e = 0.f;
+            S::st(eyp, o, e);
+        }
+    }
+}
+
+// TM node DFT: Ey averaged onto the nodes (fdtd2d_core.py:458-465).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    b2d_tm_node(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
+    const Tile tl = tile_of(inst, blk, owner);
+    const V g{tl.g};
+    if (g.pol() != 1) return;
+    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    if (i0 >= nx || j >= ny) return;
+    using S = St<T>;
+    const void *p1 = g.f(1);
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r;
+        if (i >= nx) break;
+        const size_t row = (size_t)i * P;
+        const float v = (j == 0) ? S::ld(p1, row) : (j == ny - 1) ? S::ld(p1, row + ny - 2)
+                                                                : 0.5f * (S::ld(p1, row + j - 1) + S::ld(p1, row + j));
+        dft_node(tl.g, tab, n, row + j, v);
+    }
+}
+
+bool inst_ok(const LensInst2D &g) {
+    if ((g.pol != 0 && g.pol != 1) || g.nx < 3 || g.ny < 3 || g.pitch < g.ny || (g.pitch % 32)) return false;
+    if (!g.f[0] || !g.f[1] || !g.f[2] || !g.c[0] || !g.c[1]) return false;
+    if (g.pol == 1 && (!g.c[2]) != (!g.c[3])) return false;
+    if (!lens_profile_ok(g.ax.e, g.nx) || !lens_profile_ok(g.ax.h, g.nx - 1) || !lens_profile_ok(g.ay.e, g.ny) ||
+        !lens_profile_ok(g.ay.h, g.ny - 1))
+        return false;
+    if (g.src.ix >= 0 && (!g.src.amp || !g.src.ph1 || !g.src.ph2 || g.src.ix + 1 >= g.nx || g.src.nj > g.ny))
+        return false;
+    return true;
+}
+
+long inst_blocks(const LensInst2D &g, int by) {
+    return (long)((g.ny + BXB - 1) / BXB) * ((g.nx + by * RB - 1) / (by * RB));
+}
+
+template <typename T>
+void launch(const LensInst2D *dev, const int *blk, const int *owner, int ninst, int nblk, int by,
+            const LensStepTable &tab, int n0, int nsteps, bool tm_dft, const LensInst2D *host, cudaStream_t s) {
+    const dim3 b(BXB, by);
+    for (int n = n0; n < n0 + nsteps; ++n) {
+        b2d_h<T><<<nblk, b, 0, s>>>(dev, blk, owner);
+        b2d_e<T><<<nblk, b, 0, s>>>(dev, blk, owner, tab, n);
+        if (tm_dft) {
+            bool any = false;
+            for (int q = 0; q < ninst && !any; ++q)
+                any = host[q].pol == 1 && host[q].dft && n >= host[q].dft_n0 && n < host[q].dft_n1;
+            if (any) b2d_tm_node<T><<<nblk, b, 0, s>>>(dev, blk, owner, tab, n);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int lens_batch2d_plan(const LensInst2D *inst, int ninst, int by, int *blk, int *owner) {
+    if (!inst || !blk || ninst < 1 || by < 1 || BXB * by > 256) return LENS_ERR_ARG;
+    long tot = 0;
+    for (int q = 0; q < ninst; ++q) {
+        if (!inst_ok(inst[q])) return LENS_ERR_ARG;
+        blk[q] = (int)tot;
+        const long nb = inst_blocks(inst[q], by);
+        if (tot + nb > 0x7fffffffL) return LENS_ERR_SIZE;
+        if (owner)
+            for (long b = 0; b < nb; ++b) owner[tot + b] = q;
+        tot += nb;
+    }
+    blk[ninst] = (int)tot;
+    return (int)tot;
+}
+
+extern "C" int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
+                                 const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
+                                 int n0, int nsteps, void *stream) {
+    if (!inst_host || !inst_dev || !blk_dev || !owner_dev || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0 ||
+        !lens_table_ok(tab, n0, nsteps))
+        return LENS_ERR_ARG;
+    long tot = 0;
+    bool tm_dft = false, any_dft = false;
+    for (int q = 0; q < ninst; ++q) {
+        if (!inst_ok(inst_host[q])) return LENS_ERR_ARG;
+        tot += inst_blocks(inst_host[q], by);
+        tm_dft = tm_dft || (inst_host[q].pol == 1 && inst_host[q].dft);
+        any_dft = any_dft || inst_host[q].dft;
+    }
+    if (tot > 0x7fffffffL) return LENS_ERR_SIZE;
+    if (any_dft && !tab->pe) return LENS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int nblk = (int)tot;
+    switch (storage) {
+        case LENS_F32:
+            launch<float>(inst_dev, blk_dev, owner_dev, ninst, nblk, by, *tab, n0, nsteps, tm_dft, inst_host, s);
+            break;
+        case LENS_F16:
+            launch<__half>(inst_dev, blk_dev, owner_dev, ninst, nblk, by, *tab, n0, nsteps, tm_dft, inst_host, s);
+            break;
+        case LENS_BF16:
+            launch<__nv_bfloat16>(inst_dev, blk_dev, owner_dev, ninst, nblk, by, *tab, n0, nsteps, tm_dft,
+                                  inst_host, s);
+            break;
+        default: return LENS_ERR_ARG;
+    }
+    return lens_cuda_status();
+}

@@ -1429,11 +1429,12 @@ extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, float *iavg
 extern "C" int lens_version(void) { return 100; }
 
 extern "C" int lens_abi_sizes(int *sizes, int n) {
-    const int v[9] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
-                      (int)sizeof(LensSource),  (int)sizeof(LensTE2D), (int)sizeof(LensTM2D),
-                      (int)sizeof(LensEpi2D),   (int)sizeof(LensGrid3D), (int)sizeof(LensEpi3D)};
-    for (int q = 0; q < n && q < 9; ++q) sizes[q] = v[q];
-    return 9;
+    const int v[10] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
+                       (int)sizeof(LensSource),  (int)sizeof(LensTE2D), (int)sizeof(LensTM2D),
+                       (int)sizeof(LensEpi2D),   (int)sizeof(LensGrid3D), (int)sizeof(LensEpi3D),
+                       (int)sizeof(LensInst2D)};
+    for (int q = 0; q < n && q < 10; ++q) sizes[q] = v[q];
+    return 10;
 }
 
 extern "C" const char *lens_status_string(int status) {

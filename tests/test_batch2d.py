@@ -1,0 +1,106 @@
+"""Batched 2D solves (lens_batch2d_plan / lens_batch2d_step, batch2d.Sweep).
+
+CPU: the block plan of uneven instances (counts, owner table, argument errors).
+GPU: a batch of uneven TE/TM instances against the single-grid engine (same
+per-cell arithmetic: FP32 fields identical; the batch's plain complex64 DFT
+against the single path's compensated one), graph replay against direct
+stepping, and the FP16 / BF16 storage variants against FP32 within their
+stated tolerances.
+"""
+import ctypes
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from lens_sensor_b200 import _native as N
+
+# stated phasor tolerances of the storage variants against FP32 storage (400 steps)
+TOL_F16 = 2e-3
+TOL_BF16 = 1e-2
+
+
+def _fake_inst(nx, ny, pol):
+    """A descriptor with valid sizes and non-null placeholder pointers (never dereferenced)."""
+    s = N.Inst2D()
+    s.pol, s.nx, s.ny, s.pitch = pol, nx, ny, (ny + 31) // 32 * 32
+    for q in range(3):
+        s.f[q] = 16
+    s.c[0] = s.c[1] = 16
+    for ax, n in ((s.ax, nx), (s.ay, ny)):
+        for tag, m in (('e', n), ('h', n - 1)):
+            setattr(ax, tag, N.Profile(16, 16, 16, m, 2, 2))
+    s.src = N.Source(-1, None, None, None, 0, 0, 0)
+    return s
+
+
+def test_plan_of_uneven_instances():
+    lib = N.load()
+    sizes = [(130, 70, 0), (64, 33, 1), (300, 200, 0)]
+    arr = (N.Inst2D * 3)(*[_fake_inst(*v) for v in sizes])
+    blk = (ctypes.c_int * 4)()
+    by = 4
+    n = lib.lens_batch2d_plan(arr, 3, by, blk, None)
+    per = [((ny + 31) // 32) * ((nx + 4 * by - 1) // (4 * by)) for nx, ny, _ in sizes]
+    assert n == sum(per) and list(blk) == [0, per[0], per[0] + per[1], sum(per)]
+    owner = (ctypes.c_int * n)()
+    assert lib.lens_batch2d_plan(arr, 3, by, blk, owner) == n
+    assert list(owner) == [0] * per[0] + [1] * per[1] + [2] * per[2]
+    assert lib.lens_batch2d_plan(arr, 3, 9, blk, None) == -1       # 32 x 9 threads > 256
+    bad = (N.Inst2D * 1)(_fake_inst(2, 40, 0))                      # nx < 3
+    assert lib.lens_batch2d_plan(bad, 1, 4, blk, None) == -1
+
+
+def _small_sweep():
+    from lens_sensor_b200.workloads import config2
+    specs, _ = config2(count=6)
+    return [replace(sp, nx=min(sp.nx, 150 + 23 * q), ny=min(sp.ny, 300 - 11 * q)) for q, sp in enumerate(specs)]
+
+
+@pytest.mark.gpu
+def test_batch_matches_single_grid_engine():
+    import torch
+    from lens_sensor_b200 import batch2d as B
+    from lens_sensor_b200 import engine as E
+    specs, steps = _small_sweep(), 400
+    sw = B.Sweep(specs, steps, 'f32', by=4)
+    sw.run(graphs=False)
+    torch.cuda.synchronize()
+    res = sw.results()
+    for q, sp in enumerate(specs):
+        geo = sw.insts[q].geo
+        coef = {k: geo[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if k in geo}
+        g = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, geo['cx'], geo['cy'], geo['src'])
+        ep = E.Epi2D(g, dft=sw.insts[q].window)
+        g.step(sw.table, 0, steps, ep)
+        torch.cuda.synchronize()
+        names = ('ez', 'hx', 'hy') if sp.pol == 's' else ('ex', 'ey', 'hz')
+        for c, nm in enumerate(names):
+            a = sw.insts[q].f[c][:sp.nx, :sp.ny]
+            b = getattr(g, nm)[:sp.nx, :sp.ny]
+            assert float((a - b).norm()) <= 1e-6 * max(float(b.norm()), 1e-30), (q, nm)
+        ph = (2.0 / sw.insts[q].n_acc) * ep.phasor()
+        assert float((res[q]['phasor'] - ph).abs().norm()) < 1e-5 * float(ph.abs().norm()), q
+
+
+@pytest.mark.gpu
+def test_graph_replay_and_storage_variants():
+    import torch
+    from lens_sensor_b200 import batch2d as B
+    specs, steps = _small_sweep(), 400
+    a = B.Sweep(specs, steps, 'f32', by=4)
+    a.run(graphs=False)
+    b = B.Sweep(specs, steps, 'f32', by=8, geos=[q.geo for q in a.insts])
+    b.run(graphs=True)
+    torch.cuda.synchronize()
+    for p, q in zip(a.insts, b.insts):
+        for x, y in zip(p.f, q.f):
+            assert torch.equal(x, y)
+    ref = [r['phasor'] for r in a.results()]
+    for st, tol in (('f16', TOL_F16), ('bf16', TOL_BF16)):
+        c = B.Sweep(specs, steps, st, geos=[q.geo for q in a.insts])
+        c.run()
+        torch.cuda.synchronize()
+        for q, r in enumerate(c.results()):
+            err = float((r['phasor'] - ref[q]).abs().norm() / ref[q].abs().norm())
+            assert err < tol, (st, q, err)

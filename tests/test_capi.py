@@ -40,8 +40,9 @@ def test_bindings_cover_every_declared_symbol():
 
 def test_abi_sizes_match(lib):
     from lens_sensor_b200 import _native
-    sizes = (ctypes.c_int * 9)()
-    assert lib.lens_abi_sizes(sizes, 9) == 9
+    n = len(_native.MIRRORS)
+    sizes = (ctypes.c_int * n)()
+    assert lib.lens_abi_sizes(sizes, n) == n
     assert list(sizes) == [ctypes.sizeof(m) for m in _native.MIRRORS]
 
 
@@ -58,4 +59,8 @@ def test_invalid_arguments_are_rejected_without_launch(lib):
     assert lib.lens_fdtd3d_step(None, None, None, 0, 1, None) == -1
     g = N.Grid3D()
     assert lib.lens_fdtd3d_step(ctypes.byref(g), None, None, 0, 1, None) == -1
+    inst = (N.Inst2D * 2)()
+    blk = (ctypes.c_int * 3)()
+    assert lib.lens_batch2d_plan(inst, 2, 8, blk, None) == -1    # empty descriptors
+    assert lib.lens_batch2d_step(inst, None, None, None, 2, 0, 8, None, 0, 1, None) == -1
     assert lib.lens_fdtd3d_accum_e2(ctypes.byref(g), 1, None, None) == -1

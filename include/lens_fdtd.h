@@ -169,6 +169,21 @@ int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, c
                       const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
                       int n0, int nsteps, void *stream);
 
+/* Same step as lens_batch2d_step for callers that cannot allocate device
+ * memory (an application that owns the GPU allocator, a fixed memory budget, a
+ * loop where cudaMalloc's implicit synchronisation is not allowed).  No
+ * counterpart in the reference.  The descriptors (inst, in host memory), the
+ * block offsets and the owner table are placed in one fixed device array of
+ * about 8.6 MB that every GPU loading this library holds until the process
+ * exits; at most 512 instances and 2^21 tiles (32 x 4*by nodes each) per call,
+ * larger calls return LENS_ERR_SIZE.  Nothing is allocated.  The first call on
+ * a device looks up that array's device address; make it before any stream
+ * capture.  Every call rewrites the whole array (nothing carries over between
+ * calls), so calls that overlap on the GPU (other streams, other threads) race
+ * on it; the fields, psi and DFT buffers are the caller's as usual.          */
+int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int storage, int by,
+                              const LensStepTable *tab, int n0, int nsteps, void *stream);
+
 /* ---------------------------------------------------------------- 3D grid */
 /* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
  * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same

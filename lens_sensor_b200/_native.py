@@ -104,6 +104,8 @@ SIGNATURES = {
     'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
     'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                   POINTER(StepTable), c_int, c_int, c_void_p]),
+    'lens_batch2d_step_noalloc': (c_int, [POINTER(Inst2D), c_int, c_int, c_int, POINTER(StepTable), c_int,
+                                          c_int, c_void_p]),
     'lens_version': (c_int, []),
     'lens_status_string': (ctypes.c_char_p, [c_int]),
     'lens_abi_sizes': (c_int, [POINTER(c_int), c_int]),

@@ -15,6 +15,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <atomic>
+
 #include "lens_common.cuh"
 
 namespace {
@@ -415,6 +417,100 @@ extern "C" int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *
                                   inst_host, s);
             break;
         default: return LENS_ERR_ARG;
+    }
+    return lens_cuda_status();
+}
+
+// ------------------------------------------------------ allocation-free variant
+// lens_batch2d_step needs device copies of the instance descriptors and of the
+// block plan, which the caller allocates.  Callers that cannot allocate device
+// memory at all (a host application whose allocator owns the GPU, code running
+// under a fixed memory budget or inside a loop where cudaMalloc's implicit
+// synchronisation is not allowed) use lens_batch2d_step_noalloc instead: the
+// descriptors, the block offsets and the owner table live in one file-scope
+// device array of fixed size, which every GPU that loads this library holds
+// until the process exits.
+namespace {
+
+constexpr int NA_MAX_INST = 512;                 // instances per call
+constexpr int NA_MAX_BLOCKS = 1 << 21;           // tiles per call (32 x 4*by nodes each)
+constexpr size_t NA_DESC_BYTES = ((NA_MAX_INST * sizeof(LensInst2D) + 255) / 256) * 256;
+constexpr size_t NA_BLK_BYTES = (((NA_MAX_INST + 1) * sizeof(int) + 255) / 256) * 256;
+constexpr size_t NA_BYTES = NA_DESC_BYTES + NA_BLK_BYTES + (size_t)NA_MAX_BLOCKS * sizeof(int);
+
+static __device__ __align__(256) unsigned char g_batch2d_scratch[NA_BYTES];
+
+// Device address of the scratch array on the current device, looked up once per
+// device (host code must not use the array's name as a device address).
+constexpr int NA_MAX_DEV = 64;
+std::atomic<unsigned char *> na_addr[NA_MAX_DEV];
+
+int na_scratch(unsigned char **p) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LENS_ERR_CUDA;
+    if (dev < 0 || dev >= NA_MAX_DEV) return LENS_ERR_ARG;
+    unsigned char *a = na_addr[dev].load();
+    if (!a) {
+        void *v = nullptr;
+        if (cudaGetSymbolAddress(&v, g_batch2d_scratch) != cudaSuccess || !v) return LENS_ERR_CUDA;
+        a = static_cast<unsigned char *>(v);
+        na_addr[dev].store(a);
+    }
+    *p = a;
+    return LENS_OK;
+}
+
+// owner[b] = instance of block b (binary search over the block offsets).
+__global__ void na_owner(const int *blk, int ninst, int *owner, int nblk) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (blk[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    owner[b] = lo;
+}
+
+}  // namespace
+
+extern "C" int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int storage, int by,
+                                         const LensStepTable *tab, int n0, int nsteps, void *stream) {
+    if (!inst || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) ||
+        (storage != LENS_F32 && storage != LENS_F16 && storage != LENS_BF16))
+        return LENS_ERR_ARG;
+    if (ninst > NA_MAX_INST) return LENS_ERR_SIZE;
+    int blk[NA_MAX_INST + 1];
+    long tot = 0;
+    bool tm_dft = false, any_dft = false;
+    for (int q = 0; q < ninst; ++q) {
+        if (!inst_ok(inst[q])) return LENS_ERR_ARG;
+        blk[q] = (int)tot;
+        tot += inst_blocks(inst[q], by);
+        if (tot > NA_MAX_BLOCKS) return LENS_ERR_SIZE;
+        tm_dft = tm_dft || (inst[q].pol == 1 && inst[q].dft);
+        any_dft = any_dft || inst[q].dft;
+    }
+    blk[ninst] = (int)tot;
+    if (any_dft && !tab->pe) return LENS_ERR_ARG;
+    unsigned char *base = nullptr;
+    const int st = na_scratch(&base);
+    if (st != LENS_OK) return st;
+    LensInst2D *desc = reinterpret_cast<LensInst2D *>(base);
+    int *blk_dev = reinterpret_cast<int *>(base + NA_DESC_BYTES);
+    int *owner = reinterpret_cast<int *>(base + NA_DESC_BYTES + NA_BLK_BYTES);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // every table is rewritten in full by each call (nothing carries over)
+    if (cudaMemcpyAsync(desc, inst, ninst * sizeof(LensInst2D), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(blk_dev, blk, (ninst + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return LENS_ERR_CUDA;
+    const int nblk = (int)tot;
+    na_owner<<<(nblk + 255) / 256, 256, 0, s>>>(blk_dev, ninst, owner, nblk);
+    switch (storage) {
+        case LENS_F32: launch<float>(desc, blk_dev, owner, ninst, nblk, by, *tab, n0, nsteps, tm_dft, inst, s); break;
+        case LENS_F16: launch<__half>(desc, blk_dev, owner, ninst, nblk, by, *tab, n0, nsteps, tm_dft, inst, s); break;
+        default: launch<__nv_bfloat16>(desc, blk_dev, owner, ninst, nblk, by, *tab, n0, nsteps, tm_dft, inst, s);
     }
     return lens_cuda_status();
 }

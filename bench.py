@@ -309,8 +309,8 @@ def ours_arm(args):
     achieved = 72.0 * cells / t_launch / 1e9
     traffic = None
     try:
-        with open(os.path.join(ROOT, 'profiles', 'fused3d_config1_traffic.json')) as f:
-            traffic = json.load(f).get('bytes_per_step')
+        with open(os.path.join(ROOT, 'profiles', 'yee3d_config1_traffic.json')) as f:
+            traffic = json.load(f).get('bytes_per_launch')
     except Exception:
         pass
     # end to end through the public API: host setup, H2D, the whole 4000-step schedule, D2H of phasors

@@ -233,21 +233,42 @@ typedef struct {
     double *plane_acc;           /* per plane: 2 pairs (Ey/Hz, Ez/Hy) x 4 x (ny*pitch) doubles */
 } LensEpi3D;
 
+/* Stitch-window drive (fdtd3d_core.py:1614-1617): after each E update the first
+ * nplanes x-planes of Ex, Ey and Ez become
+ *     w_i * (env * Re(D e^{+i w t})) + (1 - w_i) * E
+ * with D the complex amplitude handed over from the previous window.          */
+typedef struct {
+    int nplanes;                 /* O: driven planes, 1 <= O <= nx-1            */
+    const float *taper;          /* 2*O floats: w_0..w_{O-1}, then 1-w_0..1-w_{O-1} */
+    const float *hand[3];        /* Ex, Ey, Ez amplitudes: (O, ny, pitch) x {re, im} */
+} LensDrive3D;
+
 /* Advance nsteps; updates g->cur when the fused (double-buffered) path runs. */
 int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
                      int n0, int nsteps, void *stream);
 
+/* The same steps with the stitch drive applied to every new E before the
+ * epilogue reads it (replaces the per-step overlap assignment of
+ * fdtd3d_core.py:1611-1617 in run_3d_stitched).  The epilogue may hold DFT
+ * windows, flux planes and convergence planes but no detector boxes.          */
+int lens_fdtd3d_step_driven(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
+                            const LensDrive3D *drive, int n0, int nsteps, void *stream);
+
 /* Iavg += |E|^2 of all three components mapped onto the grid of component
- * `target` (1 Ey, 2 Ez) exactly as fdtd3d_core.py:438-474 (_sq_on_grid/_accum_E2). */
-int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, float *iavg, void *stream);
+ * `target` (1 Ey, 2 Ez) exactly as fdtd3d_core.py:438-474 (_sq_on_grid/_accum_E2),
+ * over the x-planes [0, nx_target) of the slices Ex[:nx_target-1], Ey[:nx_target],
+ * Ez[:nx_target] (nx_target = nx: the whole grid; a stitch window passes its
+ * assembled width, fdtd3d_core.py:1650).                                     */
+int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, int nx_target, float *iavg, void *stream);
 
 /* Library identity and error text. */
 int lens_version(void);
 const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
- * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D.
- * Writes min(n, 10) entries and returns 10 (bindings check their mirrors). */
+ * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D,
+ * LensDrive3D.  Writes min(n, 11) entries and returns 11 (bindings check their
+ * mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

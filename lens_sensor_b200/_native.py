@@ -92,7 +92,11 @@ class Inst2D(ctypes.Structure):
                 ('src', Source), ('dft_n0', c_int), ('dft_n1', c_int), ('dft', c_void_p)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D)
+class Drive3D(ctypes.Structure):
+    _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p * 3)]
+
+
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
@@ -100,7 +104,9 @@ SIGNATURES = {
     'lens_te2d_step': (c_int, [POINTER(TE2D), POINTER(StepTable), POINTER(Epi2D), c_int, c_int, c_void_p]),
     'lens_tm2d_step': (c_int, [POINTER(TM2D), POINTER(StepTable), POINTER(Epi2D), c_int, c_int, c_void_p]),
     'lens_fdtd3d_step': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), c_int, c_int, c_void_p]),
-    'lens_fdtd3d_accum_e2': (c_int, [POINTER(Grid3D), c_int, c_void_p, c_void_p]),
+    'lens_fdtd3d_step_driven': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), POINTER(Drive3D),
+                                        c_int, c_int, c_void_p]),
+    'lens_fdtd3d_accum_e2': (c_int, [POINTER(Grid3D), c_int, c_int, c_void_p, c_void_p]),
     'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
     'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                   POINTER(StepTable), c_int, c_int, c_void_p]),

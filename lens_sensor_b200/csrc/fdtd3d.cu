@@ -116,7 +116,7 @@ __device__ __forceinline__ float src3(const K3 &g, const LensStepTable &tab, int
 }
 
 __device__ __forceinline__ bool is_src(const K3 &g, int comp, int i, int j, int k) {
-    return g.src_comp == comp && (i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj &&
+    return g.src_comp == comp && g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj &&
            k < g.src.nk;
 }
 
@@ -1100,6 +1100,33 @@ __global__ void __launch_bounds__(NT) win3d(const K3 g, const LensStepTable tab,
     }
 }
 
+// ============================================================ stitch drive
+// Soft injection of the previous window's CW field into the first O x-planes of
+// the new E (fdtd3d_core.py:1614-1617): for Ex, Ey and Ez
+//   F = w_i * (env * Re(D e^{+i w t})) + (1 - w_i) * F
+// with D the handed-over complex amplitude and w_i the cosine taper.  Rounded
+// operation by operation (no contraction) like the complex64 / float32 NumPy
+// expression; e^{+iwt} is the conjugate of the table's DFT phase.
+__global__ void __launch_bounds__(NT) drive3d(const K3 g, const LensStepTable tab, const LensDrive3D d, int n) {
+    const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y, i = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (k >= nz || j >= ny || i >= d.nplanes) return;
+    const size_t o = ((size_t)i * ny + j) * g.P + k;
+    const int q = n - tab.t0;
+    const float c = tab.pe[2 * q], s = -tab.pe[2 * q + 1], env = tab.env[q];
+    const float w = d.taper[i], w1 = d.taper[d.nplanes + i];
+    float *F[3] = {g.wex, g.wey, g.wez};
+    const bool ok[3] = {i < nx - 1, j < ny - 1, k < nz - 1};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        if (!ok[m]) continue;
+        const float2 D = reinterpret_cast<const float2 *>(d.hand[m])[o];
+        const float re = __fsub_rn(__fmul_rn(D.x, c), __fmul_rn(D.y, s));
+        const float v = __fmul_rn(w, __fmul_rn(env, re));
+        F[m][o] = __fadd_rn(v, __fmul_rn(w1, F[m][o]));
+    }
+}
+
 // ============================================================ Iavg
 // Square of component F mapped onto the target grid (fdtd3d_core.py:438-461):
 // x: equal extent or one shorter (mean of the clipped neighbours i-1, i);
@@ -1138,10 +1165,12 @@ __device__ __forceinline__ float sq_on_grid(const float *F, const Ext &f, const 
     return 0.5f * (sqxy(F, f, t, P, ny, i, j, k - 1) + sqxy(F, f, t, P, ny, i, j, k));
 }
 
-__global__ void __launch_bounds__(NT) accum_e2(const K3 g, int target, float *iavg) {
+// nxt <= nx: only planes [0, nxt) of the components take part, as for the slices
+// Ex[:nxt-1], Ey[:nxt], Ez[:nxt] (fdtd3d_core.py:1650).
+__global__ void __launch_bounds__(NT) accum_e2(const K3 g, int target, int nxt, float *iavg) {
     const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y, i = blockIdx.z;
-    const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
-    const Ext ex{nx - 1, ny, nz}, ey{nx, ny - 1, nz}, ez{nx, ny, nz - 1};
+    const int ny = g.ny, nz = g.nz, P = g.P;
+    const Ext ex{nxt - 1, ny, nz}, ey{nxt, ny - 1, nz}, ez{nxt, ny, nz - 1};
     const Ext t = target == 1 ? ey : ez;
     if (i >= t.nx || j >= t.ny || k >= t.nz) return;
     const float a = sq_on_grid(g.ex, ex, t, P, ny, i, j, k);
@@ -1355,23 +1384,45 @@ bool encode(CUtensorMap *m, const float *base, const LensGrid3D *g, int bk, int 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-}  // namespace
+// A drive acts after the E update, where the detector boxes are summed, so a
+// driven step takes no boxes.
+bool drive3d_ok(const LensDrive3D *d, const LensStepTable *t, const LensGrid3D *g, const LensEpi3D *ep) {
+    if (!d) return true;
+    if (ep && ep->nbox > 0) return false;
+    if (d->nplanes < 1 || d->nplanes > g->nx - 1 || !d->taper || !t->pe || !t->env) return false;
+    for (int m = 0; m < 3; ++m)
+        if (!d->hand[m] || (reinterpret_cast<uintptr_t>(d->hand[m]) & 7)) return false;
+    return true;
+}
 
-extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, int n0,
-                                int nsteps, void *stream) {
-    if (!grid3d_ok(g) || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) || !epi3d_ok(ep, tab, g))
+// Steps [n0, n0+nsteps): the Yee update (source included), then the optional
+// stitch drive on the new E, then the epilogue that reads the new E.
+int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const LensDrive3D *dr, int n0,
+           int nsteps, void *stream) {
+    if (!grid3d_ok(g) || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) || !epi3d_ok(ep, tab, g) ||
+        !drive3d_ok(dr, tab, g, ep))
         return LENS_ERR_ARG;
     LensEpi3D e{};  // zero: no boxes, empty windows, no planes
     if (ep) e = *ep;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const dim3 blk(BK, BJ);
+    const dim3 grd_d(g->pitch / BK, (g->ny + BJ - 1) / BJ, dr ? dr->nplanes : 1);
     if (!has_buffer1(g)) {
         const K3 k = view(g, g->cur, g->cur);
         const int chunk = chunk_len(g->nx, 96);
         const dim3 grd(g->pitch / BK, (g->ny + BJ - 1) / BJ, (g->nx + chunk - 1) / chunk);
         for (int n = n0; n < n0 + nsteps; ++n) {
             h3d<<<grd, blk, 0, s>>>(k, chunk);
-            e3d<<<grd, blk, 0, s>>>(k, *tab, e, n, chunk);
+            if (dr) {
+                // the in-place E pass folds the epilogue in; with a drive the
+                // epilogue must see the driven E, so it runs as a pass of its own
+                e3d<<<grd, blk, 0, s>>>(k, *tab, LensEpi3D{}, n, chunk);
+                drive3d<<<grd_d, blk, 0, s>>>(k, *tab, *dr, n);
+                if (epi3d_active(&e, n))
+                    win3d<<<dim3(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx), blk, 0, s>>>(k, *tab, e, n);
+            } else {
+                e3d<<<grd, blk, 0, s>>>(k, *tab, e, n, chunk);
+            }
         }
         return lens_cuda_status();
     }
@@ -1412,6 +1463,7 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
             yee3d<uint32_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
         else
             yee3d<size_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
+        if (dr) drive3d<<<grd_d, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, *dr, n);
         if (ea && ((n >= e.dft_n0 && n < e.dft_n1) || (e.conv_prev && n >= e.prev_n0 && n < e.prev_n1)))
             win3d<<<grd_w, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, e, n);
         g->cur = 1 - rb;
@@ -1419,22 +1471,37 @@ extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const L
     return lens_cuda_status();
 }
 
-extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, float *iavg, void *stream) {
-    if (!grid3d_ok(g) || !iavg || (target != 1 && target != 2)) return LENS_ERR_ARG;
-    const dim3 blk(BK, BJ), grd(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx);
-    accum_e2<<<grd, blk, 0, static_cast<cudaStream_t>(stream)>>>(view(g, g->cur, g->cur), target, iavg);
+}  // namespace
+
+extern "C" int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, int n0,
+                                int nsteps, void *stream) {
+    return step3d(g, tab, ep, nullptr, n0, nsteps, stream);
+}
+
+extern "C" int lens_fdtd3d_step_driven(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
+                                       const LensDrive3D *drive, int n0, int nsteps, void *stream) {
+    if (!drive) return LENS_ERR_ARG;
+    return step3d(g, tab, ep, drive, n0, nsteps, stream);
+}
+
+extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, int nx_target, float *iavg, void *stream) {
+    if (!grid3d_ok(g) || !iavg || (target != 1 && target != 2) || nx_target < 2 || nx_target > g->nx)
+        return LENS_ERR_ARG;
+    const dim3 blk(BK, BJ), grd(g->pitch / BK, (g->ny + BJ - 1) / BJ, nx_target);
+    accum_e2<<<grd, blk, 0, static_cast<cudaStream_t>(stream)>>>(view(g, g->cur, g->cur), target, nx_target,
+                                                                  iavg);
     return lens_cuda_status();
 }
 
 extern "C" int lens_version(void) { return 100; }
 
 extern "C" int lens_abi_sizes(int *sizes, int n) {
-    const int v[10] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
+    const int v[11] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
                        (int)sizeof(LensSource),  (int)sizeof(LensTE2D), (int)sizeof(LensTM2D),
                        (int)sizeof(LensEpi2D),   (int)sizeof(LensGrid3D), (int)sizeof(LensEpi3D),
-                       (int)sizeof(LensInst2D)};
-    for (int q = 0; q < n && q < 10; ++q) sizes[q] = v[q];
-    return 10;
+                       (int)sizeof(LensInst2D),  (int)sizeof(LensDrive3D)};
+    for (int q = 0; q < n && q < 11; ++q) sizes[q] = v[q];
+    return 11;
 }
 
 extern "C" const char *lens_status_string(int status) {

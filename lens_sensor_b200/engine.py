@@ -247,6 +247,14 @@ class Epi2D:
 
 
 # ============================================================================ 3D
+def plane_flux(pairs, n):
+    """sum over pairs of sign * Re(sum aE conj(aH)) / 2, times (2/n)^2 (flux.py:45-57)."""
+    tot = 0.0
+    for sign, aE, aH in pairs:
+        tot += sign * 0.5 * float(torch.real(torch.sum(aE * torch.conj(aH))))
+    return tot * (2.0 / n) ** 2
+
+
 class Grid3D:
     """One 3D CPML solve resident on the GPU (fdtd3d_core.run_3d hot loop state).
 
@@ -276,12 +284,16 @@ class Grid3D:
         self.psi = [{q: z() for q in N.PSI_NAMES} for _ in range(nbuf)]
         self.ce = [_pad_upload(a, shp, dev) for a in ce]
         self.da = None if da is None else [_pad_upload(a, shp, dev) for a in da]
-        amp = np.ascontiguousarray(src['amp'], F32)
-        self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
-                      for k in ('amp', 'ph1', 'ph2')}
-        nj, nk = amp.shape
-        s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
-                     _ptr(self.src_t['ph2']), nj, nk, nk)
+        if src is None:                # no source (a stitch window driven by its predecessor)
+            self.src_t = {}
+            s = N.Source(-1, None, None, None, 0, 0, 0)
+        else:
+            amp = np.ascontiguousarray(src['amp'], F32)
+            self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
+                          for k in ('amp', 'ph1', 'ph2')}
+            nj, nk = amp.shape
+            s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
+                         _ptr(self.src_t['ph2']), nj, nk, nk)
         self.src_comp = int(src_comp)
         self.flag = torch.zeros(1, dtype=torch.int32, device=dev)
         g = N.Grid3D()
@@ -315,21 +327,53 @@ class Grid3D:
         a, b, c = shapes[name]
         return getattr(self, name)[:a, :b, :c]
 
-    def step(self, table, n0, nsteps, epi=None, stream=None):
-        e = epi.s if epi is not None else None
-        N.check(self.lib.lens_fdtd3d_step(ctypes.byref(self.s), ctypes.byref(table.s),
-                                          ctypes.byref(e) if e is not None else None,
-                                          int(n0), int(nsteps), _stream_ptr(stream)))
+    def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
+        e = ctypes.byref(epi.s) if epi is not None else None
+        if drive is None:
+            N.check(self.lib.lens_fdtd3d_step(ctypes.byref(self.s), ctypes.byref(table.s), e,
+                                              int(n0), int(nsteps), _stream_ptr(stream)))
+        else:
+            N.check(self.lib.lens_fdtd3d_step_driven(ctypes.byref(self.s), ctypes.byref(table.s), e,
+                                                     ctypes.byref(drive.s), int(n0), int(nsteps),
+                                                     _stream_ptr(stream)))
 
     def check_flag(self):
         """Raise if a pipeline wait in the fused kernel gave up (results invalid)."""
         if int(self.flag.item()) != 0:
             raise N.LensError('fused 3D kernel: a pipeline wait timed out')
 
-    def accum_e2(self, iavg, target=None, stream=None):
+    def accum_e2(self, iavg, target=None, stream=None, nx=None):
+        """iavg += |E|^2 on the driven component's grid over x-planes [0, nx)."""
         t = self.src_comp if target is None else target
-        N.check(self.lib.lens_fdtd3d_accum_e2(ctypes.byref(self.s), int(t), _ptr(iavg),
-                                              _stream_ptr(stream)))
+        N.check(self.lib.lens_fdtd3d_accum_e2(ctypes.byref(self.s), int(t), int(self.nx if nx is None else nx),
+                                              _ptr(iavg), _stream_ptr(stream)))
+
+
+class Drive3D:
+    """Overlap drive of a stitch window (fdtd3d_core.py:1611-1617).
+
+    hand: complex amplitudes (complex64) of Ex, Ey, Ez on the first O x-planes,
+    shapes (O, ny, nz-ish) of each component's own grid; taper: the O weights
+    w_i (float32).  Both are copied into the padded device layout once."""
+
+    def __init__(self, grid, hand, taper):
+        dev, ny, P = grid.dev, grid.ny, grid.pitch
+        O = int(len(taper))
+        w = np.asarray(taper, F32)
+        self.taper = torch.from_numpy(np.concatenate([w, (F32(1.0) - w).astype(F32)])).to(dev)
+        self.hand = []
+        for D in hand:
+            t = torch.zeros((O, ny, P, 2), dtype=torch.float32, device=dev)
+            D = torch.as_tensor(D).to(dev)
+            t[:, :D.shape[1], :D.shape[2], 0] = D.real.float()
+            t[:, :D.shape[1], :D.shape[2], 1] = D.imag.float()
+            self.hand.append(t)
+        s = N.Drive3D()
+        s.nplanes = O
+        s.taper = _ptr(self.taper)
+        for m in range(3):
+            s.hand[m] = _ptr(self.hand[m])
+        self.s = s
 
 
 class Epi3D:
@@ -370,24 +414,32 @@ class Epi3D:
         s.plane_acc = _ptr(self.plane_acc)
         self.s = s
 
-    def phasor(self, comp=1):
+    def phasor(self, comp=1, kind=None):
+        """sum F e^{-iwt} of component comp over the DFT window, complex128 in the
+        component's shape.  kind ('split', 'hand') names the reference's separate
+        accumulators of run_3d_stitched (float32 re/im volume, complex64 overlap);
+        the device keeps one FP32 (re, im) sum per component, which serves all."""
         g = self.grid
         nx, ny, nz = g.nx, g.ny, g.nz
         shape = {0: (nx - 1, ny, nz), 1: (nx, ny - 1, nz), 2: (nx, ny, nz - 1)}[comp]
         a = self.dft[comp].double()
         return torch.complex(a[..., 0], a[..., 1])[:shape[0], :shape[1], :shape[2]]
 
-    def flux(self, name, n_acc):
-        """Net +x Poynting flux (pairs_3d, flux.py:84-90 and :45-57)."""
+    def plane_dft(self, name):
+        """[(sign, sum E e^{-iwt}, sum H e^{-iw(t-dt/2)})] of the two field pairs
+        of plane `name` (pairs_3d, flux.py:84-90), complex128."""
         g = self.grid
         q = list(self.planes).index(name)
-        tot = 0.0
+        out = []
         for pair, (sign, nj, nk) in enumerate(((1.0, g.ny - 1, g.nz), (-1.0, g.ny, g.nz - 1))):
             a = self.plane_acc[q, pair]
-            aE = torch.complex(a[0, :nj, :nk], a[1, :nj, :nk])
-            aH = torch.complex(a[2, :nj, :nk], a[3, :nj, :nk])
-            tot += sign * 0.5 * float(torch.real(torch.sum(aE * torch.conj(aH))))
-        return tot * (2.0 / n_acc) ** 2
+            out.append((sign, torch.complex(a[0, :nj, :nk], a[1, :nj, :nk]),
+                        torch.complex(a[2, :nj, :nk], a[3, :nj, :nk])))
+        return out
+
+    def flux(self, name, n_acc):
+        """Net +x Poynting flux (pairs_3d, flux.py:84-90 and :45-57)."""
+        return plane_flux(self.plane_dft(name), n_acc)
 
     def conv_change(self, n_last, n_prev):
         """||a - b|| / ||a|| of the convergence planes a = last / n_last, b = prev / n_prev

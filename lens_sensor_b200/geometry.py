@@ -418,6 +418,12 @@ class Spec3D:
     wg_width_um: Optional[float] = None  # rectangular channel: core only for |z| < width/2
     n_clad_side: float = 1.0             # index beside the channel core
     pec_faces: Tuple[str, ...] = ()      # faces without CPML (PEC mirrors)
+    # stitch window (fdtd3d_core.py:119-145, global-x mode): x of node 0 in the
+    # whole domain; the core then exists only for x in [entry facet, x_wg_end_um]
+    # and the columns outside it keep the layers below an empty core row
+    x0_um: Optional[float] = None
+    x_wg_end_um: Optional[float] = None
+    n_sp_cells: Optional[int] = None     # absorber cells fixed by the caller (window shape)
 
     @property
     def dx(self):
@@ -430,6 +436,8 @@ class Spec3D:
     @property
     def n_sp(self):
         """Sponge thickness in cells (fdtd3d_core.py:381-396), which fixes the source plane."""
+        if self.n_sp_cells is not None:
+            return int(self.n_sp_cells)
         dx_um = self.dx_nm / 1000.0
         n = int(self.n_sponge) if self.n_sponge else int(np.ceil(float(self.sponge_um) / dx_um))
         n = max(8, n)
@@ -468,20 +476,34 @@ def build_3d(sp: Spec3D):
     y0_um, z0_um = -sp.tear_um, -Nz * dx_um / 2.0
     ys = y0_um + np.arange(Ny) * dx_um
     zs = z0_um + np.arange(Nz) * dx_um
-    xs = np.arange(Nx) * dx_um
+    glob = sp.x0_um is not None
+    x0 = float(sp.x0_um) if glob else 0.0
+    xs = x0 + np.arange(Nx) * dx_um
     air = air_path_um(sp.vcsel_distance_um, dx_um)
     x_facet_um = sp.src_ix * dx_um + air
-    # column types (fdtd3d_core.py:248-261): 1 core stack, 2 channel cladding beside
-    # the core, 3 air (in front of the entry facet, over the end facet)
-    T = np.full((Nx, Nz), 1, dtype=np.int8)
+    # column types (fdtd3d_core.py:248-261): 0 layers without the core, 1 core
+    # stack, 2 channel cladding beside the core, 3 air (in front of the entry
+    # facet, over the end facet)
     channel = sp.wg_width_um is not None and 0 < sp.wg_width_um < Nz * dx_um
-    if channel:
-        T[:, np.abs(zs) > sp.wg_width_um / 2.0] = 2
-    if sp.end_facet_um and sp.end_facet_um > 0:
-        T[xs >= (Nx * dx_um - sp.end_facet_um), :] = 3
-    T[xs < x_facet_um, :] = 3
+    if glob:     # stitch window: finite core [facet, x_wg_end], no air columns
+        in_wg = xs >= x_facet_um
+        if sp.x_wg_end_um is not None:
+            in_wg &= xs <= sp.x_wg_end_um
+        T = np.zeros((Nx, Nz), dtype=np.int8)
+        T[in_wg, :] = 1
+        if channel:
+            T[np.ix_(in_wg, np.abs(zs) > sp.wg_width_um / 2.0)] = 2
+    else:
+        T = np.full((Nx, Nz), 1, dtype=np.int8)
+        if channel:
+            T[:, np.abs(zs) > sp.wg_width_um / 2.0] = 2
+        if sp.end_facet_um and sp.end_facet_um > 0:
+            T[xs >= (Nx * dx_um - sp.end_facet_um), :] = 3
+        T[xs < x_facet_um, :] = 3
     col = column_average(ys, dx_um, st.eps_of_y(1e-6, core=True))
     cols_node = {1: col, 3: np.full(Ny, N_AIR ** 2, dtype=col.dtype)}
+    if glob:
+        cols_node[0] = column_average(ys, dx_um, st.eps_of_y(1e-6, core=False))
     if channel:   # core rows (0 <= y <= t_wg) set to the cladding index at the nodes
         c2 = col.copy()
         c2[(ys >= 0.0) & (ys <= st.t_wg_um)] = sp.n_clad_side ** 2
@@ -518,7 +540,7 @@ def build_3d(sp: Spec3D):
     for bd in sp.beads:
         r = bd.d_um / 2.0
         xc, yc, zc = bd.x_um, (bd.y_um if bd.y_um is not None else -r), bd.z_um
-        i0, i1 = max(0, int((xc - r) / dx_um) - 2), min(Nx, int((xc + r) / dx_um) + 3)
+        i0, i1 = max(0, int((xc - r - x0) / dx_um) - 2), min(Nx, int((xc + r - x0) / dx_um) + 3)
         j0, j1 = max(0, int((yc - r - y0_um) / dx_um) - 2), min(Ny, int((yc + r - y0_um) / dx_um) + 3)
         k0, k1 = max(0, int((zc - r - z0_um) / dx_um) - 2), min(Nz, int((zc + r - z0_um) / dx_um) + 3)
         if not (i1 > i0 and j1 > j0 and k1 > k0):

@@ -110,6 +110,37 @@ _COMP = {0: 'Ex', 1: 'Ey', 2: 'Ez'}
 _FACES = ('xmin', 'xmax', 'ymin', 'ymax', 'zmin', 'zmax')
 
 
+class _NoSource:
+    """A stitch window without the VCSEL (fdtd3d_core.py:1609-1617)."""
+    omega = None
+
+    def inject(self, *a):
+        pass
+
+
+def plane_flux(pairs, n):
+    """flux.py:45-57: complex64 products, complex128 sum."""
+    s = 0.0
+    for sign, aE, aH in pairs:
+        e, h = aE.numpy().astype(np.complex64), aH.numpy().astype(np.complex64)
+        s += sign * 0.5 * float(np.real(np.sum(e * np.conj(h), dtype=np.complex128)))
+    return s * (2.0 / n) ** 2
+
+
+class Drive3D:
+    """Overlap drive of a stitch window, applied as fdtd3d_core.py:1614-1617 does."""
+
+    def __init__(self, grid, hand, taper):
+        self.hand = [np.asarray(torch.as_tensor(D).numpy(), np.complex64) for D in hand]
+        self.O = len(taper)
+        self.w = np.asarray(taper, F32)[:, None, None]
+
+    def apply(self, g, omega, t, env):
+        ph = np.complex64(np.exp(1j * omega * t))
+        for F, D in zip((g.Ex, g.Ey, g.Ez), self.hand):
+            F[:self.O] = self.w * (env * np.real(D * ph)) + (1.0 - self.w) * F[:self.O]
+
+
 class Grid3D:
     """3D stand-in: oracle FP32 stepping in the reference loop order
     (fdtd3d_core.py:1106-1127; CPML step, PEC, source)."""
@@ -117,9 +148,12 @@ class Grid3D:
     def __init__(self, nx, ny, nz, dx, dt, ce, da, cpml, src, src_comp=1, pec=(1,) * 6, device=None,
                  fused=True):
         self.nx, self.ny, self.nz, self.dx, self.dt = nx, ny, nz, dx, dt
-        h = O.Huygens.__new__(O.Huygens)
-        h.ix, h.omega = int(src['ix']), float(src['omega'])
-        h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
+        if src is None:
+            h = _NoSource()
+        else:
+            h = O.Huygens.__new__(O.Huygens)
+            h.ix, h.omega = int(src['ix']), float(src['omega'])
+            h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
         self.src_comp = src_comp
         faces = tuple(f for f, on in zip(_FACES, pec) if on)
         self.g = O.Grid3D(nx, ny, nz, dx, dt, cpml, ce, da, h, _COMP[src_comp], F32, faces=faces)
@@ -127,15 +161,21 @@ class Grid3D:
     def view(self, name):
         return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
 
-    def step(self, table, n0, nsteps, epi=None, stream=None):
+    def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
+        if self.g.src.omega is None:
+            self.g.src.omega = table.omega
         for n in range(n0, n0 + nsteps):
             t = n * self.dt
-            self.g.step(n, float(table.envelope(t)))
+            env = float(table.envelope(t))
+            self.g.step(n, env)
+            if drive is not None:
+                drive.apply(self.g, table.omega, t, env)
             if epi is not None:
                 epi.after(n, t, self.g)
 
-    def accum_e2(self, iavg, target=None, stream=None):
-        O.accum_e2(iavg.numpy(), self.g.Ex, self.g.Ey, self.g.Ez)
+    def accum_e2(self, iavg, target=None, stream=None, nx=None):
+        nx = self.nx if nx is None else nx
+        O.accum_e2(iavg.numpy()[:nx], self.g.Ex[:nx - 1], self.g.Ey[:nx], self.g.Ez[:nx])
 
     def check_flag(self):
         pass
@@ -157,6 +197,11 @@ class Epi3D:
         self.win = tuple(dft)
         self.comps = tuple(comps)
         self.acc = {c: np.zeros(getattr(grid.g, _COMP[c]).shape, np.complex64) for c in comps}
+        # run_3d_stitched's own accumulators (fdtd3d_core.py:1640-1649): float32
+        # re/im of the volume and complex64 overlap handoff
+        self.acc_re = {c: np.zeros(a.shape, F32) for c, a in self.acc.items()}
+        self.acc_im = {c: np.zeros(a.shape, F32) for c, a in self.acc.items()}
+        self.acc_hand = {c: np.zeros(a.shape, np.complex64) for c, a in self.acc.items()}
         self.planes = dict(planes)
         self.kc, self.prev_win = (conv[0], tuple(conv[1])) if conv is not None else (None, (0, 0))
         self.pl_a = np.zeros(cshape[:2], np.complex64)
@@ -175,8 +220,14 @@ class Epi3D:
         F = getattr(g, _COMP[self.grid.src_comp])
         if self.win[0] <= n < self.win[1]:
             ph = np.exp(-1j * self._omega * t)
+            cs, sn = F32(np.cos(self._omega * t)), F32(np.sin(self._omega * t))
+            e64 = np.complex64(np.exp(-1j * self._omega * t))
             for c in self.comps:
-                self.acc[c] += getattr(g, _COMP[c]).astype(np.complex64) * ph
+                Fc = getattr(g, _COMP[c])
+                self.acc[c] += Fc.astype(np.complex64) * ph
+                self.acc_re[c] += Fc * cs
+                self.acc_im[c] -= Fc * sn
+                self.acc_hand[c] += Fc * e64
             for k, il in self.planes.items():
                 self.flux_acc.add(k, t, g.flux_pairs(il))
             if self.kc is not None:
@@ -188,8 +239,16 @@ class Epi3D:
     def box_acc(self):
         return torch.from_numpy(self.box.copy())
 
-    def phasor(self, comp=1):
-        return torch.from_numpy(self.acc[comp].astype(np.complex128))
+    def phasor(self, comp=1, kind=None):
+        if kind == 'split':
+            return torch.complex(torch.from_numpy(self.acc_re[comp].astype(np.float64)),
+                                 torch.from_numpy(self.acc_im[comp].astype(np.float64)))
+        a = self.acc_hand[comp] if kind == 'hand' else self.acc[comp]
+        return torch.from_numpy(a.astype(np.complex128))
+
+    def plane_dft(self, name):
+        return [(sg, torch.from_numpy(aE.astype(np.complex128)), torch.from_numpy(aH.astype(np.complex128)))
+                for sg, aE, aH in self.flux_acc.acc[name]]
 
     def flux(self, name, n_acc):
         return self.flux_acc.flux(name)

@@ -18,8 +18,11 @@ Outputs:
   dropin_2d.json                       run_beads + save_results outputs (NPZ / PKL
                                        summaries) of three whole-driver cases
   dropin_3d.json                       the same for run_3d + save_results_3d
+  dropin_3d_stitch.json                the same for run_3d_stitched + save_results_3d
 
-`python tests/golden/make_golden.py dropin` stops after the two JSON files.
+`python tests/golden/make_golden.py dropin` stops after the two JSON files;
+`python tests/golden/make_golden.py stitch` writes only the stitch fixtures
+(adds case_3d_stitch to characterization.json, writes dropin_3d_stitch.json).
 """
 import json
 import os
@@ -253,6 +256,21 @@ def characterization():
     return dict(case_3d=r3, case_2d=r2)
 
 
+def characterization_stitch():
+    """The reference's 3D stitch golden-master case (tests/test_characterization.py:87-99)
+    re-run at HEAD."""
+    sys.path.insert(0, os.path.join(REF, 'tests'))
+    import test_characterization as tc
+    prev = os.getcwd()
+    tmp = tempfile.mkdtemp(prefix='lens_golden_')
+    try:
+        os.chdir(tmp)
+        return tc._run_3d_stitch_case()
+    finally:
+        os.chdir(prev)
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 # ------------------------------------------------------------- drop-in run_beads
 # Whole-driver cases: fdtd2d_core.run_beads + save_results (method='full', CPML, CW).
 # 'te' is the reference's characterization case; 'tm_kappa' adds KAPPA losses on the
@@ -380,7 +398,78 @@ def dropin_3d():
     return out
 
 
+# ------------------------------------------------------ drop-in run_3d_stitched
+# Whole-driver cases: fdtd3d_core.run_3d_stitched + save_results_3d.  'goldenstitch' is
+# the reference's characterization case (TE, 3 windows, the last one flush with the
+# domain end so two windows assemble the same planes); 'tm_stack' a TM run over 4
+# windows on an absorbing custom stack, a rectangular channel, a bead across a window
+# seam, an input gap and a tilted offset source.
+DROPIN_3D_STITCH = dict(
+    goldenstitch=dict(kw=dict(label='goldenstitch', wg_n=1.491, window_w_um=2.0, slide_um=1.2, lx_um=4.0,
+                              air_um=1.0, tear_um=2.0, lz_um=2.0, dx_nm=100.0, t_wg_um=1.0, t_aq_um=1.0,
+                              t_mu_um=0.5, lam_nm=850.0, n_snapshots=2, vcsel_waist_um=1.0,
+                              vcsel_waist_z_um=1.0, bead=dict(x_um=2.0, d_um=0.5, n=1.59), n_sponge=8),
+                      kappa={}),
+    tm_stack=dict(kw=dict(label='tm_stack', wg_n=1.49, window_w_um=2.2, slide_um=1.0, lx_um=5.0, air_um=0.6,
+                          tear_um=2.0, lz_um=2.0, dx_nm=100.0, t_wg_um=0.9, lam_nm=850.0, n_snapshots=3,
+                          vcsel_waist_um=0.9, vcsel_waist_z_um=0.7, vcsel_tilt_deg=2.0, vcsel_offset_y_um=0.05,
+                          vcsel_offset_z_um=-0.1, input_gap_um=1.5, wg_width_um=1.2, n_clad_side=1.33,
+                          bead=dict(x_um=2.1, d_um=0.6, n=1.59, z_um=0.15), n_sponge=8, polarization='p',
+                          stack=[dict(name='Aqueous', t_um=1.0, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                                 dict(name='Mucin', t_um=0.3, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+                  kappa={}),
+)
+
+
+def dropin_3d_stitch():
+    """Run the reference stitch driver end to end for DROPIN_3D_STITCH and summarise."""
+    import glob
+    import pickle
+    out = {}
+    for name, c in DROPIN_3D_STITCH.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_stitch_')
+        old_k = d3.KAPPA
+        try:
+            os.chdir(tmp)
+            d3.KAPPA = dict(c['kappa'])
+            r = d3.run_3d_stitched(**c['kw'])
+            res = dict(transmission=float(r['transmission']), P_in=float(r['P_in']), P_out=float(r['P_out']),
+                       transmission_intensity=float(r['transmission_intensity']),
+                       steps_total=int(r['steps_total']))
+            d3.save_results_3d(r)
+            files = {}
+            for f in sorted(glob.glob('results/*.npz')):
+                z = np.load(f)
+                files[os.path.basename(f).replace(c['kw']['label'], '{label}')] = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+            left = sorted(os.listdir('results'))
+        finally:
+            d3.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        kw = {k: v for k, v in c['kw'].items() if k != 'stack'}
+        out[name] = dict(kw=kw, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         result=res, npz=files, pkl=scal, files_left=left)
+    return out
+
+
 def main():
+    if 'stitch' in sys.argv[1:]:
+        path = os.path.join(OUT, 'characterization.json')
+        ch = json.load(open(path))
+        ch['case_3d_stitch'] = characterization_stitch()
+        with open(path, 'w') as f:
+            json.dump(ch, f, indent=1)
+        with open(os.path.join(OUT, 'dropin_3d_stitch.json'), 'w') as f:
+            json.dump(dropin_3d_stitch(), f, indent=1)
+        print('wrote case_3d_stitch, dropin_3d_stitch.json')
+        return
     ch = characterization()          # first: the cases below change module globals
     with open(os.path.join(OUT, 'characterization.json'), 'w') as f:
         json.dump(ch, f, indent=1)

@@ -153,8 +153,12 @@ typedef struct {
                                     (shapes as in LensTE2D / LensTM2D)          */
     int pec[4];
     LensSource src;              /* drives Ez (TE) or Ey (TM)                   */
-    int dft_n0, dft_n1;
+    int dft_n0, dft_n1;          /* in the instance's own steps                 */
     float *dft;                  /* (nx, pitch) x {re, im} or NULL              */
+    int n_start;                 /* batch step at which this instance's step 0
+                                    runs: its own step is n - n_start (source
+                                    time, DFT window, table row), so instances
+                                    can join a batch that is already running    */
 } LensInst2D;
 
 /* Block plan of a batch for tiles of 32 columns x 4*by rows: writes blk[0..ninst]
@@ -162,9 +166,11 @@ typedef struct {
  * instance of block b, one entry per block); returns the block count, or < 0. */
 int lens_batch2d_plan(const LensInst2D *inst, int ninst, int by, int *blk, int *owner);
 
-/* Advance every instance by nsteps from step n0.  inst_host / inst_dev: the
- * same instance array in host and device memory; blk_dev / owner_dev: the
- * plan's tables in device memory; storage: LENS_F32 / LENS_F16 / LENS_BF16. */
+/* Advance every instance by nsteps from batch step n0.  inst_host / inst_dev:
+ * the same instance array in host and device memory; blk_dev / owner_dev: the
+ * plan's tables in device memory; storage: LENS_F32 / LENS_F16 / LENS_BF16.
+ * The table must hold every instance's own steps [n0 - n_start, n0 + nsteps -
+ * n_start).                                                                  */
 int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
                       const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
                       int n0, int nsteps, void *stream);

@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(256)
     const LensSource &src = tl.g->src;
     const int *pec = tl.g->pec;
     const int six = __ldg(&src.ix), snj = __ldg(&src.nj);
+    n -= __ldg(&tl.g->n_start);  // the instance's own step
     const int pec0 = __ldg(pec), pec1 = __ldg(pec + 1), pec2 = __ldg(pec + 2), pec3 = __ldg(pec + 3);
     if (g.pol() == 0) {  // TE: Ez (boundaries.py:196-215), source, PEC, node DFT
         if (i0 >= nx || j >= ny) return;
@@ -324,6 +325,7 @@ __global__ void __launch_bounds__(256)
     if (g.pol() != 1) return;
     const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
     if (i0 >= nx || j >= ny) return;
+    n -= __ldg(&tl.g->n_start);
     using S = St<T>;
     const void *p1 = g.f(1);
 #pragma unroll
@@ -363,7 +365,8 @@ void launch(const LensInst2D *dev, const int *blk, const int *owner, int ninst, 
         if (tm_dft) {
             bool any = false;
             for (int q = 0; q < ninst && !any; ++q)
-                any = host[q].pol == 1 && host[q].dft && n >= host[q].dft_n0 && n < host[q].dft_n1;
+                any = host[q].pol == 1 && host[q].dft && n - host[q].n_start >= host[q].dft_n0 &&
+                      n - host[q].n_start < host[q].dft_n1;
             if (any) b2d_tm_node<T><<<nblk, b, 0, s>>>(dev, blk, owner, tab, n);
         }
     }
@@ -390,13 +393,12 @@ extern "C" int lens_batch2d_plan(const LensInst2D *inst, int ninst, int by, int 
 extern "C" int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
                                  const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
                                  int n0, int nsteps, void *stream) {
-    if (!inst_host || !inst_dev || !blk_dev || !owner_dev || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0 ||
-        !lens_table_ok(tab, n0, nsteps))
+    if (!inst_host || !inst_dev || !blk_dev || !owner_dev || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0)
         return LENS_ERR_ARG;
     long tot = 0;
     bool tm_dft = false, any_dft = false;
     for (int q = 0; q < ninst; ++q) {
-        if (!inst_ok(inst_host[q])) return LENS_ERR_ARG;
+        if (!inst_ok(inst_host[q]) || !lens_table_ok(tab, n0 - inst_host[q].n_start, nsteps)) return LENS_ERR_ARG;
         tot += inst_blocks(inst_host[q], by);
         tm_dft = tm_dft || (inst_host[q].pol == 1 && inst_host[q].dft);
         any_dft = any_dft || inst_host[q].dft;
@@ -477,7 +479,7 @@ __global__ void na_owner(const int *blk, int ninst, int *owner, int nblk) {
 
 extern "C" int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int storage, int by,
                                          const LensStepTable *tab, int n0, int nsteps, void *stream) {
-    if (!inst || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) ||
+    if (!inst || ninst < 1 || by < 1 || BXB * by > 256 || nsteps < 0 ||
         (storage != LENS_F32 && storage != LENS_F16 && storage != LENS_BF16))
         return LENS_ERR_ARG;
     if (ninst > NA_MAX_INST) return LENS_ERR_SIZE;
@@ -485,7 +487,7 @@ extern "C" int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int 
     long tot = 0;
     bool tm_dft = false, any_dft = false;
     for (int q = 0; q < ninst; ++q) {
-        if (!inst_ok(inst[q])) return LENS_ERR_ARG;
+        if (!inst_ok(inst[q]) || !lens_table_ok(tab, n0 - inst[q].n_start, nsteps)) return LENS_ERR_ARG;
         blk[q] = (int)tot;
         tot += inst_blocks(inst[q], by);
         if (tot > NA_MAX_BLOCKS) return LENS_ERR_SIZE;

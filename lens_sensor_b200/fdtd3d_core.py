@@ -18,8 +18,9 @@ import numpy as np
 import torch
 
 from . import engine as E
-from .geometry import Sphere, Spec3D, Stack, air_path_um, build_3d
+from .geometry import Sphere, Spec3D, Stack, build_3d
 from .physics import C0
+from .stitch3d import StitchPlan, StitchSolve
 
 # module switches the reference's driver sets (fdtd3d_core.py:52-60)
 KAPPA = {}
@@ -266,39 +267,6 @@ def run_3d(label, wg_n, t_wg_um=5.0,
                 x_src_um=x_src_um, polarization=pol, cad=None, cad_region=None)
 
 
-def _window_bytes(nxw, Ny, Nz, lossy, ncomp):
-    """Device bytes of one stitch window on the engine: two field + psi buffers,
-    coefficients (+ damping), DFT sums of ncomp components, Iavg."""
-    cells = nxw * Ny * (-(-Nz // 32) * 32)     # z padded to the engine's 32-float pitch
-    return cells * 4 * (2 * (6 + 12) + 3 + (3 if lossy else 0) + 2 * ncomp + 1)
-
-
-class _FluxSum:
-    """Plane DFTs summed over the windows that carry the plane (one running
-    PlaneFluxDFT across windows, fdtd3d_core.py:1552, 1644-1645)."""
-
-    def __init__(self):
-        self.acc, self.n = {}, {}
-
-    def add(self, key, pairs, n):
-        if key not in self.acc:
-            self.acc[key] = [[sg, aE.clone(), aH.clone()] for sg, aE, aH in pairs]
-            self.n[key] = 0
-        else:
-            for a, (sg, aE, aH) in zip(self.acc[key], pairs):
-                a[1] += aE
-                a[2] += aH
-        self.n[key] += int(n)
-
-    def has(self, key):
-        return self.n.get(key, 0) > 0
-
-    def flux(self, key):
-        if not self.has(key):
-            return float('nan')
-        return E.plane_flux(self.acc[key], self.n[key])
-
-
 def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
                     t_wg_um=5.0, t_lip_um=0.0, t_aq_um=3.5, t_mu_um=0.5,
                     n_lip=1.480, n_aq=1.336, n_mu=1.342, n_co=1.376,
@@ -314,56 +282,24 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
     """3D CW solve by domain decomposition along x (fdtd3d_core.py:1311-1782).
 
     Windows of window_w_um slide by slide_um; each runs to steady state on the
-    engine.  Window 0 carries the VCSEL source; window w > 0 is driven on its
-    first O = window - slide planes by the complex Ex, Ey, Ez amplitudes of the
-    previous window's overlap (cosine taper 1 -> 0), which stay on the device
-    from one window to the next.  Interior window ends get a CPML in an
-    absorber extension that is neither assembled nor handed over.  The driven
-    component's amplitude and <|E|^2> are assembled over the whole length
-    (disk memmaps, like the reference) and written out as CW phase frames.
-    Supported: boundary='cpml', no CAD; other requests raise NotImplementedError."""
+    engine (stitch3d.StitchSolve).  Window 0 carries the VCSEL source; window
+    w > 0 is driven on its first O = window - slide planes by the complex Ex,
+    Ey, Ez amplitudes of the previous window's overlap (cosine taper 1 -> 0),
+    which stay on the device from one window to the next.  Interior window ends
+    get a CPML in an absorber extension that is neither assembled nor handed
+    over.  The driven component's amplitude and <|E|^2> are assembled over the
+    whole length (disk memmaps, like the reference) and written out as CW phase
+    frames.  Supported: boundary='cpml', no CAD; other requests raise
+    NotImplementedError."""
     bad = [nm for nm, v in (('cad', cad is not None), ('boundary', str(boundary or 'cpml').lower() != 'cpml'),
                             ('SRC_CORE_ONLY', bool(SRC_CORE_ONLY)), ('BEAD_SUBPIXEL', not BEAD_SUBPIXEL)) if v]
     if bad:
         raise NotImplementedError(f'lens_sensor_b200.run_3d_stitched: {", ".join(bad)}: only the CPML '
                                   f'stitch runs on the B200 engine')
     t_total = time.time()
-    dx = dx_nm * 1e-9
     dx_um = dx_nm / 1000.0
-    dt = 0.5 * dx / (C0 * np.sqrt(3))
-    LAM = lam_nm * 1e-9
-    f0 = C0 / LAM
-    omega = 2 * np.pi * f0
     tear_um = _resolve_tear_um(tear_um, t_lip_um, t_aq_um, t_mu_um, 10, dx_um, stack=stack)
     ly_um = t_wg_um + air_um + tear_um
-    y0_um, z0_um = -tear_um, -lz_um / 2.0
-    Ny, Nz = int(round(ly_um / dx_um)), int(round(lz_um / dx_um))
-    Nx_full = int(round(lx_um / dx_um))
-    Nx_win = min(int(round(window_w_um / dx_um)), Nx_full)
-    S_cells = max(1, min(int(round(slide_um / dx_um)), Nx_win))
-    O_cells = Nx_win - S_cells
-    n_sp = int(n_sponge) if n_sponge else int(np.ceil(float(sponge_um) / dx_um))
-    n_sp = min(max(8, n_sp), max(8, min(Nx_win, Ny, Nz) // 6))
-    vd = float(input_gap_um or 0.0)
-    src_ix = n_sp + 6
-    x_src_um = src_ix * dx_um
-    x_wg_start_um = x_src_um + air_path_um(vd, dx_um)
-    EXT = max(n_sp, 10) + 4              # CPML extension behind interior window ends
-    x_wg_end_um = lx_um + EXT * dx_um    # the core runs on into the absorber
-    n_win = (int(np.ceil((Nx_full - Nx_win) / S_cells)) + 1) if Nx_full > Nx_win else 1
-
-    def gx0(w):                          # the last window ends flush with the domain
-        return min(w * S_cells, max(Nx_full - Nx_win, 0))
-    transit = window_w_um * 1e-6 * N_G_FACTOR * wg_n / C0
-    steps_win = int(3.0 * transit / dt) + 400
-    steps_per_T = max(4, int(round((1.0 / f0) / dt)))
-    n_acc = steps_per_T * 8
-    base = steps_win - n_acc             # DFT / flux / handoff / Iavg from here to the window end
-    n_w0 = max(0, base)
-    acc_n = steps_win - n_w0
-    m_I = max(1, int(round((1.0 / f0) / dt)) // 8)
-    pol = 'p' if str(polarization).lower() in ('p', 'tm') else 's'
-    Nj, Nk = (Ny - 1, Nz) if pol == 'p' else (Ny, Nz - 1)
     lossy = _stack_lossy(stack)
     kp = dict(KAPPA or {})
     cplx = (lambda n, key: complex(float(np.real(n)), kp.get(key, 0.0)) if lossy else float(np.real(n)))
@@ -378,28 +314,18 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
     if bead is not None and bead.get('d_um', 0) > 0:
         beads.append(Sphere(bead['x_um'], bead['d_um'], cplx(bead['n'], 'bead') if lossy else bead['n'],
                             bead.get('y_um'), bead.get('z_um', 0.0)))
-    # detector planes in global x (fdtd3d_core.py:1521-1550)
-    det_in_um = 0.2 * lx_um if det_in_um is None else det_in_um
-    det_out_um = 0.8 * lx_um if det_out_um is None else det_out_um
-    j_wg0, j_wg1 = int(round((0.0 - y0_um) / dx_um)), int(round((t_wg_um - y0_um) / dx_um))
-    gi = _guard_in_plane(min(max(int(round(det_in_um / dx_um)), 1), Nx_full - 2),
-                         max(src_ix, int(round(x_wg_start_um / dx_um))), Nx_full)
-    det_in_um = gi * dx_um
-    go = min(max(int(round(det_out_um / dx_um)), 1), Nx_full - 2)
-    plan = []
-    for w in range(n_win):
-        g0, last = gx0(w), w == n_win - 1
-        glo = 0 if w == 0 else g0 + O_cells
-        ghi = Nx_full if last else min(g0 + Nx_win, Nx_full)
-        fpl = {k: g - g0 for k, g in (('in', gi), ('out', go)) if glo <= g < ghi and g - g0 >= 1}
-        if w == 0:
-            fpl.update(src_up=src_ix - 1, src_dn=src_ix + 3)
-        plan.append((g0, last, fpl))
-    if not all(any(k in p[2] for p in plan) for k in ('in', 'out')):
+    pl = StitchPlan(st, tear_um, lx_um, ly_um, lz_um, dx_nm, window_w_um, slide_um, wg_n, pol=polarization,
+                    lam_nm=lam_nm, beads=beads, n_sponge=n_sponge, sponge_um=sponge_um, input_gap_um=input_gap_um,
+                    waist_um=vcsel_waist_um, waist_z_um=vcsel_waist_z_um, tilt_deg=vcsel_tilt_deg,
+                    offset_y_um=vcsel_offset_y_um, offset_z_um=vcsel_offset_z_um, wg_width_um=wg_width_um,
+                    n_clad_side=n_clad_side, det_in_um=det_in_um, det_out_um=det_out_um, n_g_factor=N_G_FACTOR)
+    if not pl.planes_covered():
         raise NotImplementedError('lens_sensor_b200.run_3d_stitched: a detector plane falls on a window '
                                   'start (no overlap); the intensity-based fallback is not built')
+    dx, f0, omega = pl.dx, pl.f0, pl.omega
+    Nx_full, Nj, Nk, n_sp = pl.Nx_full, pl.Nj, pl.Nk, pl.n_sp
     # device footprint of one window (fdtd3d_core.py:1405-1450): refuse before the run
-    need = _window_bytes(Nx_win + EXT, Ny, Nz, lossy, 3)
+    need = pl.window_bytes(3, lossy)
     if torch.cuda.is_available():
         free = torch.cuda.mem_get_info()[0]
         if need > 0.85 * free:
@@ -426,61 +352,15 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
     ia_path = os.path.join('results', f'_stream3d_{safe}_stitch_Iavg.npy')
     stream_paths.append(ia_path)
     Iavg = np.lib.format.open_memmap(ia_path, mode='w+', dtype=np.float32, shape=(Nx_full, Nj, Nk))
-    wtap = (0.5 * (1.0 + np.cos(np.pi * np.arange(O_cells) / max(O_cells - 1, 1)))).astype(np.float32)
-    tab = E.StepTable(0, steps_win, dt, omega, omega, E.cw_envelope(f0))
-    comp = 1 if pol == 'p' else 2
-    sc = torch.tensor(2.0 / max(acc_n, 1), dtype=torch.float32)
-    flux = _FluxSum()
-    hand = None
-    geo0 = None
-    for w, (g0, last, fpl) in enumerate(plan):
-        Nxw = Nx_win + (0 if last else EXT)
-        sp = Spec3D(pol, Nxw, Ny, Nz, dx_nm, st, tear_um, beads, npml=10, lam_nm=lam_nm, waist_um=vcsel_waist_um,
-                    waist_z_um=vcsel_waist_z_um, offset_y_um=vcsel_offset_y_um, offset_z_um=vcsel_offset_z_um,
-                    tilt_deg=vcsel_tilt_deg, vcsel_distance_um=vd, end_facet_um=0.0, wg_width_um=wg_width_um,
-                    n_clad_side=n_clad_side, pec_faces=(('xmin',) if w > 0 else ()), x0_um=g0 * dx_um,
-                    x_wg_end_um=x_wg_end_um, n_sp_cells=n_sp)
-        geo = build_3d(sp)
-        if w == 0:
-            geo0 = geo
-        # window 0: VCSEL source, CPML + PEC all round; later windows: driven, open at x-lo
-        grid = E.Grid3D(Nxw, Ny, Nz, dx, dt, geo['ce'], geo['da'], geo['cpml'],
-                        geo['src'] if w == 0 else None, src_comp=comp,
-                        pec=((1,) if w == 0 else (0,)) + (1,) * 5, fused=True)
-        comps = (comp,) if last else (0, 1, 2)
-        ep = E.Epi3D(grid, dft=(n_w0, steps_win), comps=comps, planes=fpl, iavg=True)
-        drive = E.Drive3D(grid, hand, wtap) if (w > 0 and hand is not None and O_cells > 0) else None
-        n, n_I = 0, 0
-        while n < steps_win:             # run to the next <|E|^2> sample (every m_I steps)
-            ev = n_w0 if n <= n_w0 else n + (base - n) % m_I
-            ev = min(ev, steps_win - 1)
-            grid.step(tab, n, ev - n + 1, ep, drive=drive)
-            if ev >= base and (ev - base) % m_I == 0:
-                grid.accum_e2(ep.iavg, nx=Nx_win)
-                n_I += 1
-            n = ev + 1
-        grid.check_flag()
-        ph = ep.phasor(comp, kind='split')[:Nx_win]
-        Ew = torch.complex(ph.real.float() * sc, ph.imag.float() * sc).cpu().numpy()
-        if not last and O_cells > 0:         # handoff: stays on the device
-            off = gx0(w + 1) - g0
-            hand = []
-            for c in range(3):
-                a = ep.phasor(c, kind='hand')[off:off + O_cells]
-                hand.append(torch.complex(a.real.float() * sc.to(a.device), a.imag.float() * sc.to(a.device)))
-        for key in fpl:
-            flux.add(key, ep.plane_dft(key), acc_n)
-        l_lo, g_lo = (0, 0) if w == 0 else (O_cells, g0 + O_cells)
-        g_hi = Nx_full if last else min(g0 + Nx_win, Nx_full)
-        l_hi = l_lo + (g_hi - g_lo)
-        if g_hi > g_lo:
-            Efull[g_lo:g_hi] = Ew[l_lo:l_hi]
-            ia = ep.iavg[l_lo:l_hi, :Nj, :Nk] * torch.tensor(1.0 / max(n_I, 1), dtype=torch.float32).to(
-                ep.iavg.device)
-            Iavg[g_lo:g_hi] = ia.cpu().numpy()
-        del grid, ep, drive, Ew
+
+    def sink(w, g_lo, g_hi, Ew, Ia):
+        Efull[g_lo:g_hi] = Ew
+        Iavg[g_lo:g_hi] = Ia
         Efull.flush()
         Iavg.flush()
+    job = StitchSolve(pl, E, sink)
+    while not job.done:
+        job.advance(pl.steps_win)
     total_time = time.time() - t_total
     nfr = max(1, n_snapshots)
     vp = os.path.join('results', f'_stream3d_{safe}_stitch_ez.npy')
@@ -498,17 +378,18 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
     vol_buf.flush()
     Iavg.flush()
     # sensor figures from <|E|^2> on single x planes (fdtd3d_core.py:1713-1719)
+    det_in_um, det_out_um = pl.det_in_um, pl.det_out_um
     iin = min(max(int(round(det_in_um / dx_um)), 0), Nx_full - 1)
     iout = min(max(int(round(det_out_um / dx_um)), 0), Nx_full - 1)
-    P_in = 2.0 * float(np.sum(np.asarray(Iavg[iin, j_wg0:j_wg1, n_sp:-n_sp]))) * dx ** 3
-    P_out = 2.0 * float(np.sum(np.asarray(Iavg[iout, j_wg0:j_wg1, n_sp:-n_sp]))) * dx ** 3
+    P_in = 2.0 * float(np.sum(np.asarray(Iavg[iin, pl.j_wg0:pl.j_wg1, n_sp:-n_sp]))) * dx ** 3
+    P_out = 2.0 * float(np.sum(np.asarray(Iavg[iout, pl.j_wg0:pl.j_wg1, n_sp:-n_sp]))) * dx ** 3
     Tr_I = P_out / max(P_in, 1e-30)
-    Tr, tr_def, p_si = Tr_I, 'intensity', None
-    if flux.has('in') and flux.has('out'):
-        S_in, S_out = flux.flux('in'), flux.flux('out')
-        p_si = S_in * dx * dx
-        if abs(S_in) > 0:
-            Tr, tr_def = S_out / S_in, 'poynting'
+    Tr, tr_def = Tr_I, 'intensity'
+    T = job.transmission()
+    if T == T:
+        Tr, tr_def = T, 'poynting'
+    vc = job.vcsel()
+    p_si = vc['p_in']
     Efull_ret = np.array(Efull) if return_efull else None
     try:
         Efull._mmap.close()
@@ -521,26 +402,24 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
     else:
         rs = (_legacy_stack(t_lip_um, n_lip, t_aq_um, n_aq, t_mu_um, n_mu), False,
               (t_lip_um * 1e-6, t_aq_um * 1e-6, t_mu_um * 1e-6, n_aq))
-    air = geo0['src']['air_um']
-    vres = dict(laser_power_mw=LASER_POWER_MW, vcsel_distance_um=vd, vcsel_air_um=float(air),
-                x_facet_um=float(x_wg_start_um), vcsel_waist_um=float(vcsel_waist_um),
+    vres = dict(laser_power_mw=LASER_POWER_MW, vcsel_distance_um=pl.vd, vcsel_air_um=float(job.geo0['src']['air_um']),
+                x_facet_um=float(pl.x_wg_start_um), vcsel_waist_um=float(vcsel_waist_um),
                 vcsel_waist_z_um=float(vcsel_waist_z_um))
-    cw_ok = source_type != 'pulse' and flux.has('src_up') and flux.has('src_dn')
-    p_emit = (flux.flux('src_dn') - flux.flux('src_up')) * dx * dx if cw_ok else None
-    p_refl = -flux.flux('src_up') * dx * dx if cw_ok else None
+    cw_ok = source_type != 'pulse' and vc['p_emit'] is not None
+    p_emit = vc['p_emit'] if cw_ok else None
     vres['p_src_si'] = p_emit
     if p_emit and p_emit > 0:
         vres.update(coupling_efficiency=(p_si / p_emit) if p_si is not None else float('nan'),
-                    facet_reflection=p_refl / p_emit)
+                    facet_reflection=vc['p_refl'] / p_emit)
     return dict(**vres, scenario=label, dim='3D', P_in=P_in, P_out=P_out, p_in_si=p_si, p_in_unit='W',
                 transmission=Tr, vols_array=vol_buf, vols_ex=None, vols_ey=None, vector=False,
                 _stream_paths=stream_paths, snap_steps=snap_steps, snap_times=snap_times, Iavg=Iavg,
-                total_time=total_time, steps_total=steps_win * n_win, dt=dt, dx_nm=dx_nm, lx_um=lx_um,
-                ly_um=ly_um, lz_um=lz_um, y0_um=y0_um, z0_um=z0_um, t_wg_um=t_wg_um, wg_n=wg_n,
+                total_time=total_time, steps_total=pl.steps_win * pl.n_win, dt=pl.dt, dx_nm=dx_nm, lx_um=lx_um,
+                ly_um=ly_um, lz_um=lz_um, y0_um=pl.y0_um, z0_um=pl.z0_um, t_wg_um=t_wg_um, wg_n=wg_n,
                 layers=rs[2], stack=rs[0], stack_custom=rs[1], n_lip=n_lip, n_aq=n_aq, n_mu=n_mu, n_co=n_co,
                 lam_nm=lam_nm, source_type=source_type, bead=(bead if bead else {}), det_in_um=det_in_um,
-                det_out_um=det_out_um, x_wg_start_um=x_wg_start_um, end_facet_um=0.0, x_src_um=x_src_um,
-                polarization=pol, view_primary='cw', cw_only=True, cad=None, cad_region=None, Efull=Efull_ret,
+                det_out_um=det_out_um, x_wg_start_um=pl.x_wg_start_um, end_facet_um=0.0, x_src_um=pl.x_src_um,
+                polarization=pl.pol, view_primary='cw', cw_only=True, cad=None, cad_region=None, Efull=Efull_ret,
                 transmission_intensity=Tr_I, transmission_def=tr_def)
 
 

@@ -120,9 +120,13 @@ class Solve3D:
         comp = self.spec.src_comp if comp is None else comp
         return (2.0 / self.n_acc) * self.epi.phasor(comp)
 
-    def results(self):
+    def results(self, stream=None):
+        """Scalars of the finished solve; waits for `stream` (default: the device)."""
         sp, ep = self.spec, self.epi
-        torch.cuda.synchronize()
+        if stream is not None:
+            stream.synchronize()
+        else:
+            torch.cuda.synchronize()
         self.grid.check_flag()
         dx = sp.dx
         box = ep.box_acc.double().cpu().numpy()

@@ -241,6 +241,70 @@ def run_batched(plain_sample=16):
                 K_median=float(np.median(K)))
 
 
+def run_stitch(windows=3):
+    """Config 3 windows: a 3D stitch of `windows` windows of 480 x 192 x 256 cells
+    (30 nm, 40-cell overlap; 19 windows = the whole 240 um config) through
+    stitch3d.StitchSolve: per-window geometry built on a host thread while the
+    previous window runs, steady-state steps, on-device handoff of the overlap
+    amplitudes, assembly to host memory.  Rate = cell updates of every window
+    (absorber extension included) over the wall time from the first window's
+    setup to the last window's assembled slab."""
+    import concurrent.futures as cf
+    import torch
+    from lens_sensor_b200 import engine as E
+    from lens_sensor_b200.stitch3d import StitchSolve
+    from lens_sensor_b200.workloads import config3
+    windows = 19 if windows <= 0 else windows
+    pl = config3(nx_full=480 + (windows - 1) * 440)
+    Ef = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.complex64)
+    Ia = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.float32)
+
+    def sink(w, g_lo, g_hi, Ew, I):
+        Ef[g_lo:g_hi] = Ew
+        Ia[g_lo:g_hi] = I
+    pool = cf.ThreadPoolExecutor(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    job = StitchSolve(pl, E, sink, pool=pool)
+    while not job.done:
+        job.advance(pl.steps_win)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    pool.shutdown()
+    cu = pl.cell_updates()
+    T = job.transmission()
+    del job
+    torch.cuda.empty_cache()
+    return dict(workload=f'config3: 3D stitch, {pl.n_win} windows of {pl.Nx_win} x {pl.Ny} x {pl.Nz} @ 30 nm '
+                         f'(+{pl.EXT}-cell absorber on interior windows), {pl.O}-cell overlap, '
+                         f'{pl.steps_win} steps per window; {pl.Nx_full} cells = {pl.lx_um:.1f} um',
+                unit=UNIT, value=cu / wall, wall_s=wall, cell_updates=cu, windows=pl.n_win,
+                steps_per_window=pl.steps_win, transmission=T,
+                handoff='on device (3 complex components x overlap planes)',
+                full_config_windows=19)
+
+
+def run_serving(count=32, seed=4):
+    """Config 4: the first `count` requests of the seeded Poisson stream (mean 50
+    req/s; 70 % 2D, 25 % 3D, 5 % stitch) replayed in real time through
+    serve.Server (160 GB budget).  Latency = completion (result on the host)
+    minus arrival."""
+    import torch
+    from lens_sensor_b200.serve import Request, Server, summary
+    from lens_sensor_b200.workloads import config4
+    reqs = [Request(i, k, sp, n, t) for i, (k, sp, n, t) in enumerate(config4(seed=seed, count=count))]
+    srv = Server()
+    done = srv.run(reqs)
+    out = summary(done)
+    torch.cuda.empty_cache()
+    out.update(workload=f'config4: first {count} requests of the seeded Poisson stream (50 req/s): '
+                        f'{sum(r.kind == "2d" for r in reqs)} 2D, {sum(r.kind == "3d" for r in reqs)} 3D, '
+                        f'{sum(r.kind == "stitch" for r in reqs)} stitch',
+               unit=UNIT, value=out['cell_updates_per_s'], budget_bytes=srv.budget, slots3d=srv.slots3d,
+               arrival_span_s=max(r.arrival for r in reqs), gpu_launches=srv.launched)
+    return out
+
+
 def ours_arm(args):
     import torch
     ws, rank, local = dist_env()
@@ -320,6 +384,8 @@ def ours_arm(args):
     if not args.no_e2e:
         e2e = run_e2e(spec, steps_total, cells, ws, pg)
     batched = run_batched() if (ws == 1 and not args.no_batch) else None
+    stitch = run_stitch(args.stitch_windows) if (ws == 1 and not args.no_stitch) else None
+    serving = run_serving(args.serve_requests) if (ws == 1 and not args.no_serve) else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, info = cpu_baseline(spec)
@@ -338,7 +404,8 @@ def ours_arm(args):
                                   launch_ms=t_launch * 1e3,
                                   mix_alg_bytes_per_cell_update=alg / (cells * K),
                                   mix_achieved=alg / (ms * 1e-3) / 1e9),
-                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches, batched=batched)
+                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches, batched=batched,
+                    stitch=stitch, serving=serving)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -354,6 +421,10 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
     ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (config 2)')
+    ap.add_argument('--no-stitch', action='store_true', help='skip the 3D stitch (config 3 windows)')
+    ap.add_argument('--stitch-windows', type=int, default=3, help='stitch windows (0: all 19 of config 3)')
+    ap.add_argument('--no-serve', action='store_true', help='skip the serving stream (config 4)')
+    ap.add_argument('--serve-requests', type=int, default=32, help='requests of the config-4 stream')
     args = ap.parse_args()
     if args.impl == 'reference':
         reference_arm(args)

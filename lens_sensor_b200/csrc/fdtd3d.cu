@@ -506,6 +506,7 @@ constexpr int MAXCH = 96;
 struct Work {
     int ntz, nty, nc;
     int lo[3], hi[3];  // lean core: z-tiles, y-tiles, chunks
+    int plo[3], phi[3];  // z-tiles, y-tiles, chunks without z / y / x CPML psi
     int x[MAXCH + 1];  // chunk c covers planes [x[c], x[c+1])
 };
 
@@ -552,14 +553,16 @@ __host__ __device__ __forceinline__ bool work_tile(const Work &wk, int id, int &
     return false;
 }
 
+// CPML axes whose psi a tile carries (template mask M of the tile pass).
+enum : unsigned { AXZ = 1u, AXY = 2u, AXX = 4u, AXALL = 7u };
+
 // Per-cell flags of an owner row.
 enum : unsigned {
     F_IN = 1u, F_HX = 2u, F_HY = 4u, F_HZ = 8u,     // in the domain; H components that update
     F_EXU = 16u, F_EYU = 32u, F_EZU = 64u,          // E components whose curl term applies (j,k part)
     F_EYV = 128u, F_EZV = 256u,                     // Ey, Ez exist (j < ny-1, k < nz-1)
     F_PJ = 512u, F_PK = 1024u,                      // on a PEC face in y / z
-    F_ZH = 2048u, F_YH = 4096u, F_ZE = 8192u, F_YE = 16384u,  // in a z / y psi strip (H / E)
-    F_BOX0 = 1u << 16                               // bit 16 + 3b + c: component c inside box b (y, z)
+    F_ZH = 2048u, F_YH = 4096u, F_ZE = 8192u, F_YE = 16384u   // in a z / y psi strip (H / E)
 };
 
 __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep, int j, int k) {
@@ -580,11 +583,6 @@ __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep,
     if (in_strip(g.ay.h, j)) f |= F_YH;
     if (in_strip(g.az.e, k)) f |= F_ZE;
     if (in_strip(g.ay.e, j)) f |= F_YE;
-    for (int b = 0; b < LENS_MAX_BOX; ++b)
-        for (int c = 0; c < 3; ++c)
-            if (b < ep.nbox && j >= ep.box[b][2] && j < box_end(ep.box[b][3], ny - (c == 1)) &&
-                k >= ep.box[b][4] && k < box_end(ep.box[b][5], nz - (c == 2)))
-                f |= F_BOX0 << (3 * b + c);
     return f;
 }
 
@@ -607,13 +605,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Stage the H-psi of one cell (hx_z, hx_y, hy_x, hy_z, hz_y, hz_x) into dst + q*NT3*4.
-template <typename IX>
+// Stage the H-psi of one cell (hx_z, hx_y, hy_x, hy_z, hz_y, hz_x) into dst + q*NT3*4;
+// only the components of the axes in M (the others are never read).
+template <unsigned M, typename IX>
 __device__ __forceinline__ void stage_hpsi(uint32_t dst, const K3 &g, IX o, unsigned f, bool xh) {
     const bool in = f & F_IN, z = in && (f & F_ZH), y = in && (f & F_YH), x = in && xh;
     const bool on[6] = {z, y, x, z, y, x};
+    constexpr unsigned ax[6] = {AXZ, AXY, AXX, AXZ, AXY, AXX};
 #pragma unroll
-    for (int q = 0; q < 6; ++q) cp_async4(dst + q * NT3 * 4, on[q] ? g.pr[q] + o : g.pr[q], on[q]);
+    for (int q = 0; q < 6; ++q)
+        if (M & ax[q]) cp_async4(dst + q * NT3 * 4, on[q] ? g.pr[q] + o : g.pr[q], on[q]);
 }
 
 // psi values of one cell (E-psi: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y)
@@ -621,20 +622,21 @@ struct P6 {
     float v[6];
 };
 
-// E-psi values of one cell: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y (LENS_PSI_* 6..11)
-template <typename IX>
+// E-psi values of one cell: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y (LENS_PSI_* 6..11),
+// of the axes in M
+template <unsigned M, typename IX>
 __device__ __forceinline__ void load_epsi(P6 &p, const K3 &g, IX o, unsigned f, bool xe) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) p.v[q] = 0.f;
-    if (f & F_YE) {
+    if ((M & AXY) && (f & F_YE)) {
         p.v[0] = ldg_early(g.pr[LENS_PSI_EX_Y] + o);
         p.v[5] = ldg_early(g.pr[LENS_PSI_EZ_Y] + o);
     }
-    if (f & F_ZE) {
+    if ((M & AXZ) && (f & F_ZE)) {
         p.v[1] = ldg_early(g.pr[LENS_PSI_EX_Z] + o);
         p.v[2] = ldg_early(g.pr[LENS_PSI_EY_Z] + o);
     }
-    if (xe) {
+    if ((M & AXX) && xe) {
         p.v[3] = ldg_early(g.pr[LENS_PSI_EY_X] + o);
         p.v[4] = ldg_early(g.pr[LENS_PSI_EZ_X] + o);
     }
@@ -648,7 +650,7 @@ struct F3 {
 //   e = E(i,j,k); exk, eyk = E(i,j,k+1); exj, ezj = E(i,j+1,k); eyn, ezn = E(i+1,j,k).
 // iok: i < nx-1 (Hy, Hz exist).  ST: CPML tile (psi corrections in the strips).
 // zt / yt: the cell's entries of the z / y profile tables; x: this plane's x values.
-template <bool ST, typename IX>
+template <bool ST, unsigned M, typename IX>
 __device__ __forceinline__ F3 h_new(const K3 &g, F3 h, float ex, float ey, float ez, float exk, float eyk,
                                     float exj, float ezj, float eyn, float ezn, unsigned f, bool iok,
                                     const float *zt, const float *yt, const PX &x, const float *hs, IX o,
@@ -662,24 +664,24 @@ __device__ __forceinline__ F3 h_new(const K3 &g, F3 h, float ex, float ey, float
     if (!ST || (f & F_HX)) {
         float v = h.x + ch * (d1x - d2x);
         if (ST) {
-            if (f & F_ZH) v = v + ch * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[0 * NT3], d1x, g.pw[LENS_PSI_HX_Z], o, wr);
-            if (f & F_YH) v = v + (-ch) * psi_u(yt[0], yt[YN], yt[2 * YN], hs[1 * NT3], d2x, g.pw[LENS_PSI_HX_Y], o, wr);
+            if ((M & AXZ) && (f & F_ZH)) v = v + ch * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[0 * NT3], d1x, g.pw[LENS_PSI_HX_Z], o, wr);
+            if ((M & AXY) && (f & F_YH)) v = v + (-ch) * psi_u(yt[0], yt[YN], yt[2 * YN], hs[1 * NT3], d2x, g.pw[LENS_PSI_HX_Y], o, wr);
         }
         h.x = v;
     }
     if (!ST || (iok && (f & F_HY))) {
         float v = h.y + ch * (d1y - d2y);
         if (ST) {
-            if (xh) v = v + ch * psi_u(x.hb, x.hc, x.hk, hs[2 * NT3], d1y, g.pw[LENS_PSI_HY_X], o, wr);
-            if (f & F_ZH) v = v + (-ch) * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[3 * NT3], d2y, g.pw[LENS_PSI_HY_Z], o, wr);
+            if ((M & AXX) && xh) v = v + ch * psi_u(x.hb, x.hc, x.hk, hs[2 * NT3], d1y, g.pw[LENS_PSI_HY_X], o, wr);
+            if ((M & AXZ) && (f & F_ZH)) v = v + (-ch) * psi_u(zt[0], zt[ZN], zt[2 * ZN], hs[3 * NT3], d2y, g.pw[LENS_PSI_HY_Z], o, wr);
         }
         h.y = v;
     }
     if (!ST || (iok && (f & F_HZ))) {
         float v = h.z + ch * (d1z - d2z);
         if (ST) {
-            if (f & F_YH) v = v + ch * psi_u(yt[0], yt[YN], yt[2 * YN], hs[4 * NT3], d1z, g.pw[LENS_PSI_HZ_Y], o, wr);
-            if (xh) v = v + (-ch) * psi_u(x.hb, x.hc, x.hk, hs[5 * NT3], d2z, g.pw[LENS_PSI_HZ_X], o, wr);
+            if ((M & AXY) && (f & F_YH)) v = v + ch * psi_u(yt[0], yt[YN], yt[2 * YN], hs[4 * NT3], d1z, g.pw[LENS_PSI_HZ_Y], o, wr);
+            if ((M & AXX) && xh) v = v + (-ch) * psi_u(x.hb, x.hc, x.hk, hs[5 * NT3], d2z, g.pw[LENS_PSI_HZ_X], o, wr);
         }
         h.z = v;
     }
@@ -715,7 +717,7 @@ struct PlE {
 // New E of one cell (boundaries3d.py:333-362, fdtd3d_core.py:1116-1127):
 //   D*E, curl of the new H (h = H(i,j,k), hxk/hyk = H(i,j,k-1), hxj/hzj = H(i,j-1,k),
 //   hym/hzm = H(i-1,j,k)), psi in the strips, PEC on the absorbing faces, source.
-template <bool ST, typename IX>
+template <bool ST, unsigned M, typename IX>
 __device__ __forceinline__ F3 e_new(const K3 &g, F3 e, F3 h, float hxk, float hyk, float hxj, float hzj,
                                     float hym, float hzm, const C6 &c, unsigned f, const PlE &pl, int j,
                                     int k, const float *zt, const float *yt, const PX &x, const P6 &ps,
@@ -732,16 +734,16 @@ __device__ __forceinline__ F3 e_new(const K3 &g, F3 e, F3 h, float hxk, float hy
     if (uz) vz = vz + c.cz * (d1z - d2z);
     if (ST) {
         if (ux) {
-            if (f & F_YE) vx = vx + c.cx * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[0], d1x, g.pw[LENS_PSI_EX_Y], o, true);
-            if (f & F_ZE) vx = vx + (-c.cx) * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[1], d2x, g.pw[LENS_PSI_EX_Z], o, true);
+            if ((M & AXY) && (f & F_YE)) vx = vx + c.cx * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[0], d1x, g.pw[LENS_PSI_EX_Y], o, true);
+            if ((M & AXZ) && (f & F_ZE)) vx = vx + (-c.cx) * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[1], d2x, g.pw[LENS_PSI_EX_Z], o, true);
         }
         if (uy) {
-            if (f & F_ZE) vy = vy + c.cy * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[2], d1y, g.pw[LENS_PSI_EY_Z], o, true);
-            if (pl.xe) vy = vy + (-c.cy) * psi_u(x.eb, x.ec, x.ek, ps.v[3], d2y, g.pw[LENS_PSI_EY_X], o, true);
+            if ((M & AXZ) && (f & F_ZE)) vy = vy + c.cy * psi_u(zt[3 * ZN], zt[4 * ZN], zt[5 * ZN], ps.v[2], d1y, g.pw[LENS_PSI_EY_Z], o, true);
+            if ((M & AXX) && pl.xe) vy = vy + (-c.cy) * psi_u(x.eb, x.ec, x.ek, ps.v[3], d2y, g.pw[LENS_PSI_EY_X], o, true);
         }
         if (uz) {
-            if (pl.xe) vz = vz + c.cz * psi_u(x.eb, x.ec, x.ek, ps.v[4], d1z, g.pw[LENS_PSI_EZ_X], o, true);
-            if (f & F_YE) vz = vz + (-c.cz) * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[5], d2z, g.pw[LENS_PSI_EZ_Y], o, true);
+            if ((M & AXX) && pl.xe) vz = vz + c.cz * psi_u(x.eb, x.ec, x.ek, ps.v[4], d1z, g.pw[LENS_PSI_EZ_X], o, true);
+            if ((M & AXY) && (f & F_YE)) vz = vz + (-c.cz) * psi_u(yt[3 * YN], yt[4 * YN], yt[5 * YN], ps.v[5], d2z, g.pw[LENS_PSI_EZ_Y], o, true);
         }
     }
     if (ST) {
@@ -760,8 +762,10 @@ __device__ __forceinline__ F3 e_new(const K3 &g, F3 e, F3 h, float hxk, float hy
     return F3{vx, vy, vz};
 }
 
-// IX: index type of the field volumes (32-bit when nx*ny*pitch < 2^31).
-template <bool ST, typename IX>
+// IX: index type of the field volumes (32-bit when nx*ny*pitch < 2^31).  ST: a
+// tile that touches a CPML strip or a domain face (per-cell flags); M: the axes
+// whose CPML psi the tile carries (a subset of ST tiles' work; 0 for faces only).
+template <bool ST, unsigned M, typename IX>
 __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensStepTable &tab,
                                        const LensEpi3D &ep, int n, int epi, int k0, int j0, int x0,
                                        int x1, unsigned char *smem) {
@@ -782,9 +786,12 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
 
     // ---- producer (lane 0 of the halo warp): E ring and H/coefficient ring.
     // E(p) sits in slot (p-xs) % NSE, HC(p) in slot (p-xs) % NHC; the u-th fill of a
-    // slot completes mbarrier phase u.  Planes (issued] are in flight, (waited] ready.
-    // After a wait gives up nothing new is issued or awaited (the flag reports it)
-    // and the copies in flight are drained (bounded) before the CTA exits.
+    // slot completes mbarrier phase u.  Every thread waits itself for the planes it
+    // reads (E(i+1) and HC(i) at the top of iteration i), so a late copy stalls only
+    // the warps that need it; the CTA barrier of each plane orders the slot reuse.
+    // After a wait gives up a thread awaits nothing more and the producer issues
+    // nothing more (the flag reports it); the producer drains the copies in flight
+    // (bounded) before the CTA exits.
     bool ok = true;
     int ie = xs - 1, we = xs - 1, ih = xs - 1, wh = xs - 1;
     auto issue_e = [&](int p) {
@@ -804,23 +811,15 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         for (int q = 0; q < ncoef; ++q) tma3(dst + (3 + q) * HT * 4, &tm.c[q], k0, j0, p, bar);
         ih = p;
     };
-    auto wait_e = [&](int p) {
-        if (ok) ok = mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1);
-        if (ok) we = p;
-    };
-    auto wait_hc = [&](int p) {
-        if (ok) ok = mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1);
-        if (ok) wh = p;
-    };
     if (prod) {
         for (int q = 0; q < NSE + NHC; ++q) mbar_init(bar0 + 8u * q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         for (int p = xs; p <= min(x1, xs + NSE - 1); ++p) issue_e(p);
         for (int p = xs; p <= min(x1 - 1, xs + NHC - 1); ++p) issue_hc(p);
-        wait_e(xs);
-        if (xs + 1 <= x1) wait_e(xs + 1);
-        wait_hc(xs);
     }
+    // consumer side: slot and phase parity of E(i), E(i+1) and HC(i) (ring counters)
+    int se = 0, sn = 1 % NSE, sh = 0;
+    unsigned pe = 0u, pn = NSE == 1 ? 1u : 0u, ph = 0u;
 
     // ---- per-thread cells.  Owners: rows a = j0+2w, b = a+1 at k = k0+lane.
     // Halo warp: A = (j0-1, k0+lane), B = (j0+lane, k0-1) for lane < TJ.
@@ -852,12 +851,12 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     // profile-table entries of the two cells
     const float *zta = sZT + lane + 1, *ztb = owner ? zta : sZT;
     const float *yta = sYT + (owner ? 2 * w + 1 : 0), *ytb = owner ? yta + 1 : sYT + hl + 1;
-    if (ST) {
+    if (ST && (M & (AXZ | AXY))) {
         const int t = w * TK + lane;
-        if (t < ZN) {
+        if ((M & AXZ) && t < ZN) {
             fill_row(sZT + t, ZN, g.az.h, k0 - 1 + t);
             fill_row(sZT + 3 * ZN + t, ZN, g.az.e, k0 - 1 + t);
-        } else if (t < ZN + YN) {
+        } else if ((M & AXY) && t >= ZN && t < ZN + YN) {
             fill_row(sYT + (t - ZN), YN, g.ay.h, j0 - 1 + (t - ZN));
             fill_row(sYT + 3 * YN + (t - ZN), YN, g.ay.e, j0 - 1 + (t - ZN));
         }
@@ -879,33 +878,30 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     // H-psi of plane p into staging buffer (p - xs) & 1 (cp.async, one plane ahead)
     auto stage_hp = [&](int p) {
         const IX base = (IX)p * S;
-        const bool xh = in_strip(g.ax.h, p);
+        const bool xh = (M & AXX) && in_strip(g.ax.h, p);
         const uint32_t d = hs_s + (((unsigned)(p - xs) & 1u) * HS_STAGE) * 4;
-        stage_hpsi(d, g, base + oa, fa, xh);
-        stage_hpsi(d + 6 * NT3 * 4, g, base + ob, fb, xh);
+        stage_hpsi<M>(d, g, base + oa, fa, xh);
+        stage_hpsi<M>(d + 6 * NT3 * 4, g, base + ob, fb, xh);
         cp_async_commit();
     };
     auto load_ep = [&](int p) {
         const IX base = (IX)p * S;
-        const bool xe = in_strip(g.ax.e, p);
-        if (fa & F_IN) load_epsi(epa, g, base + oa, fa, xe);
-        if (fb & F_IN) load_epsi(epb, g, base + ob, fb, xe);
+        const bool xe = (M & AXX) && in_strip(g.ax.e, p);
+        if (fa & F_IN) load_epsi<M>(epa, g, base + oa, fa, xe);
+        if (fb & F_IN) load_epsi<M>(epb, g, base + ob, fb, xe);
     };
     if (!owner) load_hold(xs);
-    if (ST) stage_hp(xs);
-    if (ST && owner) load_ep(x0);
+    if (ST && M) stage_hp(xs);
+    if (ST && M && owner) load_ep(x0);
 
-    // detector boxes: per-thread float sums over the chunk, added to the FP64 totals at the end
-    float bacc[LENS_MAX_BOX];
-#pragma unroll
-    for (int b = 0; b < LENS_MAX_BOX; ++b) bacc[b] = 0.f;
-    const bool boxes = epi && ep.nbox > 0;
     const float env = tab.env[q0], wt = tab.wt[q0];
 
     // E(i) of the owner cells at (j, k): Ey, Ez carried from the previous plane's "next" reads
     float cya = 0.f, cza = 0.f, cyb = 0.f, czb = 0.f;
     float hyma = 0.f, hzma = 0.f, hymb = 0.f, hzmb = 0.f;  // new H(i-1)
-    __syncthreads();  // E(xs), E(xs+1), HC(xs) visible (waited by the producer)
+    __syncthreads();  // the mbarriers are initialised
+    if (ok) ok = mbar_wait(bar0, 0u);  // E(xs)
+    if (prod && ok) we = xs;
     if (owner) {  // plane xs sits in slot 0
         cya = sE[EF + ea];
         cza = sE[2 * EF + ea];
@@ -916,18 +912,20 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     for (int i = xs; i < x1; ++i) {
         const bool eon = i >= x0;
         const unsigned u = i - xs;
-        const unsigned sc = u % NSE, sn = (u + 1) % NSE;
-        const float *eC = sE + sc * 3 * EF, *eN = sE + sn * 3 * EF;
-        const float *hc = sHC + (u % NHC) * (HC_SLOT / 4);
+        if (ok) ok = mbar_wait(bar0 + 8u * sn, pn);   // E(i+1)
+        if (ok) ok = mbar_wait(barh + 8u * sh, ph);   // HC(i)
+        if (prod && ok) { we = i + 1; wh = i; }
+        const float *eC = sE + se * 3 * EF, *eN = sE + sn * 3 * EF;
+        const float *hc = sHC + sh * (HC_SLOT / 4);
         float *shw = sH + (u & 1) * 3 * SH_N;
         const bool iok = i < nx - 1;
-        const bool xh = ST && in_strip(g.ax.h, i);
-        const PX px = ST ? px_at(g, i) : PX{};
+        const bool xh = ST && (M & AXX) && in_strip(g.ax.h, i);
+        const PX px = (ST && (M & AXX)) ? px_at(g, i) : PX{};
         const IX base = (IX)i * S;
         F3 ha{0.f, 0.f, 0.f}, hb{0.f, 0.f, 0.f};
         float exa = 0.f, exb = 0.f, nya = 0.f, nza = 0.f, nyb = 0.f, nzb = 0.f;
         const float *hs = hs_p + (u & 1u) * HS_STAGE;  // staged H-psi of plane i (own slots)
-        if (ST) cp_async_wait_all();
+        if (ST && M) cp_async_wait_all();
         // ---------------- H(i)
         if (owner) {
             exa = eC[ea];
@@ -942,17 +940,17 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             const F3 h0a{hc[ta], hc[HT + ta], hc[2 * HT + ta]};
             const F3 h0b{hc[ta + TK], hc[HT + ta + TK], hc[2 * HT + ta + TK]};
             const bool wr = eon;
-            ha = h_new<ST, IX>(g, h0a, exa, cya, cza, exa1, eya1, exb, czb, nya, nza, fa, iok, zta, yta, px,
+            ha = h_new<ST, M, IX>(g, h0a, exa, cya, cza, exa1, eya1, exb, czb, nya, nza, fa, iok, zta, yta, px,
                                hs, base + oa, wr, xh);
-            hb = h_new<ST, IX>(g, h0b, exb, cyb, czb, exb1, eyb1, exc, ezc, nyb, nzb, fb, iok, ztb, ytb, px,
+            hb = h_new<ST, M, IX>(g, h0b, exb, cyb, czb, exb1, eyb1, exc, ezc, nyb, nzb, fb, iok, ztb, ytb, px,
                                hs + 6 * NT3, base + ob, wr, xh);
         } else if (eon) {
             // halo cells: A on row 0 of the boxes, B on column 0 (read-only psi)
             const float *c = eC + ea;
-            ha = h_new<ST, IX>(g, hoa, c[0], c[EF], c[2 * EF], c[1], c[EF + 1], c[EK], c[2 * EF + EK],
+            ha = h_new<ST, M, IX>(g, hoa, c[0], c[EF], c[2 * EF], c[1], c[EF + 1], c[EK], c[2 * EF + EK],
                                eN[EF + ea], eN[2 * EF + ea], fa, iok, zta, yta, px, hs, base + oa, false, xh);
             const float *d = eC + eb;
-            hb = h_new<ST, IX>(g, hob, d[0], d[EF], d[2 * EF], d[1], d[EF + 1], d[EK], d[2 * EF + EK],
+            hb = h_new<ST, M, IX>(g, hob, d[0], d[EF], d[2 * EF], d[1], d[EF + 1], d[EK], d[2 * EF + EK],
                                eN[EF + eb], eN[2 * EF + eb], fb, iok, ztb, ytb, px, hs + 6 * NT3, base + ob, false, xh);
         }
         if (owner || eon) {
@@ -966,11 +964,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             }
         }
         if (!owner && i + 1 < x1) load_hold(i + 1);
-        if (ST && i + 1 < x1) stage_hp(i + 1);
-        if (prod) {
-            if (i + 2 <= x1) wait_e(i + 2);
-            if (i + 1 < x1) wait_hc(i + 1);
-        }
+        if (ST && M && i + 1 < x1) stage_hp(i + 1);
         __syncthreads();
         if (prod && ok) {
             if (i + NSE <= x1) issue_e(i + NSE);                        // E(i)'s slot is free
@@ -983,7 +977,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             pl.iok = iok;
             pl.iin = i >= 1 && i <= nx - 2;
             pl.pec_i = (g.pec[0] && i == 0) || (g.pec[1] && i == nx - 1);
-            pl.xe = ST && in_strip(g.ax.e, i);
+            pl.xe = ST && (M & AXX) && in_strip(g.ax.e, i);
             pl.src = g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1);
             pl.sgn = i == g.src.ix ? 1.f : -1.f;
             pl.env = env;
@@ -997,9 +991,9 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             cs += TK;
             const C6 cb{cs[0], cs[HT], cs[2 * HT], lossy ? cs[3 * HT] : 1.f, lossy ? cs[4 * HT] : 1.f,
                         lossy ? cs[5 * HT] : 1.f};
-            const F3 Ea = e_new<ST, IX>(g, F3{exa, cya, cza}, ha, hxka, hyka, hxja, hzja, hyma, hzma, ca, fa,
+            const F3 Ea = e_new<ST, M, IX>(g, F3{exa, cya, cza}, ha, hxka, hyka, hxja, hzja, hyma, hzma, ca, fa,
                                         pl, ja, k, zta, yta, px, epa, base + oa);
-            const F3 Eb = e_new<ST, IX>(g, F3{exb, cyb, czb}, hb, hxkb, hykb, ha.x, ha.z, hymb, hzmb, cb, fb,
+            const F3 Eb = e_new<ST, M, IX>(g, F3{exb, cyb, czb}, hb, hxkb, hykb, ha.x, ha.z, hymb, hzmb, cb, fb,
                                         pl, jb, k, ztb, ytb, px, epb, base + ob);
             if (!ST || (fa & F_IN)) {
                 const IX o = base + oa;
@@ -1011,31 +1005,16 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
                 g.whx[o] = hb.x; g.why[o] = hb.y; g.whz[o] = hb.z;
                 g.wex[o] = Eb.x; g.wey[o] = Eb.y; g.wez[o] = Eb.z;
             }
-            if (boxes) {
-                // detector boxes: Ex^2+Ey^2+Ez^2 (fdtd3d_core.py:477-481; invalid components are zero)
-#pragma unroll
-                for (int b = 0; b < LENS_MAX_BOX; ++b) {
-                    if (b < ep.nbox && i >= ep.box[b][0] && i < box_end(ep.box[b][1], nx)) {
-                        const bool ix = i < box_end(ep.box[b][1], nx - 1);  // Ex is one plane shorter
-                        const unsigned m = F_BOX0 << (3 * b);
-                        bacc[b] += ((ix && (fa & m) ? Ea.x * Ea.x : 0.f) + ((fa & (m << 1)) ? Ea.y * Ea.y : 0.f)) +
-                                   ((fa & (m << 2)) ? Ea.z * Ea.z : 0.f);
-                        bacc[b] += ((ix && (fb & m) ? Eb.x * Eb.x : 0.f) + ((fb & (m << 1)) ? Eb.y * Eb.y : 0.f)) +
-                                   ((fb & (m << 2)) ? Eb.z * Eb.z : 0.f);
-                    }
-                }
-            }
         }
-        if (ST && owner && i + 1 < x1) load_ep(i + 1);
-        // carry
+        if (ST && M && owner && i + 1 < x1) load_ep(i + 1);
+        // carry; advance the ring counters
         cya = nya; cza = nza; cyb = nyb; czb = nzb;
         hyma = ha.y; hzma = ha.z; hymb = hb.y; hzmb = hb.z;
+        se = sn; pe = pn;
+        if (++sn == NSE) { sn = 0; pn ^= 1u; }
+        if (++sh == NHC) { sh = 0; ph ^= 1u; }
     }
-    if (owner && boxes) {
-#pragma unroll
-        for (int b = 0; b < LENS_MAX_BOX; ++b)
-            if (b < ep.nbox) warp_atomic_add(ep.box_acc + b, (double)bacc[b]);
-    }
+    if (!ok && g.flag) atomicExch(g.flag, 1);
     if (prod && !ok) {
         for (int p = we + 1; p <= ie; ++p) mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1);
         for (int p = wh + 1; p <= ih; ++p) mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1);
@@ -1050,10 +1029,28 @@ __global__ void __launch_bounds__(NW3 * 32, 2)
     int tz, ty, c;
     const bool lean = work_tile(wk, blockIdx.x, tz, ty, c);
     extern __shared__ __align__(128) unsigned char smem[];
-    if (!lean)
-        tile3d<true, IX>(tm, g, tab, ep, n, epi, tz * TK, ty * TJ, wk.x[c], wk.x[c + 1], smem);
-    else
-        tile3d<false, IX>(tm, g, tab, ep, n, epi, tz * TK, ty * TJ, wk.x[c], wk.x[c + 1], smem);
+    const int k0 = tz * TK, j0 = ty * TJ, x0 = wk.x[c], x1 = wk.x[c + 1];
+    if (lean) {
+        tile3d<false, 0u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem);
+        return;
+    }
+    if (sizeof(IX) > 4) {  // very large grids: one generic CPML pass
+        tile3d<true, AXALL, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem);
+        return;
+    }
+    const unsigned m = ((tz < wk.plo[0] || tz >= wk.phi[0]) ? AXZ : 0u) |
+                       ((ty < wk.plo[1] || ty >= wk.phi[1]) ? AXY : 0u) |
+                       ((c < wk.plo[2] || c >= wk.phi[2]) ? AXX : 0u);
+    switch (m) {  // tile pass specialised on the CPML axes it carries
+        case 0u: tile3d<true, 0u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 1u: tile3d<true, 1u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 2u: tile3d<true, 2u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 3u: tile3d<true, 3u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 4u: tile3d<true, 4u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 5u: tile3d<true, 5u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        case 6u: tile3d<true, 6u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+        default: tile3d<true, 7u, IX>(tm, g, tab, ep, n, epi, k0, j0, x0, x1, smem); break;
+    }
 }
 
 // Window epilogue after a fused step (DFT / convergence windows): volume DFTs,
@@ -1097,6 +1094,47 @@ __global__ void __launch_bounds__(NT) win3d(const K3 g, const LensStepTable tab,
             hzm = g.hz[o - S];
         }
         epi_cell(g, tab, ep, n, i, j, k, true, Hv{ex, ey, ez}, hym, hzm, h, false, false);
+    }
+}
+
+// ============================================================ detector boxes
+// Detector box sums of the new E after a fused step (fdtd3d_core.py:477-481):
+// sum over the box of Ex^2 + Ey^2 + Ez^2, each component over its own slice
+// (box_end), squares in float32 summed in FP64.  Box b, BOXX planes per thread;
+// one FP64 atomic per CTA.
+constexpr int BOXX = 8;
+
+__global__ void __launch_bounds__(NT) box3d(const K3 g, const LensEpi3D ep, int b) {
+    const int *bx = ep.box[b];
+    const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
+    const int k = bx[4] + blockIdx.x * BK + threadIdx.x, j = bx[2] + blockIdx.y * BJ + threadIdx.y;
+    const int i0 = bx[0] + blockIdx.z * BOXX, i1 = min(i0 + BOXX, box_end(bx[1], nx));
+    double v = 0.0;
+    if (j >= 0 && j < ny && k >= 0 && k < nz) {
+        for (int i = max(i0, 0); i < i1; ++i) {
+            const size_t o = ((size_t)i * ny + j) * P + k;
+            if (i < nx - 1 && in_box(bx, 0, i, j, k, nx, ny, nz)) {
+                const float e = g.ex[o];
+                v += (double)(e * e);
+            }
+            if (j < ny - 1 && in_box(bx, 1, i, j, k, nx, ny, nz)) {
+                const float e = g.ey[o];
+                v += (double)(e * e);
+            }
+            if (k < nz - 1 && in_box(bx, 2, i, j, k, nx, ny, nz)) {
+                const float e = g.ez[o];
+                v += (double)(e * e);
+            }
+        }
+    }
+    __shared__ double red[NT / 32];
+    v = warp_sum(v);
+    if (threadIdx.x == 0) red[threadIdx.y] = v;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        v = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0 && v != 0.0) atomicAdd(ep.box_acc + b, v);
     }
 }
 
@@ -1338,6 +1376,20 @@ Work make_work(const LensGrid3D *g, int slots) {
                j0 + TJ - 1 > g->ny - 2;
     }, y0, y1);
     lean_range(nc, [&](int c) { return cstrip[c] != 0 || wk.x[c] < 1 || wk.x[c + 1] > g->nx - 1; }, c0, c1);
+    // tiles / chunks without psi of an axis (a contiguous run, else none: every
+    // tile then carries that axis, which is always correct)
+    lean_range(ntz, [&](int t) {
+        const int k0 = t * TK;
+        return meets(k0 - 1, k0 + TK - 1, g->az.h) || meets(k0, k0 + TK - 1, g->az.e);
+    }, wk.plo[0], wk.phi[0]);
+    lean_range(nty, [&](int t) {
+        const int j0 = t * TJ;
+        return meets(j0 - 1, j0 + TJ - 1, g->ay.h) || meets(j0, j0 + TJ - 1, g->ay.e);
+    }, wk.plo[1], wk.phi[1]);
+    lean_range(nc, [&](int c) {
+        const int a = wk.x[c], b = wk.x[c + 1];
+        return meets(a > 0 ? a - 1 : 0, b - 1, g->ax.h) || meets(a, b - 1, g->ax.e);
+    }, wk.plo[2], wk.phi[2]);
     if (z1 == z0 || y1 == y0 || c1 == c0) z0 = z1 = y0 = y1 = c0 = c1 = 0;
     wk.ntz = ntz; wk.nty = nty; wk.nc = nc;
     wk.lo[0] = z0; wk.hi[0] = z1;
@@ -1384,8 +1436,8 @@ bool encode(CUtensorMap *m, const float *base, const LensGrid3D *g, int bk, int 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// A drive acts after the E update, where the detector boxes are summed, so a
-// driven step takes no boxes.
+// The two-pass path sums the detector boxes inside its E pass, before a drive
+// could act, so a driven step takes no boxes.
 bool drive3d_ok(const LensDrive3D *d, const LensStepTable *t, const LensGrid3D *g, const LensEpi3D *ep) {
     if (!d) return true;
     if (ep && ep->nbox > 0) return false;
@@ -1464,6 +1516,14 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
         else
             yee3d<size_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
         if (dr) drive3d<<<grd_d, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, *dr, n);
+        for (int b = 0; b < e.nbox; ++b) {  // detector boxes of the new E
+            const int *bx = e.box[b];
+            const int zl = box_end(bx[5], g->nz) - bx[4], yl = box_end(bx[3], g->ny) - bx[2],
+                      xl = box_end(bx[1], g->nx) - bx[0];
+            if (zl > 0 && yl > 0 && xl > 0)
+                box3d<<<dim3((zl + BK - 1) / BK, (yl + BJ - 1) / BJ, (xl + BOXX - 1) / BOXX), blk, 0, s>>>(
+                    view(g, 1 - rb, 1 - rb), e, b);
+        }
         if (ea && ((n >= e.dft_n0 && n < e.dft_n1) || (e.conv_prev && n >= e.prev_n0 && n < e.prev_n1)))
             win3d<<<grd_w, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, e, n);
         g->cur = 1 - rb;

@@ -9,7 +9,8 @@ fdtd3d_core.py:1405-1450).  This loop takes a stream of timed requests and:
     a large job is not starved by a run of small ones);
   * keeps every admitted solve resident (fields, CPML psi, coefficients, DFT
     sums stay on the device until the result is read);
-  * advances all resident solves concurrently: the 2D requests of one time step
+  * advances all resident solves concurrently (CUDA stream priorities put the
+    short 2D work ahead of 3D jobs and those ahead of stitch jobs): the 2D requests of one time step
     and wavelength share ONE batched launch per half step (lens_batch2d_step
     over every tile of every member; a request joins the running batch at the
     next quantum boundary with its own step origin, n_start) and each 3D or
@@ -99,7 +100,7 @@ class _Batch2D:
         self.group = None
         self.n = 0                   # batch step counter
         self.table = None
-        self.stream = torch.cuda.Stream(device=server.dev)
+        self.stream = torch.cuda.Stream(device=server.dev, priority=server.prio['2d'])
         self.event = None
 
     def busy(self):
@@ -170,7 +171,7 @@ class _Job:
 
     def __init__(self, server, req, geo_future):
         self.srv, self.req, self.geo = server, req, geo_future
-        self.stream = torch.cuda.Stream(device=server.dev)
+        self.stream = torch.cuda.Stream(device=server.dev, priority=server.prio[req.kind])
         self.event = None
         self.solve = None
 
@@ -250,6 +251,11 @@ class Server:
         self.storage_code, self.dtype = B.DTYPES[storage]
         self.by = by
         self.pool = cf.ThreadPoolExecutor(max_workers=host_threads)
+        # shortest work first on the device: the 2D batch's stream has the highest
+        # priority, 3D jobs the middle one, stitch jobs the lowest
+        a, b = torch.cuda.Stream.priority_range()
+        hi, lo = min(a, b), max(a, b)                    # a lower value runs first
+        self.prio = {'2d': hi, '3d': (hi + lo) // 2, 'stitch': lo}
         self.used = 0
         self.t0 = 0.0
         self.launched = 0

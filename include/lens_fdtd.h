@@ -40,6 +40,7 @@ extern "C" {
 #define LENS_ERR_CUDA (-2)
 #define LENS_ERR_SIZE (-3)
 
+#define LENS_MAX_CTYPE 4
 #define LENS_MAX_BOX 4
 #define LENS_MAX_PLANE 4
 
@@ -221,6 +222,18 @@ typedef struct {
     int src_comp;                /* 0 Ex, 1 Ey, 2 Ez                           */
     int *flag;                   /* optional device int, set nonzero when a
                                     pipeline wait gave up (results invalid)    */
+    /* Optional column form of the six coefficient volumes (NULL ctype: the
+       fused step reads every coefficient from the volumes).  A layered slab
+       repeats a few coefficient columns (over y) at almost every (x, z): the
+       fused step then reads those from ctab and the volumes only where
+       ctype == 255.  Values are the volumes' own, bit for bit.              */
+    const unsigned char *ctype;  /* (nx, pitch): column type 0..ntype-1 of the
+                                    cells (i, *, k), or 255 (read the volumes) */
+    const float *ctab;           /* (ntype, 6, ny): ce_x, ce_y, ce_z, D_x, D_y,
+                                    D_z down each column type                  */
+    const unsigned char *cexpl;  /* (nx, pitch/32): nonzero where the 32-column
+                                    group of plane i holds a type-255 column   */
+    int ntype;                   /* 1..4 (LENS_MAX_CTYPE)                      */
 } LensGrid3D;
 
 typedef struct {

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, '_lib', 'liblens_fdtd.so')
 
 MAX_BOX = 4
+MAX_CTYPE = 4
 MAX_PLANE = 4
 
 
@@ -71,7 +72,8 @@ class Grid3D(ctypes.Structure):
                 ('ce_x', c_void_p), ('ce_y', c_void_p), ('ce_z', c_void_p),
                 ('da_x', c_void_p), ('da_y', c_void_p), ('da_z', c_void_p),
                 ('ch', c_float), ('ax', Axis), ('ay', Axis), ('az', Axis),
-                ('pec', c_int * 6), ('src', Source), ('src_comp', c_int), ('flag', c_void_p)]
+                ('pec', c_int * 6), ('src', Source), ('src_comp', c_int), ('flag', c_void_p),
+                ('ctype', c_void_p), ('ctab', c_void_p), ('cexpl', c_void_p), ('ntype', c_int)]
 
 
 class Epi3D(ctypes.Structure):

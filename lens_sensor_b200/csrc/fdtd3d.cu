@@ -44,6 +44,9 @@ struct K3 {
     LensSource src;
     int src_comp;
     int *flag;
+    const unsigned char *ctype, *cexpl;  // coefficient column form (LensGrid3D)
+    const float *ctab;
+    int ntype;
 };
 
 struct Hv {
@@ -404,7 +407,8 @@ constexpr int NT3 = NW3 * 32;                // threads of a CTA
 constexpr int OFF_HS = OFF_PT + (((6 * (TK + 1 + TJ + 1)) * 4 + 127) / 128) * 128;
 constexpr int HS_STAGE = 12 * NT3;           // H-psi of a thread's two cells, 6 components each
 constexpr int OFF_BAR = OFF_HS + 2 * HS_STAGE * 4;
-constexpr int SMEM3 = OFF_BAR + (NSE + NHC) * 8;
+constexpr int OFF_CT = OFF_BAR + (NSE + NHC) * 8;  // coefficient column types: the tile's rows
+constexpr int SMEM3 = OFF_CT + LENS_MAX_CTYPE * 6 * TJ * 4;
 static_assert(OFF_HC % 128 == 0 && HC_SLOT % 128 == 0 && (HT * 4) % 128 == 0, "TMA alignment");
 static_assert(OFF_SH % 128 == 0 && OFF_BAR % 8 == 0, "alignment");
 
@@ -592,6 +596,12 @@ __device__ __forceinline__ unsigned cell_flags(const K3 &g, const LensEpi3D &ep,
 __device__ __forceinline__ float ldg_early(const float *p) {
     float v;
     asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ unsigned ldg_u8_early(const unsigned char *p) {
+    unsigned v;
+    asm volatile("ld.global.nc.u8 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
 
@@ -802,13 +812,16 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         for (int q = 0; q < 3; ++q) tma3(sbase + (s * 3 + q) * E_SLOT, &tm.e[q], k0 - 4, j0 - 1, p, bar);
         ie = p;
     };
+    // the coefficient boxes of plane p only where its 32-column group holds a
+    // column without a type (the others come from the type table in shared memory)
     auto issue_hc = [&](int p) {
         const int s = (p - xs) % NHC;
         const uint32_t bar = barh + 8u * s, dst = sbase + OFF_HC + s * HC_SLOT;
-        mbar_expect(bar, (3 + ncoef) * HT * 4);
+        const int nc = (!g.ctype || g.cexpl[(size_t)p * (P / TK) + k0 / TK]) ? ncoef : 0;
+        mbar_expect(bar, (3 + nc) * HT * 4);
 #pragma unroll
         for (int q = 0; q < 3; ++q) tma3(dst + q * HT * 4, &tm.h[q], k0, j0, p, bar);
-        for (int q = 0; q < ncoef; ++q) tma3(dst + (3 + q) * HT * 4, &tm.c[q], k0, j0, p, bar);
+        for (int q = 0; q < nc; ++q) tma3(dst + (3 + q) * HT * 4, &tm.c[q], k0, j0, p, bar);
         ih = p;
     };
     if (prod) {
@@ -893,6 +906,16 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     if (!owner) load_hold(xs);
     if (ST && M) stage_hp(xs);
     if (ST && M && owner) load_ep(x0);
+    // coefficient column types: the tile's rows of the type table into shared
+    // memory; each owner lane's column type one plane ahead
+    float *sCT = reinterpret_cast<float *>(smem + OFF_CT);
+    const bool ccol = g.ctype != nullptr;
+    if (ccol)
+        for (int t = tid; t < g.ntype * 6 * TJ; t += NT3) {
+            const int r = t % TJ, q = t / TJ;
+            sCT[t] = j0 + r < ny ? __ldg(g.ctab + (size_t)q * ny + j0 + r) : 0.f;
+        }
+    unsigned tcn = (owner && ccol) ? ldg_u8_early(g.ctype + (IX)xs * P + k) : 255u;
 
     const float env = tab.env[q0], wt = tab.wt[q0];
 
@@ -912,6 +935,8 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     for (int i = xs; i < x1; ++i) {
         const bool eon = i >= x0;
         const unsigned u = i - xs;
+        const unsigned tc = tcn;  // column type of (i, k)
+        if (owner && ccol && i + 1 < x1) tcn = ldg_u8_early(g.ctype + (IX)(i + 1) * P + k);
         if (ok) ok = mbar_wait(bar0 + 8u * sn, pn);   // E(i+1)
         if (ok) ok = mbar_wait(barh + 8u * sh, ph);   // HC(i)
         if (prod && ok) { we = i + 1; wh = i; }
@@ -985,12 +1010,15 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             const float hxja = shw[sa - SHK], hzja = shw[2 * SH_N + sa - SHK];
             const float hxka = shw[sa - 1], hyka = shw[SH_N + sa - 1];
             const float hxkb = shw[sb - 1], hykb = shw[SH_N + sb - 1];
-            const float *cs = hc + 3 * HT + ta;
-            const C6 ca{cs[0], cs[HT], cs[2 * HT], lossy ? cs[3 * HT] : 1.f, lossy ? cs[4 * HT] : 1.f,
-                        lossy ? cs[5 * HT] : 1.f};
-            cs += TK;
-            const C6 cb{cs[0], cs[HT], cs[2 * HT], lossy ? cs[3 * HT] : 1.f, lossy ? cs[4 * HT] : 1.f,
-                        lossy ? cs[5 * HT] : 1.f};
+            // coefficients: the staged boxes (a column without a type) or the type table
+            const bool tb = tc != 255u;
+            const float *cs = tb ? sCT + tc * (6 * TJ) + 2 * w : hc + 3 * HT + ta;
+            const int st = tb ? TJ : HT, nb = tb ? 1 : TK;  // coefficient stride, row b offset
+            const C6 ca{cs[0], cs[st], cs[2 * st], lossy ? cs[3 * st] : 1.f, lossy ? cs[4 * st] : 1.f,
+                        lossy ? cs[5 * st] : 1.f};
+            cs += nb;
+            const C6 cb{cs[0], cs[st], cs[2 * st], lossy ? cs[3 * st] : 1.f, lossy ? cs[4 * st] : 1.f,
+                        lossy ? cs[5 * st] : 1.f};
             const F3 Ea = e_new<ST, M, IX>(g, F3{exa, cya, cza}, ha, hxka, hyka, hxja, hzja, hyma, hzma, ca, fa,
                                         pl, ja, k, zta, yta, px, epa, base + oa);
             const F3 Eb = e_new<ST, M, IX>(g, F3{exb, cyb, czb}, hb, hxkb, hykb, ha.x, ha.z, hymb, hzmb, cb, fb,
@@ -1254,6 +1282,7 @@ bool grid3d_ok(const LensGrid3D *g) {
     const bool d0 = !g->da_x, d1 = !g->da_y, d2 = !g->da_z;
     if (d0 != d1 || d1 != d2) return false;
     if (!ax_ok(g->ax, g->nx) || !ax_ok(g->ay, g->ny) || !ax_ok(g->az, g->nz)) return false;
+    if (g->ctype && (!g->ctab || !g->cexpl || g->ntype < 1 || g->ntype > LENS_MAX_CTYPE)) return false;
     if (g->src.ix >= 0) {
         if (!g->src.amp || !g->src.ph1 || !g->src.ph2 || g->src.ix + 1 >= g->nx) return false;
         if (g->src_comp < 0 || g->src_comp > 2 || g->src.pitch_k < g->src.nk) return false;
@@ -1298,6 +1327,7 @@ K3 view(const LensGrid3D *g, int rb, int wb) {
     k.ch = g->ch; k.ax = g->ax; k.ay = g->ay; k.az = g->az;
     for (int q = 0; q < 6; ++q) k.pec[q] = g->pec[q];
     k.src = g->src; k.src_comp = g->src_comp; k.flag = g->flag;
+    k.ctype = g->ctype; k.cexpl = g->cexpl; k.ctab = g->ctab; k.ntype = g->ntype;
     return k;
 }
 

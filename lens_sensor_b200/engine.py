@@ -247,6 +247,54 @@ class Epi2D:
 
 
 # ============================================================================ 3D
+MAX_CTYPE = 4
+
+
+def coef_columns(vols, nx, ny, nz, min_count=64):
+    """Column form of the coefficient volumes (LensGrid3D.ctype/ctab/cexpl).
+
+    vols: the padded (nx, ny, pitch) float32 device volumes ce_x, ce_y, ce_z
+    (+ D_x, D_y, D_z).  The (i, k) columns over y are grouped by an exact
+    fingerprint of their bit patterns; the up to 4 most frequent groups (each
+    of at least min_count columns) whose members equal their representative bit
+    for bit become column types.  Returns (ctype uint8 (nx, pitch), ctab
+    float32 (ntype, 6, ny), cexpl uint8 (nx, pitch/32), ntype), or None when no
+    group qualifies."""
+    dev = vols[0].device
+    P = vols[0].shape[2]
+    g = torch.Generator(device='cpu').manual_seed(12345)
+    w = (torch.randint(1, 2 ** 62, (len(vols), ny), generator=g, dtype=torch.int64) | 1).to(dev)
+    h = torch.zeros((nx, P), dtype=torch.int64, device=dev)
+    for a, wa in zip(vols, w):   # sum of bit patterns times odd weights (mod 2^64)
+        h += (a.view(torch.int32).to(torch.int64) * wa[None, :, None]).sum(dim=1)
+    hv = h[:, :nz].reshape(-1)
+    uniq, inv, cnt = torch.unique(hv, return_inverse=True, return_counts=True)
+    order = torch.argsort(cnt, descending=True)[:MAX_CTYPE].tolist()
+    ctype = torch.full((nx, P), 255, dtype=torch.uint8, device=dev)
+    ctab = torch.zeros((MAX_CTYPE, 6, ny), dtype=torch.float32, device=dev)
+    nt = 0
+    for u in order:
+        if int(cnt[u]) < min_count:
+            break
+        pos = torch.nonzero(inv == u).squeeze(1)
+        ii, kk = pos // nz, pos % nz
+        ok = torch.ones(pos.numel(), dtype=torch.bool, device=dev)
+        i0, k0 = int(ii[0]), int(kk[0])
+        for c, a in enumerate(vols):
+            rep = a[i0, :, k0].view(torch.int32)
+            ok &= (a[ii, :, kk].view(torch.int32) == rep[None, :]).all(dim=1)
+            ctab[nt, c] = a[i0, :, k0]
+        if not bool(ok.any()):
+            continue
+        ctype[ii[ok], kk[ok]] = nt
+        nt += 1
+    if nt == 0:
+        return None
+    ctype[:, nz:] = 0                      # padding columns are never read
+    cexpl = (ctype == 255).view(nx, P // 32, 32).any(dim=2).to(torch.uint8).contiguous()
+    return ctype.contiguous(), ctab[:nt].contiguous(), cexpl, nt
+
+
 def plane_flux(pairs, n):
     """sum over pairs of sign * Re(sum aE conj(aH)) / 2, times (2/n)^2 (flux.py:45-57)."""
     tot = 0.0
@@ -313,6 +361,11 @@ class Grid3D:
         g.src = s
         g.src_comp = self.src_comp
         g.flag = self.flag.data_ptr()
+        # the fused step reads repeated coefficient columns from a small table
+        self.cols = coef_columns(self.ce + (self.da or []), nx, ny, nz) if fused else None
+        if self.cols is not None:
+            ct, tab, ex, nt = self.cols
+            g.ctype, g.ctab, g.cexpl, g.ntype = ct.data_ptr(), tab.data_ptr(), ex.data_ptr(), nt
         self.s = g
 
     def __getattr__(self, name):

@@ -52,7 +52,9 @@ struct St<__nv_bfloat16> {
 // A block covers a tile of 32 columns (lanes, contiguous y) x blockDim.y * RB
 // rows of one instance; each thread updates RB consecutive rows of its column,
 // issuing all of their loads before the arithmetic (the rows share the
-// x-neighbour loads).  owner[b] is the instance of block b and blk[q] its first
+// x-neighbour loads).  The H and E passes are held to 64 registers (4 blocks of
+// 256 threads per SM): these passes wait on memory, and the extra resident
+// warps hide more of that latency than the registers would save.  owner[b] is the instance of block b and blk[q] its first
 // block; the descriptor fields are read through the read-only cache (every
 // thread of the block reads the same words).
 constexpr int RB = 4;
@@ -119,7 +121,7 @@ __device__ __forceinline__ float psi_step(const LensProfile &pf, int m, float *q
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
+__global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
     const Tile tl = tile_of(inst, blk, owner);
     const V g{tl.g};
     const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(256) b2d_h(const LensInst2D *inst, const int *
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     b2d_e(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
     const Tile tl = tile_of(inst, blk, owner);
     const V g{tl.g};

@@ -19,6 +19,7 @@
 //    per step (72 B per cell update for the lossy case, 60 lossless).
 //  * h3d + e3d (in place, no buffer 1): two streaming passes.
 #include <cuda.h>
+#include <algorithm>
 
 #include <cmath>
 
@@ -1128,33 +1129,39 @@ __global__ void __launch_bounds__(NT) win3d(const K3 g, const LensStepTable tab,
 // ============================================================ detector boxes
 // Detector box sums of the new E after a fused step (fdtd3d_core.py:477-481):
 // sum over the box of Ex^2 + Ey^2 + Ez^2, each component over its own slice
-// (box_end), squares in float32 summed in FP64.  Box b, BOXX planes per thread;
-// one FP64 atomic per CTA.
-constexpr int BOXX = 8;
+// (box_end), squares in float32 summed in FP64.  One launch for every box:
+// blockIdx.z runs over the boxes' planes in groups of BOXX (xb[b] is the first
+// group of box b); all loads of a thread are issued before its sums; one FP64
+// atomic per CTA.
+constexpr int BOXX = 2;
 
-__global__ void __launch_bounds__(NT) box3d(const K3 g, const LensEpi3D ep, int b) {
+struct BoxGrid {
+    int xb[LENS_MAX_BOX + 1];
+};
+
+__global__ void __launch_bounds__(NT) box3d(const K3 g, const LensEpi3D ep, const BoxGrid bg) {
+    int b = 0;
+    while (b + 1 < ep.nbox && (int)blockIdx.z >= bg.xb[b + 1]) ++b;
     const int *bx = ep.box[b];
     const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
     const int k = bx[4] + blockIdx.x * BK + threadIdx.x, j = bx[2] + blockIdx.y * BJ + threadIdx.y;
-    const int i0 = bx[0] + blockIdx.z * BOXX, i1 = min(i0 + BOXX, box_end(bx[1], nx));
-    double v = 0.0;
-    if (j >= 0 && j < ny && k >= 0 && k < nz) {
-        for (int i = max(i0, 0); i < i1; ++i) {
-            const size_t o = ((size_t)i * ny + j) * P + k;
-            if (i < nx - 1 && in_box(bx, 0, i, j, k, nx, ny, nz)) {
-                const float e = g.ex[o];
-                v += (double)(e * e);
-            }
-            if (j < ny - 1 && in_box(bx, 1, i, j, k, nx, ny, nz)) {
-                const float e = g.ey[o];
-                v += (double)(e * e);
-            }
-            if (k < nz - 1 && in_box(bx, 2, i, j, k, nx, ny, nz)) {
-                const float e = g.ez[o];
-                v += (double)(e * e);
-            }
-        }
+    const int i0 = bx[0] + ((int)blockIdx.z - bg.xb[b]) * BOXX, i1 = min(i0 + BOXX, box_end(bx[1], nx));
+    const bool col = j >= 0 && j < ny && k >= 0 && k < nz && k < box_end(bx[5], nz) && j < box_end(bx[3], ny);
+    float e[BOXX][3];
+#pragma unroll
+    for (int q = 0; q < BOXX; ++q) {
+        const int i = i0 + q;
+        const size_t o = ((size_t)i * ny + j) * P + k;
+        const bool pl = col && i >= 0 && i < i1;
+        e[q][0] = (pl && i < nx - 1 && in_box(bx, 0, i, j, k, nx, ny, nz)) ? g.ex[o] : 0.f;
+        e[q][1] = (pl && j < ny - 1 && in_box(bx, 1, i, j, k, nx, ny, nz)) ? g.ey[o] : 0.f;
+        e[q][2] = (pl && k < nz - 1 && in_box(bx, 2, i, j, k, nx, ny, nz)) ? g.ez[o] : 0.f;
     }
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < BOXX; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v += (double)(e[q][c] * e[q][c]);
     __shared__ double red[NT / 32];
     v = warp_sum(v);
     if (threadIdx.x == 0) red[threadIdx.y] = v;
@@ -1536,6 +1543,21 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
         return LENS_ERR_CUDA;
     const Work wk = make_work(g, 2 * nsm);
     const int nblk = wk.ntz * wk.nty * wk.nc;
+    // box-sum grid: the largest y-z extent of the boxes, their plane groups stacked in z
+    BoxGrid bgr{};
+    int bgx = 0, bgy = 0, bgz = 0;
+    for (int b = 0; b < e.nbox; ++b) {
+        const int *bx = e.box[b];
+        const int zl = box_end(bx[5], g->nz) - bx[4], yl = box_end(bx[3], g->ny) - bx[2],
+                  xl = box_end(bx[1], g->nx) - bx[0];
+        bgr.xb[b] = bgz;
+        if (zl > 0 && yl > 0 && xl > 0) {
+            bgx = std::max(bgx, (zl + BK - 1) / BK);
+            bgy = std::max(bgy, (yl + BJ - 1) / BJ);
+            bgz += (xl + BOXX - 1) / BOXX;
+        }
+    }
+    bgr.xb[e.nbox] = bgz;
     const dim3 grd_w(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx);
     for (int n = n0; n < n0 + nsteps; ++n) {
         const int rb = g->cur;
@@ -1546,14 +1568,8 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
         else
             yee3d<size_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
         if (dr) drive3d<<<grd_d, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, *dr, n);
-        for (int b = 0; b < e.nbox; ++b) {  // detector boxes of the new E
-            const int *bx = e.box[b];
-            const int zl = box_end(bx[5], g->nz) - bx[4], yl = box_end(bx[3], g->ny) - bx[2],
-                      xl = box_end(bx[1], g->nx) - bx[0];
-            if (zl > 0 && yl > 0 && xl > 0)
-                box3d<<<dim3((zl + BK - 1) / BK, (yl + BJ - 1) / BJ, (xl + BOXX - 1) / BOXX), blk, 0, s>>>(
-                    view(g, 1 - rb, 1 - rb), e, b);
-        }
+        if (e.nbox > 0 && bgz > 0)  // detector boxes of the new E, every box in one launch
+            box3d<<<dim3(bgx, bgy, bgz), blk, 0, s>>>(view(g, 1 - rb, 1 - rb), e, bgr);
         if (ea && ((n >= e.dft_n0 && n < e.dft_n1) || (e.conv_prev && n >= e.prev_n0 && n < e.prev_n1)))
             win3d<<<grd_w, blk, 0, s>>>(view(g, 1 - rb, 1 - rb), *tab, e, n);
         g->cur = 1 - rb;

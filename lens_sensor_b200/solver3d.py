@@ -108,12 +108,12 @@ class Solve3D:
 
     def _launches(self, n0, n1, fused):
         """Kernel launches of steps [n0, n1): fused, one step kernel and one box-sum
-        kernel per detector box, plus the window epilogue on DFT / convergence-window
-        steps; two passes otherwise."""
+        kernel (every detector box), plus the window epilogue on DFT /
+        convergence-window steps; two passes otherwise."""
         if not fused:
             return 2 * (n1 - n0)
         w0, w1 = self.prev[0], self.dft[1]
-        return (n1 - n0) * (1 + len(self.boxes)) + max(0, min(n1, w1) - max(n0, w0))
+        return (n1 - n0) * (1 + (1 if self.boxes else 0)) + max(0, min(n1, w1) - max(n0, w0))
 
     # ---------------------------------------------------------------- results
     def phasor(self, comp=None):

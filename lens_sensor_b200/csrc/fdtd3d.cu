@@ -1087,42 +1087,52 @@ __global__ void __launch_bounds__(NW3 * 32, 2)
 // step wrote).  A separate streaming pass keeps the step kernel's registers for
 // its pipeline: it reads E once (12 B per cell) and updates the complex
 // accumulators (16 B per component and cell) on window steps only.
+constexpr int WK = 4;  // window epilogue: cells per thread along z
+
 __global__ void __launch_bounds__(NT) win3d(const K3 g, const LensStepTable tab, const LensEpi3D ep, int n) {
-    const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y, i = blockIdx.z;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    if (k >= nz || j >= ny) return;  // no warp-collective operations below
-    const size_t S = (size_t)ny * g.P, o = i * S + (size_t)j * g.P + k;
-    const bool vx = i < nx - 1, vy = j < ny - 1, vz = k < nz - 1;
+    const int k0 = (blockIdx.x * BK + threadIdx.x) * WK, j = blockIdx.y * BJ + threadIdx.y, i = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, P = g.P;
+    if (k0 >= P || j >= ny) return;  // no warp-collective operations below
+    const size_t S = (size_t)ny * P, o = i * S + (size_t)j * P + k0;
     const bool win = n >= ep.dft_n0 && n < ep.dft_n1;
     const int q = n - tab.t0;
     const float pr = tab.pe[2 * q], pim = tab.pe[2 * q + 1];
-    const float ex = vx ? g.ex[o] : 0.f, ey = vy ? g.ey[o] : 0.f, ez = vz ? g.ez[o] : 0.f;
+    // E of WK cells; the step leaves zero wherever a component does not exist
+    // (its last plane / row / column, the z padding), so those sums stay zero
+    const float4 E[3] = {*reinterpret_cast<const float4 *>(g.ex + o), *reinterpret_cast<const float4 *>(g.ey + o),
+                         *reinterpret_cast<const float4 *>(g.ez + o)};
     if (win) {
-        const float v[3] = {ex, ey, ez};
-        const bool ok[3] = {vx, vy, vz};
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            if (ep.dft[c] && ok[c]) {
-                float2 *a = reinterpret_cast<float2 *>(ep.dft[c]) + o;
-                float2 s = *a;
-                s.x += v[c] * pr;
-                s.y += v[c] * pim;
-                *a = s;
-            }
+            if (!ep.dft[c]) continue;
+            float4 *a = reinterpret_cast<float4 *>(ep.dft[c] + 2 * o);
+            float4 s0 = a[0], s1 = a[1];
+            s0.x += E[c].x * pr; s0.y += E[c].x * pim; s0.z += E[c].y * pr; s0.w += E[c].y * pim;
+            s1.x += E[c].z * pr; s1.y += E[c].z * pim; s1.z += E[c].w * pr; s1.w += E[c].w * pim;
+            a[0] = s0;
+            a[1] = s1;
         }
     }
     const bool conv = (win && ep.conv_last) || (ep.conv_prev && n >= ep.prev_n0 && n < ep.prev_n1);
     bool fl = false;
     for (int p = 0; p < ep.nplane; ++p) fl |= (i == ep.plane[p]);
-    if ((conv && k == ep.conv_k) || (win && fl)) {
+    const bool cz = conv && ep.conv_k >= k0 && ep.conv_k < k0 + WK;
+    if (!cz && !(win && fl)) return;
+    const float ev[3][WK] = {{E[0].x, E[0].y, E[0].z, E[0].w}, {E[1].x, E[1].y, E[1].z, E[1].w},
+                             {E[2].x, E[2].y, E[2].z, E[2].w}};
+#pragma unroll
+    for (int m = 0; m < WK; ++m) {
+        const int k = k0 + m;
+        if (k >= nz || !((cz && k == ep.conv_k) || (win && fl))) continue;
+        const size_t om = o + m;
         Hv h{0.f, 0.f, 0.f};
         float hym = 0.f, hzm = 0.f;
         if (fl) {
-            h = Hv{g.hx[o], g.hy[o], g.hz[o]};
-            hym = g.hy[o - S];
-            hzm = g.hz[o - S];
+            h = Hv{g.hx[om], g.hy[om], g.hz[om]};
+            hym = g.hy[om - S];
+            hzm = g.hz[om - S];
         }
-        epi_cell(g, tab, ep, n, i, j, k, true, Hv{ex, ey, ez}, hym, hzm, h, false, false);
+        epi_cell(g, tab, ep, n, i, j, k, true, Hv{ev[0][m], ev[1][m], ev[2][m]}, hym, hzm, h, false, false);
     }
 }
 
@@ -1508,7 +1518,8 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
                 e3d<<<grd, blk, 0, s>>>(k, *tab, LensEpi3D{}, n, chunk);
                 drive3d<<<grd_d, blk, 0, s>>>(k, *tab, *dr, n);
                 if (epi3d_active(&e, n))
-                    win3d<<<dim3(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx), blk, 0, s>>>(k, *tab, e, n);
+                    win3d<<<dim3((g->pitch + BK * WK - 1) / (BK * WK), (g->ny + BJ - 1) / BJ, g->nx), blk, 0, s>>>(
+                        k, *tab, e, n);
             } else {
                 e3d<<<grd, blk, 0, s>>>(k, *tab, e, n, chunk);
             }
@@ -1558,7 +1569,7 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
         }
     }
     bgr.xb[e.nbox] = bgz;
-    const dim3 grd_w(g->pitch / BK, (g->ny + BJ - 1) / BJ, g->nx);
+    const dim3 grd_w((g->pitch + BK * WK - 1) / (BK * WK), (g->ny + BJ - 1) / BJ, g->nx);
     for (int n = n0; n < n0 + nsteps; ++n) {
         const int rb = g->cur;
         const K3 k = view(g, rb, 1 - rb);

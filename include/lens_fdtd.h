@@ -162,7 +162,7 @@ typedef struct {
                                     can join a batch that is already running    */
 } LensInst2D;
 
-/* Block plan of a batch for tiles of 32 columns x 4*by rows: writes blk[0..ninst]
+/* Block plan of a batch for tiles of 128 columns x 2*by rows: writes blk[0..ninst]
  * (first block of each instance) and, when owner is not NULL, owner[b] (the
  * instance of block b, one entry per block); returns the block count, or < 0. */
 int lens_batch2d_plan(const LensInst2D *inst, int ninst, int by, int *blk, int *owner);
@@ -182,7 +182,7 @@ int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, c
  * counterpart in the reference.  The descriptors (inst, in host memory), the
  * block offsets and the owner table are placed in one fixed device array of
  * about 8.6 MB that every GPU loading this library holds until the process
- * exits; at most 512 instances and 2^21 tiles (32 x 4*by nodes each) per call,
+ * exits; at most 512 instances and 2^21 tiles (128 x 2*by nodes each) per call,
  * larger calls return LENS_ERR_SIZE.  Nothing is allocated.  The first call on
  * a device looks up that array's device address; make it before any stream
  * capture.  Every call rewrites the whole array (nothing carries over between

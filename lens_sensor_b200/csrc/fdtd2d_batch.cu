@@ -1,9 +1,9 @@
 // Batched 2D TE/TM steps for sm_100a: many independent solves of uneven sizes
 // advanced together (tear-film / bead sweeps).
 //
-// One launch per half step covers every tile of every instance (32 columns x
-// 4 * blockDim.y rows, four rows per thread); block b reads its instance from
-// the plan's owner table (lens_batch2d_plan).  The per-cell arithmetic is term for
+// One launch per half step covers every tile of every instance (128 columns x
+// 2 * blockDim.y rows; a thread updates 4 columns of 2 rows); block b reads its
+// instance from the plan's owner table (lens_batch2d_plan).  The per-cell arithmetic is term for
 // term the single-grid kernels' (fdtd2d.cu, after planar_beads/boundaries.py:
 // 164-274, source vcsel.py:151-156, loss fdtd2d_core.py:796-797), with the
 // fields read and written in the batch's storage type (FP32, FP16 or BF16) and
@@ -25,43 +25,79 @@ constexpr int BXB = 32;  // lanes along y (contiguous)
 
 template <typename T>
 struct St;
+// Storage access of VEC = 4 consecutive values (16 bytes FP32, 8 bytes FP16/BF16;
+// every access starts at a multiple of 4 elements).  Conversions round to
+// nearest even per element.
 template <>
 struct St<float> {
+    static __device__ __forceinline__ float4 ld4(const void *p, size_t o) {
+        return *reinterpret_cast<const float4 *>(static_cast<const float *>(p) + o);
+    }
+    static __device__ __forceinline__ void st4(void *p, size_t o, float4 v) {
+        *reinterpret_cast<float4 *>(static_cast<float *>(p) + o) = v;
+    }
     static __device__ __forceinline__ float ld(const void *p, size_t o) { return static_cast<const float *>(p)[o]; }
-    static __device__ __forceinline__ void st(void *p, size_t o, float v) { static_cast<float *>(p)[o] = v; }
 };
 template <>
 struct St<__half> {
+    static __device__ __forceinline__ float4 ld4(const void *p, size_t o) {
+        const uint2 u = *reinterpret_cast<const uint2 *>(static_cast<const __half *>(p) + o);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    static __device__ __forceinline__ void st4(void *p, size_t o, float4 v) {
+        const __half2 a = __floats2half2_rn(v.x, v.y), b = __floats2half2_rn(v.z, v.w);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned *>(&a);
+        u.y = *reinterpret_cast<const unsigned *>(&b);
+        *reinterpret_cast<uint2 *>(static_cast<__half *>(p) + o) = u;
+    }
     static __device__ __forceinline__ float ld(const void *p, size_t o) {
         return __half2float(static_cast<const __half *>(p)[o]);
-    }
-    static __device__ __forceinline__ void st(void *p, size_t o, float v) {
-        static_cast<__half *>(p)[o] = __float2half_rn(v);
     }
 };
 template <>
 struct St<__nv_bfloat16> {
+    static __device__ __forceinline__ float4 ld4(const void *p, size_t o) {
+        const uint2 u = *reinterpret_cast<const uint2 *>(static_cast<const __nv_bfloat16 *>(p) + o);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    static __device__ __forceinline__ void st4(void *p, size_t o, float4 v) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned *>(&a);
+        u.y = *reinterpret_cast<const unsigned *>(&b);
+        *reinterpret_cast<uint2 *>(static_cast<__nv_bfloat16 *>(p) + o) = u;
+    }
     static __device__ __forceinline__ float ld(const void *p, size_t o) {
         return __bfloat162float(static_cast<const __nv_bfloat16 *>(p)[o]);
     }
-    static __device__ __forceinline__ void st(void *p, size_t o, float v) {
-        static_cast<__nv_bfloat16 *>(p)[o] = __float2bfloat16_rn(v);
-    }
 };
 
-// A block covers a tile of 32 columns (lanes, contiguous y) x blockDim.y * RB
-// rows of one instance; each thread updates RB consecutive rows of its column,
-// issuing all of their loads before the arithmetic (the rows share the
-// x-neighbour loads).  The H and E passes are held to 64 registers (4 blocks of
-// 256 threads per SM): these passes wait on memory, and the extra resident
-// warps hide more of that latency than the registers would save.  owner[b] is the instance of block b and blk[q] its first
-// block; the descriptor fields are read through the read-only cache (every
-// thread of the block reads the same words).
-constexpr int RB = 4;
+__device__ __forceinline__ void f4_to(const float4 v, float *a) { a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w; }
+__device__ __forceinline__ float4 to_f4(const float *a) { return make_float4(a[0], a[1], a[2], a[3]); }
+
+// A block covers a tile of TW = 128 columns (y, contiguous) x blockDim.y * RB
+// rows (x) of one instance: each thread updates VEC = 4 consecutive columns of
+// RB consecutive rows, with one 16-byte (FP32) or 8-byte (FP16/BF16) access per
+// field and row, all issued before the arithmetic; the single column beyond
+// the thread's four (j+4 for H, j-1 for E) is a scalar load that hits the line
+// the neighbouring lane brought in.  The H and E passes are held to 64
+// registers (4 blocks of 256 threads per SM): they wait on memory, and the
+// extra resident warps hide more of that latency than registers would save.
+// owner[b] is the instance of block b and blk[q] its first block; the
+// descriptor fields are read through the read-only cache (every thread of the
+// block reads the same words).
+constexpr int RB = 2;
+constexpr int VEC = 4;
+constexpr int TW = BXB * VEC;
 
 struct Tile {
     const LensInst2D *g;
-    int i, j;  // first row of this thread, column
+    int i, j;  // first row and first column of this thread
 };
 
 __device__ __forceinline__ Tile tile_of(const LensInst2D *inst, const int *blk, const int *owner) {
@@ -69,8 +105,9 @@ __device__ __forceinline__ Tile tile_of(const LensInst2D *inst, const int *blk, 
     const int q = __ldg(owner + b);
     const LensInst2D *g = inst + q;
     const int t = b - __ldg(blk + q);
-    const int ntj = (__ldg(&g->ny) + BXB - 1) / BXB;
-    return Tile{g, (t / ntj) * (int)blockDim.y * RB + (int)threadIdx.y * RB, (t % ntj) * BXB + (int)threadIdx.x};
+    const int ntj = (__ldg(&g->ny) + TW - 1) / TW;
+    return Tile{g, (t / ntj) * (int)blockDim.y * RB + (int)threadIdx.y * RB,
+                (t % ntj) * TW + (int)threadIdx.x * VEC};
 }
 
 // Read-only view of one instance descriptor (loads through the non-coherent cache).
@@ -124,76 +161,101 @@ template <typename T>
 __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
     const Tile tl = tile_of(inst, blk, owner);
     const V g{tl.g};
-    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    if (i0 >= nx || j0 >= ny) return;   // j0 < ny <= P: the four columns lie inside the row pitch
     const float ch = g.ch();
     using S = St<T>;
     const LensProfile &xh = g.prof(true, false), &yh = g.prof(false, false);
+    const int wy = yh.lo + yh.hi;
     if (g.pol() == 0) {  // TE: Hx, Hy from Ez (boundaries.py:186-194)
-        if (i0 >= nx || j >= ny) return;
         const void *ezp = g.f(0);
         void *hxp = g.f(1), *hyp = g.f(2);
-        float ez[RB + 1], ezj[RB], hx[RB], hy[RB];
+        float ez[RB + 1][VEC], ezn[RB], hx[RB][VEC], hy[RB][VEC];
 #pragma unroll
-        for (int r = 0; r <= RB; ++r) ez[r] = (i0 + r < nx) ? S::ld(ezp, (size_t)(i0 + r) * P + j) : 0.f;
+        for (int r = 0; r <= RB; ++r) {
+            const bool in = i0 + r < nx;
+            f4_to(in ? S::ld4(ezp, (size_t)(i0 + r) * P + j0) : make_float4(0.f, 0.f, 0.f, 0.f), ez[r]);
+        }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
-            const size_t o = (size_t)(i0 + r) * P + j;
+            const size_t o = (size_t)(i0 + r) * P + j0;
             const bool in = i0 + r < nx;
-            ezj[r] = (in && j < ny - 1) ? S::ld(ezp, o + 1) : 0.f;
-            hx[r] = in ? S::ld(hxp, o) : 0.f;
-            hy[r] = in ? S::ld(hyp, o) : 0.f;
+            ezn[r] = (in && j0 + VEC < ny) ? S::ld(ezp, o + VEC) : 0.f;
+            f4_to(in ? S::ld4(hxp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hx[r]);
+            f4_to(in ? S::ld4(hyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hy[r]);
         }
-        const int sj = j < ny - 1 ? strip_of(j, yh.lo, yh.hi, yh.n) : -1;
-        const float kj = j < ny - 1 ? __ldg(yh.ik + j) : 0.f;
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
             const int i = i0 + r;
             if (i >= nx) break;
-            const size_t o = (size_t)i * P + j;
-            if (j < ny - 1) {
-                const float d = ezj[r] - ez[r];
-                float p = 0.f;
-                if (sj >= 0) p = psi_step(yh, j, g.psi(0) + (size_t)i * (yh.lo + yh.hi) + sj, d);
-                S::st(hxp, o, hx[r] - ch * (d * kj + p));
+            const size_t o = (size_t)i * P + j0;
+            float nhx[VEC], nhy[VEC];
+            const int s = i < nx - 1 ? strip_of(i, xh.lo, xh.hi, xh.n) : -1;
+            const float ki = i < nx - 1 ? __ldg(xh.ik + i) : 0.f;
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+                const int j = j0 + c;
+                nhx[c] = hx[r][c];
+                nhy[c] = hy[r][c];
+                if (j < ny - 1) {
+                    const float d = (c + 1 < VEC ? ez[r][c + 1] : ezn[r]) - ez[r][c];
+                    float p = 0.f;
+                    const int sj = strip_of(j, yh.lo, yh.hi, yh.n);
+                    if (sj >= 0) p = psi_step(yh, j, g.psi(0) + (size_t)i * wy + sj, d);
+                    nhx[c] = hx[r][c] - ch * (d * __ldg(yh.ik + j) + p);
+                }
+                if (i < nx - 1 && j < ny) {
+                    const float d = ez[r + 1][c] - ez[r][c];
+                    float p = 0.f;
+                    if (s >= 0) p = psi_step(xh, i, g.psi(1) + (size_t)s * P + j, d);
+                    nhy[c] = hy[r][c] + ch * (d * ki + p);
+                }
             }
-            if (i < nx - 1) {
-                const float d = ez[r + 1] - ez[r];
-                float p = 0.f;
-                const int s = strip_of(i, xh.lo, xh.hi, xh.n);
-                if (s >= 0) p = psi_step(xh, i, g.psi(1) + (size_t)s * P + j, d);
-                S::st(hyp, o, hy[r] + ch * (d * __ldg(xh.ik + i) + p));
-            }
+            S::st4(hxp, o, to_f4(nhx));
+            S::st4(hyp, o, to_f4(nhy));
         }
         return;
     }
     // TM: Hz from Ex, Ey (boundaries.py:240-247)
-    if (i0 >= nx - 1 || j >= ny - 1) return;
+    if (i0 >= nx - 1) return;
     const void *exp_ = g.f(0), *eyp = g.f(1);
     void *hzp = g.f(2);
-    float ey[RB + 1], ex[RB], exj[RB], hz[RB];
+    float ey[RB + 1][VEC], ex[RB][VEC], exn[RB], hz[RB][VEC];
 #pragma unroll
-    for (int r = 0; r <= RB; ++r) ey[r] = (i0 + r < nx) ? S::ld(eyp, (size_t)(i0 + r) * P + j) : 0.f;
+    for (int r = 0; r <= RB; ++r) {
+        const bool in = i0 + r < nx;
+        f4_to(in ? S::ld4(eyp, (size_t)(i0 + r) * P + j0) : make_float4(0.f, 0.f, 0.f, 0.f), ey[r]);
+    }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
-        const size_t o = (size_t)(i0 + r) * P + j;
+        const size_t o = (size_t)(i0 + r) * P + j0;
         const bool in = i0 + r < nx - 1;
-        ex[r] = in ? S::ld(exp_, o) : 0.f;
-        exj[r] = in ? S::ld(exp_, o + 1) : 0.f;
-        hz[r] = in ? S::ld(hzp, o) : 0.f;
+        f4_to(in ? S::ld4(exp_, o) : make_float4(0.f, 0.f, 0.f, 0.f), ex[r]);
+        exn[r] = (in && j0 + VEC < ny) ? S::ld(exp_, o + VEC) : 0.f;
+        f4_to(in ? S::ld4(hzp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hz[r]);
     }
-    const int sj = strip_of(j, yh.lo, yh.hi, yh.n);
-    const float kj = __ldg(yh.ik + j);
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
         const int i = i0 + r;
         if (i >= nx - 1) break;
-        const size_t o = (size_t)i * P + j;
-        const float dyx = ey[r + 1] - ey[r], dxy = exj[r] - ex[r];
-        float px = 0.f, py = 0.f;
+        const size_t o = (size_t)i * P + j0;
         const int s = strip_of(i, xh.lo, xh.hi, xh.n);
-        if (s >= 0) px = psi_step(xh, i, g.psi(0) + (size_t)s * P + j, dyx);
-        if (sj >= 0) py = psi_step(yh, j, g.psi(1) + (size_t)i * (yh.lo + yh.hi) + sj, dxy);
-        S::st(hzp, o, hz[r] - ch * ((dyx * __ldg(xh.ik + i) + px) - (dxy * kj + py)));
+        const float ki = __ldg(xh.ik + i);
+        float nhz[VEC];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+            const int j = j0 + c;
+            nhz[c] = hz[r][c];
+            if (j < ny - 1) {
+                const float dyx = ey[r + 1][c] - ey[r][c], dxy = (c + 1 < VEC ? ex[r][c + 1] : exn[r]) - ex[r][c];
+                float px = 0.f, py = 0.f;
+                const int sj = strip_of(j, yh.lo, yh.hi, yh.n);
+                if (s >= 0) px = psi_step(xh, i, g.psi(0) + (size_t)s * P + j, dyx);
+                if (sj >= 0) py = psi_step(yh, j, g.psi(1) + (size_t)i * wy + sj, dxy);
+                nhz[c] = hz[r][c] - ch * ((dyx * ki + px) - (dxy * __ldg(yh.ik + j) + py));
+            }
+        }
+        S::st4(hzp, o, to_f4(nhz));
     }
 }
 
@@ -202,119 +264,134 @@ __global__ void __launch_bounds__(256, 4)
     b2d_e(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
     const Tile tl = tile_of(inst, blk, owner);
     const V g{tl.g};
-    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    if (i0 >= nx || j0 >= ny) return;
     using S = St<T>;
     const LensProfile &xe = g.prof(true, true), &ye = g.prof(false, true);
+    const int wy = ye.lo + ye.hi;
     const LensSource &src = tl.g->src;
     const int *pec = tl.g->pec;
     const int six = __ldg(&src.ix), snj = __ldg(&src.nj);
     n -= __ldg(&tl.g->n_start);  // the instance's own step
     const int pec0 = __ldg(pec), pec1 = __ldg(pec + 1), pec2 = __ldg(pec + 2), pec3 = __ldg(pec + 3);
     if (g.pol() == 0) {  // TE: Ez (boundaries.py:196-215), source, PEC, node DFT
-        if (i0 >= nx || j >= ny) return;
         void *ezp = g.f(0);
         const void *hxp = g.f(1), *hyp = g.f(2);
         const float *ce = g.c(0), *chh = g.c(1);
-        const bool jin = j > 0 && j < ny - 1;
-        float hy[RB + 1], hx[RB], hxm[RB], ez[RB], c0[RB], c1[RB];
+        float hy[RB + 1][VEC], hx[RB][VEC], hxp1[RB], ez[RB][VEC];
 #pragma unroll
         for (int r = 0; r <= RB; ++r) {  // hy[r] = Hy(i0 + r - 1)
             const int i = i0 + r - 1;
-            hy[r] = (i >= 0 && i < nx && jin) ? S::ld(hyp, (size_t)i * P + j) : 0.f;
+            f4_to((i >= 0 && i < nx) ? S::ld4(hyp, (size_t)i * P + j0) : make_float4(0.f, 0.f, 0.f, 0.f), hy[r]);
         }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
             const int i = i0 + r;
-            const size_t o = (size_t)i * P + j;
+            const size_t o = (size_t)i * P + j0;
             const bool in = i < nx;
-            const bool upd = in && jin && i > 0 && i < nx - 1;
-            hx[r] = upd ? S::ld(hxp, o) : 0.f;
-            hxm[r] = upd ? S::ld(hxp, o - 1) : 0.f;
-            ez[r] = in ? S::ld(ezp, o) : 0.f;
-            c0[r] = upd ? __ldg(ce + o) : 0.f;
-            c1[r] = upd ? __ldg(chh + o) : 0.f;
+            f4_to(in ? S::ld4(hxp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hx[r]);
+            hxp1[r] = (in && j0 >= 1) ? S::ld(hxp, o - 1) : 0.f;       // Hx(i, j0-1)
+            f4_to(in ? S::ld4(ezp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ez[r]);
         }
-        const int sj = jin ? strip_of(j, ye.lo, ye.hi, ye.n) : -1;
-        const float kj = __ldg(ye.ik + j);
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
             const int i = i0 + r;
             if (i >= nx) break;
-            const size_t o = (size_t)i * P + j;
-            float v = ez[r];
-            if (jin && i > 0 && i < nx - 1) {
-                const float dhy = hy[r + 1] - hy[r], dhx = hx[r] - hxm[r];
-                float qx = 0.f, qy = 0.f;
-                const int s = strip_of(i, xe.lo, xe.hi, xe.n);
-                if (s >= 0) qx = psi_step(xe, i, g.psi(2) + (size_t)s * P + j, dhy);
-                if (sj >= 0) qy = psi_step(ye, j, g.psi(3) + (size_t)i * (ye.lo + ye.hi) + sj, dhx);
-                v = c0[r] * v + c1[r] * (dhy * __ldg(xe.ik + i) + qx - dhx * kj - qy);
+            const size_t o = (size_t)i * P + j0;
+            const int s = (i > 0 && i < nx - 1) ? strip_of(i, xe.lo, xe.hi, xe.n) : -1;
+            const float ki = __ldg(xe.ik + i);
+            float c0[VEC], c1[VEC], v4[VEC];
+            f4_to(__ldg(reinterpret_cast<const float4 *>(ce + o)), c0);
+            f4_to(__ldg(reinterpret_cast<const float4 *>(chh + o)), c1);
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+                const int j = j0 + c;
+                float v = ez[r][c];
+                if (j > 0 && j < ny - 1 && i > 0 && i < nx - 1) {
+                    const float dhy = hy[r + 1][c] - hy[r][c], dhx = hx[r][c] - (c > 0 ? hx[r][c - 1] : hxp1[r]);
+                    float qx = 0.f, qy = 0.f;
+                    const int sj = strip_of(j, ye.lo, ye.hi, ye.n);
+                    if (s >= 0) qx = psi_step(xe, i, g.psi(2) + (size_t)s * P + j, dhy);
+                    if (sj >= 0) qy = psi_step(ye, j, g.psi(3) + (size_t)i * wy + sj, dhx);
+                    v = c0[c] * v + c1[c] * (dhy * ki + qx - dhx * __ldg(ye.ik + j) - qy);
+                }
+                if ((i == six || i == six + 1) && j < snj) v += src_b(src, tab, n, i, j);
+                if ((pec0 && i == 0) || (pec1 && i == nx - 1) || (pec2 && j == 0) || (pec3 && j == ny - 1)) v = 0.f;
+                if (j >= ny) v = 0.f;
+                v4[c] = v;
+                if (j < ny) dft_node(tl.g, tab, n, o + c, v);
             }
-            if ((i == six || i == six + 1) && j < snj) v += src_b(src, tab, n, i, j);
-            if ((pec0 && i == 0) || (pec1 && i == nx - 1) || (pec2 && j == 0) || (pec3 && j == ny - 1)) v = 0.f;
-            S::st(ezp, o, v);
-            dft_node(tl.g, tab, n, o, v);
+            S::st4(ezp, o, to_f4(v4));
         }
         return;
     }
     // TM: loss damping, Ex / Ey (boundaries.py:249-268), source, PEC
-    if (i0 >= nx || j >= ny) return;
     void *exp_ = g.f(0), *eyp = g.f(1);
     const void *hzp = g.f(2);
     const float *cax = g.c(0), *cay = g.c(1), *dax = g.c(2), *day = g.c(3);
-    const bool jin = j > 0 && j < ny - 1;
-    float hz[RB + 1], hzj[RB], ex[RB], ey[RB], ax_[RB], ay_[RB], dx_[RB], dy_[RB];
+    float hz[RB + 1][VEC], hzp1[RB], ex[RB][VEC], ey[RB][VEC];
 #pragma unroll
     for (int r = 0; r <= RB; ++r) {  // hz[r] = Hz(i0 + r - 1)
         const int i = i0 + r - 1;
-        hz[r] = (i >= 0 && i < nx - 1 && j < ny - 1) ? S::ld(hzp, (size_t)i * P + j) : 0.f;
+        f4_to((i >= 0 && i < nx - 1) ? S::ld4(hzp, (size_t)i * P + j0) : make_float4(0.f, 0.f, 0.f, 0.f), hz[r]);
     }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
         const int i = i0 + r;
-        const size_t o = (size_t)i * P + j;
-        const bool exv = i < nx - 1, eyv = i < nx && j < ny - 1;
-        hzj[r] = (exv && jin) ? S::ld(hzp, o - 1) : 0.f;
-        ex[r] = exv ? S::ld(exp_, o) : 0.f;
-        ey[r] = eyv ? S::ld(eyp, o) : 0.f;
-        ax_[r] = (exv && jin) ? __ldg(cax + o) : 0.f;
-        ay_[r] = (eyv && i > 0 && i < nx - 1) ? __ldg(cay + o) : 0.f;
-        dx_[r] = (exv && dax) ? __ldg(dax + o) : 1.f;
-        dy_[r] = (eyv && day) ? __ldg(day + o) : 1.f;
+        const size_t o = (size_t)i * P + j0;
+        f4_to(i < nx - 1 ? S::ld4(exp_, o) : make_float4(0.f, 0.f, 0.f, 0.f), ex[r]);
+        hzp1[r] = (i < nx - 1 && j0 >= 1) ? S::ld(hzp, o - 1) : 0.f;   // Hz(i, j0-1)
+        f4_to(i < nx ? S::ld4(eyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ey[r]);
     }
-    const int sj = jin ? strip_of(j, ye.lo, ye.hi, ye.n) : -1;
-    const float kj = __ldg(ye.ik + j);
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
         const int i = i0 + r;
         if (i >= nx) break;
-        const size_t o = (size_t)i * P + j;
-        if (i < nx - 1) {  // Ex at (i+1/2, j)
-            float e = ex[r];
-            if (dax) e = e * dx_[r];
-            if (jin) {
-                const float d = hz[r + 1] - hzj[r];
-                float p = 0.f;
-                if (sj >= 0) p = psi_step(ye, j, g.psi(2) + (size_t)i * (ye.lo + ye.hi) + sj, d);
-                e = e + ax_[r] * (d * kj + p);
+        const size_t o = (size_t)i * P + j0;
+        const float4 ax4 = __ldg(reinterpret_cast<const float4 *>(cax + o));
+        const float4 ay4 = __ldg(reinterpret_cast<const float4 *>(cay + o));
+        const float4 dx4 = dax ? __ldg(reinterpret_cast<const float4 *>(dax + o)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        const float4 dy4 = day ? __ldg(reinterpret_cast<const float4 *>(day + o)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        float ax_[VEC], ay_[VEC], dx_[VEC], dy_[VEC];
+        f4_to(ax4, ax_); f4_to(ay4, ay_); f4_to(dx4, dx_); f4_to(dy4, dy_);
+        const int s = (i > 0 && i < nx - 1) ? strip_of(i, xe.lo, xe.hi, xe.n) : -1;
+        const float ki = __ldg(xe.ik + i);
+        float nex[VEC], ney[VEC];
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+            const int j = j0 + c;
+            const bool jin = j > 0 && j < ny - 1;
+            nex[c] = ex[r][c];
+            ney[c] = ey[r][c];
+            if (i < nx - 1 && j < ny) {  // Ex at (i+1/2, j)
+                float e = ex[r][c];
+                if (dax) e = e * dx_[c];
+                if (jin) {
+                    const float d = hz[r + 1][c] - (c > 0 ? hz[r + 1][c - 1] : hzp1[r]);
+                    float p = 0.f;
+                    const int sj = strip_of(j, ye.lo, ye.hi, ye.n);
+                    if (sj >= 0) p = psi_step(ye, j, g.psi(2) + (size_t)i * wy + sj, d);
+                    e = e + ax_[c] * (d * __ldg(ye.ik + j) + p);
+                }
+                if ((pec2 && j == 0) || (pec3 && j == ny - 1)) e = 0.f;
+                nex[c] = e;
             }
-            if ((pec2 && j == 0) || (pec3 && j == ny - 1)) e = 0.f;
-            S::st(exp_, o, e);
-        }
-        if (j < ny - 1) {  // Ey at (i, j+1/2)
-            float e = ey[r];
-            if (day) e = e * dy_[r];
-            if (i > 0 && i < nx - 1) {
-                const float d = hz[r + 1] - hz[r];
-                float p = 0.f;
-                const int s = strip_of(i, xe.lo, xe.hi, xe.n);
-                if (s >= 0) p = psi_step(xe, i, g.psi(3) + (size_t)s * P + j, d);
-                e = e + (-ay_[r]) * (d * __ldg(xe.ik + i) + p);
+            if (j < ny - 1) {  // Ey at (i, j+1/2)
+                float e = ey[r][c];
+                if (day) e = e * dy_[c];
+                if (i > 0 && i < nx - 1) {
+                    const float d = hz[r + 1][c] - hz[r][c];
+                    float p = 0.f;
+                    if (s >= 0) p = psi_step(xe, i, g.psi(3) + (size_t)s * P + j, d);
+                    e = e + (-ay_[c]) * (d * ki + p);
+                }
+                if ((i == six || i == six + 1) && j < snj) e += src_b(src, tab, n, i, j);
+                if ((pec0 && i == 0) || (pec1 && i == nx - 1)) e = 0.f;
+                ney[c] = e;
             }
-            if ((i == six || i == six + 1) && j < snj) e += src_b(src, tab, n, i, j);
-            if ((pec0 && i == 0) || (pec1 && i == nx - 1)) e = 0.f;
-            S::st(eyp, o, e);
         }
+        if (i < nx - 1) S::st4(exp_, o, to_f4(nex));
+        S::st4(eyp, o, to_f4(ney));
     }
 }
 
@@ -325,8 +402,8 @@ __global__ void __launch_bounds__(256)
     const Tile tl = tile_of(inst, blk, owner);
     const V g{tl.g};
     if (g.pol() != 1) return;
-    const int i0 = tl.i, j = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
-    if (i0 >= nx || j >= ny) return;
+    const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
+    if (i0 >= nx || j0 >= ny) return;
     n -= __ldg(&tl.g->n_start);
     using S = St<T>;
     const void *p1 = g.f(1);
@@ -335,9 +412,14 @@ __global__ void __launch_bounds__(256)
         const int i = i0 + r;
         if (i >= nx) break;
         const size_t row = (size_t)i * P;
-        const float v = (j == 0) ? S::ld(p1, row) : (j == ny - 1) ? S::ld(p1, row + ny - 2)
-                                                                : 0.5f * (S::ld(p1, row + j - 1) + S::ld(p1, row + j));
-        dft_node(tl.g, tab, n, row + j, v);
+#pragma unroll
+        for (int c = 0; c < VEC; ++c) {
+            const int j = j0 + c;
+            if (j >= ny) break;
+            const float v = (j == 0) ? S::ld(p1, row) : (j == ny - 1) ? S::ld(p1, row + ny - 2)
+                                                                    : 0.5f * (S::ld(p1, row + j - 1) + S::ld(p1, row + j));
+            dft_node(tl.g, tab, n, row + j, v);
+        }
     }
 }
 
@@ -354,7 +436,7 @@ bool inst_ok(const LensInst2D &g) {
 }
 
 long inst_blocks(const LensInst2D &g, int by) {
-    return (long)((g.ny + BXB - 1) / BXB) * ((g.nx + by * RB - 1) / (by * RB));
+    return (long)((g.ny + TW - 1) / TW) * ((g.nx + by * RB - 1) / (by * RB));
 }
 
 template <typename T>
@@ -437,7 +519,7 @@ extern "C" int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *
 namespace {
 
 constexpr int NA_MAX_INST = 512;                 // instances per call
-constexpr int NA_MAX_BLOCKS = 1 << 21;           // tiles per call (32 x 4*by nodes each)
+constexpr int NA_MAX_BLOCKS = 1 << 21;           // tiles per call (128 x 2*by nodes each)
 constexpr size_t NA_DESC_BYTES = ((NA_MAX_INST * sizeof(LensInst2D) + 255) / 256) * 256;
 constexpr size_t NA_BLK_BYTES = (((NA_MAX_INST + 1) * sizeof(int) + 255) / 256) * 256;
 constexpr size_t NA_BYTES = NA_DESC_BYTES + NA_BLK_BYTES + (size_t)NA_MAX_BLOCKS * sizeof(int);

@@ -41,7 +41,7 @@ def test_plan_of_uneven_instances():
     blk = (ctypes.c_int * 4)()
     by = 4
     n = lib.lens_batch2d_plan(arr, 3, by, blk, None)
-    per = [((ny + 31) // 32) * ((nx + 4 * by - 1) // (4 * by)) for nx, ny, _ in sizes]
+    per = [((ny + 127) // 128) * ((nx + 2 * by - 1) // (2 * by)) for nx, ny, _ in sizes]
     assert n == sum(per) and list(blk) == [0, per[0], per[0] + per[1], sum(per)]
     owner = (ctypes.c_int * n)()
     assert lib.lens_batch2d_plan(arr, 3, by, blk, owner) == n

@@ -236,7 +236,7 @@ def run_batched(plain_sample=16):
                 unit=UNIT, cells_total=cells, steps=steps, plain=plain,
                 plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time',
                 batched_f32=f32, batched_f16=f16, batched_vs_plain=f32 / plain, f16_vs_plain=f16 / plain,
-                tile_rows=4 * by, group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
+                tile=f'128 x {2 * by} nodes', group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
                 f16_phasor_err_vs_f32_max=max(err), f16_phasor_err_vs_f32_median=float(np.median(err)),
                 K_median=float(np.median(K)))
 

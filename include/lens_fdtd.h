@@ -122,6 +122,10 @@ typedef struct {
     double *plane_acc;           /* per plane: 4 rows of pitch doubles:
                                     E re, E im, H re, H im (H = mean of il-1, il);
                                     accumulated during the dft window          */
+    float *dft_raw;              /* TM: Ey on its own grid (nx, pitch), Kahan
+                                    layout as dft, during the dft window, or NULL */
+    float *ex2;                  /* TM: Ex^2 on the nodes summed during the dft
+                                    window (nx, pitch), or NULL                */
 } LensEpi2D;
 
 /* Advance `nsteps` steps starting at step n0 (t = n*dt, n = n0 ... n0+nsteps-1). */
@@ -129,6 +133,27 @@ int lens_te2d_step(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D 
                    int n0, int nsteps, void *stream);
 int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
                    int n0, int nsteps, void *stream);
+
+/* Stitch-window drive of a 2D grid (fdtd2d_core.py:1439-1440, 1462-1463): after
+ * each E update, before the PEC termination, the first nplanes x-rows of the
+ * driven component (TE: Ez, TM: Ey) become
+ *     w_i * (env * Re(D e^{+i w t})) + (1 - w_i) * E
+ * evaluated as the reference does: the complex64 amplitude D times the
+ * complex128 phase in FP64, w_i * (...) in FP64, (1 - w_i) * E in FP32, the sum
+ * rounded to FP32.                                                          */
+typedef struct {
+    int nplanes;                 /* O driven rows (0: no drive)                */
+    const float *taper;          /* O weights w_i                              */
+    const float *hand;           /* (O, pitch) x {re, im}: complex amplitudes   */
+    const double *tab;           /* per step n - t0: env, cos(w t), sin(w t)    */
+} LensDrive2D;
+
+/* lens_te2d_step / lens_tm2d_step with a stitch drive (no counterpart entry in
+ * the reference: its stitch loop assigns the overlap rows in NumPy).         */
+int lens_te2d_step_driven(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                          const LensDrive2D *drive, int n0, int nsteps, void *stream);
+int lens_tm2d_step_driven(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                          const LensDrive2D *drive, int n0, int nsteps, void *stream);
 
 /* ------------------------------------------------------- batched 2D solves
  * Many independent 2D solves of uneven sizes (TE and TM mixed) advanced together:
@@ -286,8 +311,8 @@ const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
  * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D,
- * LensDrive3D.  Writes min(n, 11) entries and returns 11 (bindings check their
- * mirrors). */
+ * LensDrive3D, LensDrive2D.  Writes min(n, 12) entries and returns 12 (bindings
+ * check their mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

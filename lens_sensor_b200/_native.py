@@ -58,7 +58,8 @@ class Epi2D(ctypes.Structure):
                 ('dft_n0', c_int), ('dft_n1', c_int), ('dft', c_void_p), ('dft_ex', c_void_p),
                 ('prev_n0', c_int), ('prev_n1', c_int), ('dft_prev', c_void_p),
                 ('iavg_n0', c_int), ('iavg', c_void_p),
-                ('nplane', c_int), ('plane', c_int * MAX_PLANE), ('plane_acc', c_void_p)]
+                ('nplane', c_int), ('plane', c_int * MAX_PLANE), ('plane_acc', c_void_p),
+                ('dft_raw', c_void_p), ('ex2', c_void_p)]
 
 
 NPSI = 12
@@ -98,13 +99,21 @@ class Drive3D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p * 3)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D)
+class Drive2D(ctypes.Structure):
+    _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p), ('tab', c_void_p)]
+
+
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
 SIGNATURES = {
     'lens_te2d_step': (c_int, [POINTER(TE2D), POINTER(StepTable), POINTER(Epi2D), c_int, c_int, c_void_p]),
     'lens_tm2d_step': (c_int, [POINTER(TM2D), POINTER(StepTable), POINTER(Epi2D), c_int, c_int, c_void_p]),
+    'lens_te2d_step_driven': (c_int, [POINTER(TE2D), POINTER(StepTable), POINTER(Epi2D), POINTER(Drive2D), c_int,
+                                      c_int, c_void_p]),
+    'lens_tm2d_step_driven': (c_int, [POINTER(TM2D), POINTER(StepTable), POINTER(Epi2D), POINTER(Drive2D), c_int,
+                                      c_int, c_void_p]),
     'lens_fdtd3d_step': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), c_int, c_int, c_void_p]),
     'lens_fdtd3d_step_driven': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), POINTER(Drive3D),
                                         c_int, c_int, c_void_p]),

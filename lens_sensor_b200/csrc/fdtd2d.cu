@@ -76,6 +76,18 @@ __device__ __forceinline__ bool in_window(const LensEpi2D &ep, int n) {
     return n >= ep.dft_n0 && n < ep.dft_n1;
 }
 
+// Stitch drive of one cell of the driven component (rows i < d.nplanes):
+// w * (env * Re(D e^{iwt})) in FP64 plus (1 - w) * E in FP32, rounded to FP32.
+__device__ __forceinline__ float drive2(const LensDrive2D &d, const LensStepTable &tab, int n, int i,
+                                        size_t o, float e) {
+    const double *t = d.tab + 3 * (size_t)(n - tab.t0);
+    const float2 D = reinterpret_cast<const float2 *>(d.hand)[o];
+    const double re = __dsub_rn(__dmul_rn((double)D.x, t[1]), __dmul_rn((double)D.y, t[2]));
+    const double din = __dmul_rn(t[0], re);
+    const float w = d.taper[i];
+    return (float)__dadd_rn(__dmul_rn((double)w, din), (double)__fmul_rn(__fsub_rn(1.0f, w), e));
+}
+
 // ------------------------------------------------------------------ TE
 __global__ void __launch_bounds__(BX *BY) te2d_h(const LensTE2D g) {
     const int j = blockIdx.x * BX + threadIdx.x;
@@ -109,7 +121,7 @@ __global__ void __launch_bounds__(BX *BY) te2d_h(const LensTE2D g) {
 }
 
 __global__ void __launch_bounds__(BX *BY)
-    te2d_e(const LensTE2D g, const LensStepTable tab, const LensEpi2D ep, int n) {
+    te2d_e(const LensTE2D g, const LensStepTable tab, const LensEpi2D ep, int n, const LensDrive2D d) {
     const int j = blockIdx.x * BX + threadIdx.x;
     const int i = blockIdx.y * BY + threadIdx.y;
     const bool valid = i < g.nx && j < g.ny;
@@ -137,7 +149,9 @@ __global__ void __launch_bounds__(BX *BY)
             ez = g.ce_e[o] * ez +
                  g.ce_h[o] * (dhy * g.ax.e.ik[i] + qx - dhx * g.ay.e.ik[j] - qy);
         }
-        if ((i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj) ez += src_term(g.src, tab, n, i, j);
+        if (g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj)
+            ez += src_term(g.src, tab, n, i, j);
+        if (i < d.nplanes) ez = drive2(d, tab, n, i, o, ez);
         if ((g.pec[0] && i == 0) || (g.pec[1] && i == g.nx - 1) || (g.pec[2] && j == 0) ||
             (g.pec[3] && j == g.ny - 1))
             ez = 0.f;
@@ -177,7 +191,7 @@ __global__ void __launch_bounds__(BX *BY) tm2d_h(const LensTM2D g) {
 }
 
 __global__ void __launch_bounds__(BX *BY)
-    tm2d_e(const LensTM2D g, const LensStepTable tab, int n) {
+    tm2d_e(const LensTM2D g, const LensStepTable tab, int n, const LensDrive2D d) {
     const int j = blockIdx.x * BX + threadIdx.x;
     const int i = blockIdx.y * BY + threadIdx.y;
     const int P = g.pitch;
@@ -213,7 +227,9 @@ __global__ void __launch_bounds__(BX *BY)
             }
             e = e + (-g.ca_y[o]) * (d * g.ax.e.ik[i] + p);
         }
-        if ((i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj) e += src_term(g.src, tab, n, i, j);
+        if (g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1) && j < g.src.nj)
+            e += src_term(g.src, tab, n, i, j);
+        if (i < d.nplanes) e = drive2(d, tab, n, i, o, e);
         if ((g.pec[0] && i == 0) || (g.pec[1] && i == g.nx - 1)) e = 0.f;
         g.ey[o] = e;
     }
@@ -247,6 +263,14 @@ __global__ void __launch_bounds__(BX *BY)
             exn = 0.5f * (a + b);
         }
         inten = field * field + s2;
+        if (in_window(ep, n)) {  // stitch: Ey on its own grid, Ex^2 on the nodes
+            if (ep.dft_raw && j < ny - 1) {
+                const int k = n - tab.t0;
+                const float v = g.ey[o];
+                kahan_add(reinterpret_cast<float4 *>(ep.dft_raw) + o, v * tab.pe[2 * k], v * tab.pe[2 * k + 1]);
+            }
+            if (ep.ex2) ep.ex2[o] += s2;
+        }
         if (ep.nplane > 0 && in_window(ep, n) && j < ny - 1) {
             for (int p = 0; p < ep.nplane; ++p)
                 if (i == ep.plane[p])
@@ -259,7 +283,8 @@ __global__ void __launch_bounds__(BX *BY)
 bool epi2d_active(const LensEpi2D *ep, int n) {
     if (!ep) return false;
     if (ep->nbox > 0) return true;
-    if ((ep->dft || ep->dft_ex || ep->nplane > 0) && n >= ep->dft_n0 && n < ep->dft_n1) return true;
+    if ((ep->dft || ep->dft_ex || ep->dft_raw || ep->ex2 || ep->nplane > 0) && n >= ep->dft_n0 && n < ep->dft_n1)
+        return true;
     if (ep->dft_prev && n >= ep->prev_n0 && n < ep->prev_n1) return true;
     return ep->iavg && n >= ep->iavg_n0;
 }
@@ -271,7 +296,7 @@ bool epi2d_ok(const LensEpi2D *ep, const LensStepTable *t, int nx) {
         return false;
     for (int p = 0; p < ep->nplane; ++p)  // H is averaged over rows il-1 and il
         if (ep->plane[p] < 1 || ep->plane[p] > nx - 2) return false;
-    const bool dft = ep->dft || ep->dft_ex || ep->dft_prev || ep->nplane > 0;
+    const bool dft = ep->dft || ep->dft_ex || ep->dft_prev || ep->dft_raw || ep->nplane > 0;
     return !dft || (t->pe && t->ph);
 }
 
@@ -291,36 +316,66 @@ LensEpi2D empty_epi() {
     return e;
 }
 
-}  // namespace
+// A drive table must cover the steps run, its amplitudes the driven rows.
+bool drive2d_ok(const LensDrive2D *d, const LensStepTable *tab, int nx) {
+    return !d || d->nplanes == 0 || (d->nplanes > 0 && d->nplanes <= nx && d->taper && d->hand && d->tab &&
+                                     (reinterpret_cast<uintptr_t>(d->hand) & 7) == 0 && tab);
+}
 
-extern "C" int lens_te2d_step(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep,
-                              int n0, int nsteps, void *stream) {
+int te2d_run(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep, const LensDrive2D *dr, int n0,
+             int nsteps, void *stream) {
     if (!grid2d_ok(g) || !g->ez || !g->hx || !g->hy || !g->ce_e || !g->ce_h || nsteps < 0 ||
-        !lens_table_ok(tab, n0, nsteps) || !epi2d_ok(ep, tab, g->nx))
+        !lens_table_ok(tab, n0, nsteps) || !epi2d_ok(ep, tab, g->nx) || !drive2d_ok(dr, tab, g->nx))
         return LENS_ERR_ARG;
     const LensEpi2D e = ep ? *ep : empty_epi();
+    const LensDrive2D d = dr ? *dr : LensDrive2D{};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const dim3 blk(BX, BY), grd((g->ny + BX - 1) / BX, (g->nx + BY - 1) / BY);
     for (int n = n0; n < n0 + nsteps; ++n) {
         te2d_h<<<grd, blk, 0, s>>>(*g);
-        te2d_e<<<grd, blk, 0, s>>>(*g, *tab, e, n);
+        te2d_e<<<grd, blk, 0, s>>>(*g, *tab, e, n, d);
     }
     return lens_cuda_status();
 }
 
-extern "C" int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
-                              int n0, int nsteps, void *stream) {
+int tm2d_run(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep, const LensDrive2D *dr, int n0,
+             int nsteps, void *stream) {
     if (!grid2d_ok(g) || !g->ex || !g->ey || !g->hz || !g->ca_x || !g->ca_y ||
         (!g->da_x) != (!g->da_y) || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) ||
-        !epi2d_ok(ep, tab, g->nx))
+        !epi2d_ok(ep, tab, g->nx) || !drive2d_ok(dr, tab, g->nx))
         return LENS_ERR_ARG;
     const LensEpi2D e = ep ? *ep : empty_epi();
+    const LensDrive2D d = dr ? *dr : LensDrive2D{};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const dim3 blk(BX, BY), grd((g->ny + BX - 1) / BX, (g->nx + BY - 1) / BY);
     for (int n = n0; n < n0 + nsteps; ++n) {
         tm2d_h<<<grd, blk, 0, s>>>(*g);
-        tm2d_e<<<grd, blk, 0, s>>>(*g, *tab, n);
+        tm2d_e<<<grd, blk, 0, s>>>(*g, *tab, n, d);
         if (epi2d_active(&e, n)) tm2d_epi<<<grd, blk, 0, s>>>(*g, *tab, e, n);
     }
     return lens_cuda_status();
+}
+
+}  // namespace
+
+extern "C" int lens_te2d_step(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                              int n0, int nsteps, void *stream) {
+    return te2d_run(g, tab, ep, nullptr, n0, nsteps, stream);
+}
+
+extern "C" int lens_tm2d_step(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                              int n0, int nsteps, void *stream) {
+    return tm2d_run(g, tab, ep, nullptr, n0, nsteps, stream);
+}
+
+extern "C" int lens_te2d_step_driven(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                                     const LensDrive2D *drive, int n0, int nsteps, void *stream) {
+    if (!drive) return LENS_ERR_ARG;
+    return te2d_run(g, tab, ep, drive, n0, nsteps, stream);
+}
+
+extern "C" int lens_tm2d_step_driven(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep,
+                                     const LensDrive2D *drive, int n0, int nsteps, void *stream) {
+    if (!drive) return LENS_ERR_ARG;
+    return tm2d_run(g, tab, ep, drive, n0, nsteps, stream);
 }

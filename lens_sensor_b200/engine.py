@@ -140,10 +140,14 @@ class Grid2D:
         self.ch = F32(dt / (MU0 * dx))
         self.axx, self.axy = _Axis(cx, nx, dev), _Axis(cy, ny, dev)
         wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
-        self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
-                      for k in ('amp', 'ph1', 'ph2')}
-        s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
-                     _ptr(self.src_t['ph2']), len(src['amp']), 1, len(src['amp']))
+        if src is None:                # no source (a stitch window driven by its predecessor)
+            self.src_t = {}
+            s = N.Source(-1, None, None, None, 0, 0, 0)
+        else:
+            self.src_t = {k: torch.from_numpy(np.ascontiguousarray(src[k], F32)).to(dev)
+                          for k in ('amp', 'ph1', 'ph2')}
+            s = N.Source(int(src['ix']), _ptr(self.src_t['amp']), _ptr(self.src_t['ph1']),
+                         _ptr(self.src_t['ph2']), len(src['amp']), 1, len(src['amp']))
         pec4 = (ctypes.c_int * 4)(*[int(bool(v)) for v in pec])
         if self.pol == 's':
             self.ez, self.hx, self.hy = z(), z(), z()
@@ -178,18 +182,48 @@ class Grid2D:
         a, b = shapes[name]
         return getattr(self, name)[:a, :b]
 
-    def step(self, table, n0, nsteps, epi=None, stream=None):
-        fn = self.lib.lens_te2d_step if self.pol == 's' else self.lib.lens_tm2d_step
-        e = epi.s if epi is not None else None
-        N.check(fn(ctypes.byref(self.s), ctypes.byref(table.s),
-                   ctypes.byref(e) if e is not None else None, int(n0), int(nsteps),
-                   _stream_ptr(stream)))
+    def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
+        e = ctypes.byref(epi.s) if epi is not None else None
+        if drive is None:
+            fn = self.lib.lens_te2d_step if self.pol == 's' else self.lib.lens_tm2d_step
+            N.check(fn(ctypes.byref(self.s), ctypes.byref(table.s), e, int(n0), int(nsteps), _stream_ptr(stream)))
+        else:
+            fn = self.lib.lens_te2d_step_driven if self.pol == 's' else self.lib.lens_tm2d_step_driven
+            N.check(fn(ctypes.byref(self.s), ctypes.byref(table.s), e, ctypes.byref(drive.s), int(n0),
+                       int(nsteps), _stream_ptr(stream)))
+
+
+class Drive2D:
+    """Overlap drive of a 2D stitch window (fdtd2d_core.py:1439-1440, 1462-1463).
+
+    hand: complex64 amplitudes (O, ny_c) of the driven component (TE Ez, TM Ey);
+    taper: the O weights w_i (float32); env, cos_wt, sin_wt: float64 per step
+    n - t0 of the step table (the reference's float envelope and complex128
+    phase e^{i w t})."""
+
+    def __init__(self, grid, hand, taper, env, cos_wt, sin_wt):
+        dev, P = grid.dev, grid.pitch
+        D = torch.as_tensor(hand).to(dev)
+        O = int(D.shape[0])
+        self.taper = torch.from_numpy(np.ascontiguousarray(taper, F32)).to(dev)
+        self.hand = torch.zeros((O, P, 2), dtype=torch.float32, device=dev)
+        self.hand[:, :D.shape[1], 0] = D.real.float()
+        self.hand[:, :D.shape[1], 1] = D.imag.float()
+        tab = np.stack([np.asarray(env, np.float64), np.asarray(cos_wt, np.float64),
+                        np.asarray(sin_wt, np.float64)], axis=1)
+        self.tab = torch.from_numpy(np.ascontiguousarray(tab)).to(dev)
+        s = N.Drive2D()
+        s.nplanes, s.taper, s.hand, s.tab = O, _ptr(self.taper), _ptr(self.hand), _ptr(self.tab)
+        self.s = s
 
 
 class Epi2D:
     """Epilogue buffers of a 2D solve (detector boxes, DFTs, Iavg, flux planes)."""
 
-    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=()):
+    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=(),
+                 dft_raw=False, ex2=False):
+        """dft_raw / ex2 (TM): the DFT of Ey on its own grid and the sum of Ex^2 on
+        the nodes over the dft window (run_beads_stitched, fdtd2d_core.py:1441-1446)."""
         dev, nx, P = grid.dev, grid.nx, grid.pitch
         self.grid = grid
         self.boxes = [tuple(int(v) for v in b) for b in boxes]
@@ -198,6 +232,8 @@ class Epi2D:
         self.dft = d4() if dft is not None else None
         self.dft_ex = d4() if (dft is not None and dft_ex) else None
         self.prev = d4() if prev is not None else None
+        self.dft_raw = d4() if (dft is not None and dft_raw) else None
+        self.ex2 = torch.zeros((nx, P), dtype=torch.float32, device=dev) if (dft is not None and ex2) else None
         self.iavg = torch.zeros((nx, P), dtype=torch.float32, device=dev) if iavg_n0 is not None else None
         self.planes = dict(planes)
         self.plane_acc = torch.zeros((max(1, len(self.planes)), 4, P), dtype=torch.float64, device=dev)
@@ -216,11 +252,24 @@ class Epi2D:
         for q, il in enumerate(self.planes.values()):
             s.plane[q] = int(il)
         s.plane_acc = _ptr(self.plane_acc)
+        s.dft_raw, s.ex2 = _ptr(self.dft_raw), _ptr(self.ex2)
         self.s = s
 
-    def phasor(self, which='dft'):
-        """Accumulated sum(F e^{-i w t}) on the nodes (nx, ny), complex128."""
-        return _kahan_value(getattr(self, which))[:, :self.grid.ny]
+    def phasor(self, which='dft', kind=None):
+        """Accumulated sum(F e^{-i w t}) on the nodes (nx, ny) ('dft_raw': on the
+        Ey grid (nx, ny-1)), complex128.  kind='stitch' names the reference's
+        complex64 window sums of run_beads_stitched; the device keeps one
+        compensated FP32 sum per quantity, which serves both."""
+        ny = self.grid.ny - (1 if which == 'dft_raw' else 0)
+        return _kahan_value(getattr(self, which))[:, :ny]
+
+    def plane_dft(self, name):
+        """[(sign, sum E e^{-iwt}, sum H e^{-iw(t-dt/2)})] of plane `name` (pairs_2d), complex128."""
+        q = list(self.planes).index(name)
+        a = self.plane_acc[q]
+        ny = self.grid.ny if self.grid.pol == 's' else self.grid.ny - 1
+        sign = -1.0 if self.grid.pol == 's' else 1.0
+        return [(sign, torch.complex(a[0, :ny], a[1, :ny]), torch.complex(a[2, :ny], a[3, :ny]))]
 
     def restart_dft(self, window):
         """Open a new DFT window [n0, n1) after a failed CW convergence check

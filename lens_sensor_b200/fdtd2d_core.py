@@ -63,12 +63,32 @@ def run_beads(wg_mat, bead_mat, bead_d_um, dx_nm=20.0, save_frames=True, n_snaps
               cad=None, pulse_cycles=30.0, pulse_tmax_fs=None, pulse_nfreq=None,
               pulse_dispersion=True, pulse_mode='fourier', n_aq_tear_offset=None,
               tear_buffer_um=None, stack=None):
-    """2D TE/TM full-domain CW solve (fdtd2d_core.py:531-927) on the GPU engine."""
+    """2D TE/TM full-domain CW solve (fdtd2d_core.py:531-927) on the GPU engine;
+    method='stitch' runs run_beads_stitched (fdtd2d_core.py:599-608)."""
+    if method == 'stitch' and str(source_type).lower() != 'pulse':
+        global TEAR_BUFFER
+        old = TEAR_BUFFER
+        if stack is not None and tear_buffer_um is None and cad is None:
+            need = sum(float(L['t_um']) for L in stack) + 1.5 + 10 * dx_nm * 1e-3
+            if need * 1e-6 > TEAR_BUFFER + 1e-12:
+                tear_buffer_um = need
+        if tear_buffer_um is not None:
+            TEAR_BUFFER = float(tear_buffer_um) * 1e-6
+        try:
+            return run_beads_stitched(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
+                                      wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt, vcsel_offset,
+                                      source_type, window_w_um, slide_um, place_bead, t_aqueous_um,
+                                      t_mucin_um=t_mucin_um, t_lipid_um=t_lipid_um, input_gap_um=input_gap_um,
+                                      length_um=length_um, bead_x_um=bead_x_um, bead_y_um=bead_y_um, wg_n=wg_n,
+                                      bead_n=bead_n, n_aqueous=n_aqueous, n_mucin=n_mucin, n_cornea=n_cornea,
+                                      n_lipid=n_lipid, polarization=polarization, curved=curved,
+                                      boundary=boundary, cad=cad, stack=stack)
+        finally:
+            TEAR_BUFFER = old
     if method != 'full' or str(boundary).lower() != 'cpml' or source_type != 'cw' or cad is not None or curved:
         raise NotImplementedError(f'lens_sensor_b200.run_beads: method={method!r} boundary={boundary!r} '
                                   f'source_type={source_type!r} cad={cad is not None} curved={curved}: '
                                   f'only the full-domain CPML CW path runs on the B200 engine')
-    global TEAR_BUFFER
     if stack is not None and tear_buffer_um is None:
         need = sum(float(L['t_um']) for L in stack) + 1.5 + 10 * dx_nm * 1e-3
         if need * 1e-6 > TEAR_BUFFER + 1e-12:
@@ -220,6 +240,264 @@ def run_beads(wg_mat, bead_mat, bead_d_um, dx_nm=20.0, save_frames=True, n_snaps
     return res
 
 
+def _stack_2d(wg_n, wg_thickness_um, t_lipid_um, n_lip, t_aq_um, n_aq, t_mucin_um, n_mu, n_co, stack):
+    """Layer stack and loss switch of run_beads (fdtd2d_core.py:144-213)."""
+    k = dict(KAPPA or {})
+    if stack is None:
+        lossy = any(v > 0 for v in k.values())
+        t_mu = (t_mucin_um * 1e-6) if t_mucin_um is not None else T_MU
+        st = _legacy_stack(wg_n, wg_thickness_um, (t_lipid_um or 0.0) * 1e-6, n_lip, t_aq_um * 1e-6,
+                           n_aq, t_mu, n_mu, n_co, lossy, k)
+    else:
+        lossy = any(v > 0 for v in k.values()) or any(complex(Ly['n']).imag > 0 for Ly in stack)
+        st = Stack(complex(wg_n, k.get('wg', 0.0)) if lossy else wg_n, wg_thickness_um,
+                   [(float(Ly['t_um']), complex(Ly['n'])) for Ly in stack], n_co,
+                   k_sub=k.get('co', 0.0) if lossy else 0.0, force_lossy=lossy)
+    return st, lossy, k
+
+
+def _node2d(F):
+    """(nx, ny-1) -> (nx, ny) onto the nodes (fdtd2d_core.py:1497-1500)."""
+    o = np.zeros((F.shape[0], F.shape[1] + 1), dtype=np.float32)
+    o[:, 1:-1] = 0.5 * (F[:, :-1] + F[:, 1:])
+    o[:, 0], o[:, -1] = F[:, 0], F[:, -1]
+    return o
+
+
+def run_beads_stitched(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
+                       wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt,
+                       vcsel_offset, source_type, window_w_um, slide_um, place_bead=True,
+                       t_aqueous_um=None, t_mucin_um=None, t_lipid_um=0.0, input_gap_um=0.0,
+                       length_um=None, bead_x_um=None, bead_y_um=None, wg_n=None, bead_n=None,
+                       n_aqueous=None, n_mucin=None, n_cornea=None, n_lipid=None,
+                       polarization='s', curved=False, boundary='cpml', cad=None,
+                       return_efull=False, stack=None):
+    """2D CW solve by domain decomposition along x (fdtd2d_core.py:1197-1583).
+
+    Windows of window_w_um slide by slide_um; each runs steps_win steps on the
+    engine.  Window 0 carries the VCSEL; window w > 0 is driven on its first
+    O = window - slide rows by the previous window's complex amplitude of the
+    driven component (TE Ez, TM Ey) with a cosine taper; the amplitude stays on
+    the device between windows.  Interior window ends get a CPML in an absorber
+    extension that is not assembled.  The assembled CW amplitude gives the CW
+    phase frames, the detector powers and (TM) <|E|^2> and the Ex amplitude.
+    Supported: boundary='cpml', no CAD, flat geometry."""
+    if str(boundary or 'cpml').lower() != 'cpml' or cad is not None or curved:
+        raise NotImplementedError(f'lens_sensor_b200.run_beads_stitched: boundary={boundary!r} '
+                                  f'cad={cad is not None} curved={curved}: only the CPML stitch runs on '
+                                  f'the B200 engine')
+    pol = 'p' if str(polarization).lower() in ('p', 'tm') else 's'
+    t_total = time.time()
+    t_aq_um = t_aqueous_um if t_aqueous_um is not None else T_AQ * 1e6
+    wg_n = wg_n if wg_n is not None else n_at(wg_mat, lambda_nm)
+    bead_n = bead_n if bead_n is not None else n_at(bead_mat, lambda_nm)
+    n_aq_l = n_aqueous if n_aqueous is not None else n_at('aqueous', lambda_nm)
+    n_mu_l = n_mucin if n_mucin is not None else n_at('mucin', lambda_nm)
+    n_co_l = n_cornea if n_cornea is not None else cornea_default(lambda_nm)
+    n_lip_l = n_lipid if n_lipid is not None else n_at('lipid', lambda_nm)
+    L = (length_um * 1e-6) if length_um is not None else L_DEMO
+    L_um = L * 1e6
+    T_WG = wg_thickness_um * 1e-6
+    LAM = lambda_nm * 1e-9
+    bx_um = bead_x_um if bead_x_um is not None else L_um / 2.0
+    label = f'WG-{wg_mat}_Bead-{bead_mat}_d{bead_d_um:g}_L{lambda_nm:g}' + ('' if place_bead else '_ref')
+    dx = dx_nm * 1e-9
+    dt = 0.5 * dx / (C0 * np.sqrt(2))
+    NPML = 10
+    src_ix = NPML + 2
+    vd = float(input_gap_um or 0.0)
+    air = air_path_um(vd, dx * 1e6)
+    x_facet_um = src_ix * dx * 1e6 + air
+    tear_m = TEAR_BUFFER
+    y0_m = -tear_m
+    H_total = T_WG + AIR_BUFFER + tear_m
+    Ny = int(round(H_total / dx))
+    Nx_win = int(round(window_w_um * 1e-6 / dx))
+    S = int(round(slide_um * 1e-6 / dx))
+    O = Nx_win - S
+    Nx_full = int(round(L / dx))
+    if O < 8:
+        O = max(O, 1)
+    f0 = C0 / LAM
+    omega = 2 * np.pi * f0
+    sigma_t = 4 / (2 * np.pi * f0)
+    transit = window_w_um * 1e-6 * N_G_FACTOR * wg_n / C0
+    steps_win = int(3.0 * transit / dt) + 400
+    steps_per_T = max(4, int(round((1.0 / f0) / dt)))
+    n_acc = steps_per_T * 8
+    n_win = (int(np.ceil((Nx_full - Nx_win) / S)) + 1) if Nx_full > Nx_win else 1
+    n_w0 = max(0, steps_win - n_acc)
+    acc_n = steps_win - n_w0
+    st, lossy, k = _stack_2d(wg_n, wg_thickness_um, t_lipid_um, n_lip_l, t_aq_um, n_aq_l, t_mucin_um, n_mu_l,
+                             n_co_l, stack)
+    bead = None
+    if place_bead and bead_d_um:
+        bead = Bead2D(bx_um, bead_d_um, complex(bead_n, k.get('bead', 0.0)) if lossy else bead_n, bead_y_um)
+
+    def gx0(w):                          # the last window ends flush with the domain
+        return min(w * S, max(Nx_full - Nx_win, 0))
+    EXT = NPML + 4
+    len_mat = L_um + EXT * dx * 1e6      # the core runs on into the absorber extension
+    iy_lo, iy_hi = int(round((0.0 + tear_m) / dx)), int(round((T_WG + tear_m) / dx))
+    ix_in, ix_out = int(round(0.1 * Nx_full)), int(round(0.9 * Nx_full))
+    ix_in = _guard_in_plane(ix_in, max(src_ix, int(round(x_facet_um / (dx * 1e6)))), Nx_full)
+    plan = []
+    for w in range(n_win):
+        g0, last = gx0(w), w == n_win - 1
+        glo = 0 if w == 0 else g0 + O
+        ghi = min(g0 + Nx_win, Nx_full)
+        fpl = {q: g - g0 for q, g in (('in', ix_in), ('out', ix_out)) if glo <= g < ghi and g - g0 >= 1}
+        if w == 0:
+            fpl.update(src_up=src_ix - 1, src_dn=src_ix + 3)
+        plan.append((g0, last, fpl))
+    if not all(any(q in p[2] for p in plan) for q in ('in', 'out')):
+        raise NotImplementedError('lens_sensor_b200.run_beads_stitched: a detector plane falls on a window '
+                                  'start (no overlap); the E-only flux estimate is not built')
+    Nyc = Ny - 1 if pol == 'p' else Ny
+    Efull = np.zeros((Nx_full, Nyc), dtype=np.complex64)
+    safe = ''.join(c if (c.isalnum() or c in '-_.') else '_' for c in label)
+    ExI_full = ExA_full = None
+    if pol == 'p':
+        os.makedirs('results', exist_ok=True)
+        tag = f'{os.getpid()}_{int(time.time() * 1000)}'
+        ExI_full = np.lib.format.open_memmap(os.path.join('results', f'_stream_beads_{safe}_stitch_Iavg_{tag}.npy'),
+                                             mode='w+', dtype=np.float32, shape=(Nx_full, Ny))
+        ExA_full = np.lib.format.open_memmap(os.path.join('results', f'_stream_beads_{safe}_stitch_ExA_{tag}.npy'),
+                                             mode='w+', dtype=np.complex64, shape=(Nx_full, Ny))
+    wtap = (0.5 * (1.0 + np.cos(np.pi * np.arange(O) / max(O - 1, 1)))).astype(np.float32)
+    # per-step FP64 drive values: the envelope and e^{i w t} as the reference forms them
+    tq = np.arange(steps_win) * dt
+    env_t = np.array([float(1 - np.exp(-((t / (2 * sigma_t)) ** 2))) for t in tq])
+    ph_t = np.exp(1j * omega * tq)
+    flux = FluxSum2D(E)
+    hand = None
+    geo0 = None
+    tab = None
+    sc = torch.tensor(2.0 / max(acc_n, 1), dtype=torch.float32)
+    for w, (g0, last, fpl) in enumerate(plan):
+        Nxw = Nx_win + (0 if last else EXT)
+        sp = Spec2D(pol, Nxw, Ny, dx, st, tear_m, bead, npml=NPML, lam_nm=lambda_nm, waist_um=vcsel_waist,
+                    length_m=len_mat * 1e-6, vcsel_distance_um=vd, vcsel_offset_um=vcsel_offset,
+                    vcsel_tilt_deg=vcsel_tilt, src_core_only=SRC_CORE_ONLY, x_start_um=g0 * dx * 1e6,
+                    npml_x=(NPML if w == 0 else 0, NPML))
+        geo = build_2d(sp)
+        if w == 0:
+            geo0 = geo
+            tab = E.StepTable(0, steps_win, dt, geo['src']['omega'], omega, E.cw_envelope(f0))
+        coef = {q: geo[q] for q in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if q in geo}
+        grid = E.Grid2D(pol, Nxw, Ny, dx, dt, coef, geo['cx'], geo['cy'], geo['src'] if w == 0 else None,
+                        pec=(1 if w == 0 else 0, 1, 1, 1))
+        ep = E.Epi2D(grid, dft=(n_w0, steps_win), dft_ex=(pol == 'p'), planes=fpl, dft_raw=(pol == 'p'),
+                     ex2=(pol == 'p'))
+        drive = (E.Drive2D(grid, hand, wtap, env_t, ph_t.real, ph_t.imag)
+                 if (w > 0 and hand is not None) else None)
+        grid.step(tab, 0, steps_win, ep, drive=drive)
+        a = ep.phasor('dft_raw' if pol == 'p' else 'dft', kind='stitch')
+        s_ = sc.to(a.device)
+        Ew_d = torch.complex(a.real.float() * s_, a.imag.float() * s_)
+        if not last:
+            off = gx0(w + 1) - g0
+            hand = Ew_d[off:off + O]
+        for q in fpl:
+            flux.add(q, ep.plane_dft(q), acc_n)
+        l_lo, g_lo = (0, 0) if w == 0 else (O, g0 + O)
+        g_hi = min(g0 + Nx_win, Nx_full)
+        l_hi = l_lo + (g_hi - g_lo)
+        if g_hi > g_lo:
+            Efull[g_lo:g_hi] = Ew_d[l_lo:l_hi].cpu().numpy()
+            if ExI_full is not None:
+                ExI_full[g_lo:g_hi] = ep.ex2[l_lo:l_hi, :Ny].cpu().numpy() / max(acc_n, 1)
+                xa = ep.phasor('dft_ex', kind='stitch')[l_lo:l_hi]
+                ExA_full[g_lo:g_hi] = torch.complex(xa.real.float() * s_, xa.imag.float() * s_).cpu().numpy()
+        del grid, ep, drive
+    total_time = time.time() - t_total
+    frames, mm_path = [], None
+    nfr = max(1, n_snapshots)
+    if save_frames:
+        os.makedirs('results', exist_ok=True)
+        mm_path = os.path.join('results', f'_stream_beads_{safe}_stitch.npy')
+        ez_mm = np.lib.format.open_memmap(mm_path, mode='w+', dtype=np.float32, shape=(nfr, Nx_full, Ny))
+        for q in range(nfr):
+            tk = (q / nfr) * (1.0 / f0)
+            fr = np.real(Efull * np.exp(1j * omega * tk)).astype(np.float32)
+            ez_mm[q] = _node2d(fr) if pol == 'p' else fr
+            frames.append({'x_start': 0.0, 'x_end': L_um, 'y_start': y0_m * 1e6,
+                           'y_end': (y0_m + H_total) * 1e6, 'slide_i': 0, 'step': q, 'time': tk})
+        ez_mm.flush()
+        del ez_mm
+    # detector powers from the assembled amplitude (fdtd2d_core.py:1506-1519)
+    P_in = float(np.sum(np.abs(Efull[ix_in, iy_lo:iy_hi]) ** 2))
+    P_out = float(np.sum(np.abs(Efull[ix_out, iy_lo:iy_hi]) ** 2))
+    if ExI_full is not None:
+        P_in += 2.0 * float(np.sum(ExI_full[ix_in, iy_lo:iy_hi]))
+        P_out += 2.0 * float(np.sum(ExI_full[ix_out, iy_lo:iy_hi]))
+        for x0 in range(0, Nx_full, 4096):
+            x1 = min(x0 + 4096, Nx_full)
+            s2 = 0.5 * np.abs(Efull[x0:x1]) ** 2
+            ey2 = np.empty((x1 - x0, Ny), dtype=np.float32)
+            ey2[:, 1:-1] = 0.5 * (s2[:, :-1] + s2[:, 1:])
+            ey2[:, 0], ey2[:, -1] = s2[:, 0], s2[:, -1]
+            ExI_full[x0:x1] += ey2
+        ExI_full.flush()
+    Tr_I = P_out / max(P_in, 1e-30)
+    S_in, S_out = flux.flux('in'), flux.flux('out')
+    p_si = S_in * dx
+    Tr = S_out / S_in if abs(S_in) > 0 else Tr_I
+    res = _result_dict(label, P_in, P_out, Tr, frames, total_time, bead_d_um, wg_mat, bead_mat, wg_n, bead_n,
+                       wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt, vcsel_offset, source_type, 'stitch',
+                       place_bead, n_aq_l, n_mu_l, n_co_l, mm_path, t_aq_um, t_mucin_um, t_lipid_um, bx_um,
+                       x_facet_um, L_um, pol, stack, n_lip_l)
+    res['transmission_intensity'] = Tr_I
+    res['transmission_def'] = 'poynting'
+    res['view_primary'] = 'cw'
+    res['cw_only'] = True
+    res['p_in_si'] = p_si
+    res['p_in_unit'] = 'W/m'
+    ok = flux.has('src_up') and flux.has('src_dn')
+    p_emit = (flux.flux('src_dn') - flux.flux('src_up')) * dx if ok else None
+    p_refl = -flux.flux('src_up') * dx if ok else None
+    res.update(laser_power_mw=LASER_POWER_MW, vcsel_distance_um=vd, vcsel_air_um=float(geo0['src']['air_um']),
+               vcsel_waist_um=float(vcsel_waist), x_facet_um=float(x_facet_um), p_src_si=p_emit)
+    if p_emit and p_emit > 0:
+        res['coupling_efficiency'] = (p_si / p_emit) if p_si is not None else float('nan')
+        res['facet_reflection'] = (p_refl / p_emit) if p_refl is not None else float('nan')
+    if ExI_full is not None:
+        res['Iavg'] = ExI_full
+    if ExA_full is not None:
+        ExA_full.flush()
+        res['Ex_cw_amp'] = ExA_full
+    if return_efull:
+        res['Efull'] = Efull
+    return res
+
+
+class FluxSum2D:
+    """Plane DFTs summed over the windows that carry the plane (one running
+    PlaneFluxDFT across windows, fdtd2d_core.py:1395, 1466-1469)."""
+
+    def __init__(self, engine):
+        self.E = engine
+        self.acc, self.n = {}, {}
+
+    def add(self, key, pairs, n):
+        if key not in self.acc:
+            self.acc[key] = [[sg, aE.clone(), aH.clone()] for sg, aE, aH in pairs]
+            self.n[key] = 0
+        else:
+            for a, (sg, aE, aH) in zip(self.acc[key], pairs):
+                a[1] += aE
+                a[2] += aH
+        self.n[key] += int(n)
+
+    def has(self, key):
+        return self.n.get(key, 0) > 0
+
+    def flux(self, key):
+        if not self.has(key):
+            return float('nan')
+        return self.E.plane_flux(self.acc[key], self.n[key])
+
+
 def _field_2d(g):
     """Ez (TE) or Ey averaged onto the nodes (TM), fdtd2d_core.py:458-465."""
     if g.pol == 's':
@@ -275,7 +553,7 @@ def save_results(result, out_dir='results'):
     if not frames:
         return None
     n_fr = len(frames)
-    ez = np.load(result['frames_memmap'], mmap_mode='r')[:n_fr]
+    ez = np.array(np.load(result['frames_memmap'], mmap_mode='r')[:n_fr])
     sx = next((s for s in (1, 2, 3, 4, 6, 8, 12, 16, 32) if ez.shape[1] // s <= 5000), 32)
     sy = next((s for s in (1, 2, 4, 8) if ez.shape[2] // s <= 2000), 8)
     meta = np.array([(fr['x_start'], fr['x_end'], fr['y_start'], fr['y_end'], fr['slide_i'], fr['time'],
@@ -312,11 +590,14 @@ def save_results(result, out_dir='results'):
     cw_frames = result.get('cw_frames') or []
     cw_path = result.get('cw_frames_memmap')
     if cw_path and os.path.exists(cw_path) and cw_frames:
-        kw['Ez_cw'] = np.ascontiguousarray(np.load(cw_path, mmap_mode='r')[:len(cw_frames), ::sx, ::sy])
+        kw['Ez_cw'] = np.array(np.load(cw_path, mmap_mode='r')[:len(cw_frames), ::sx, ::sy])
         kw['meta_cw'] = np.array([(fr['x_start'], fr['x_end'], fr['y_start'], fr['y_end'], fr['slide_i'],
                                    fr['time'], fr.get('step', 0)) for fr in cw_frames], dtype=np.float64)
-    kw.update(has_transient=np.array([1]), has_cw=np.array([1 if 'Ez_cw' in kw else 0]),
-              cw_only=np.array([0]), view_primary=np.array([str(result.get('view_primary', 'transient'))]))
+    cw_only = bool(result.get('cw_only', False)) or result.get('method') == 'stitch'
+    kw.update(has_transient=np.array([0 if cw_only else 1]),
+              has_cw=np.array([1 if (cw_only or 'Ez_cw' in kw) else 0]),
+              cw_only=np.array([1 if cw_only else 0]),
+              view_primary=np.array([str(result.get('view_primary', 'transient'))]))
     if result.get('Iavg') is not None:
         kw['Iavg'] = np.asarray(result['Iavg'])[::sx, ::sy].astype(np.float32)
         kw['iavg_full'] = np.array([1])
@@ -332,4 +613,8 @@ def save_results(result, out_dir='results'):
             kw[q] = np.array([float(v)])
     npz = f'{out_dir}/beads_{tag}_frames.npz'
     np.savez_compressed(npz, **kw)
+    # the temporary frame stream files go once the NPZ is written (fdtd2d_core.py:2243-2265)
+    for path in (cw_path, result.get('frames_memmap')):
+        if path and os.path.exists(path):
+            os.remove(path)
     return npz

@@ -250,6 +250,10 @@ class Spec2D:
     vcsel_offset_um: float = 0.0
     vcsel_tilt_deg: float = 0.0
     src_core_only: bool = False
+    # stitch window (fdtd2d_core.py:1396-1412): x of node 0 in the whole domain (um)
+    # and the CPML cells at the x-lo / x-hi ends (default npml at both)
+    x_start_um: Optional[float] = None
+    npml_x: Optional[Tuple[int, int]] = None
 
     @property
     def dt(self):
@@ -275,7 +279,8 @@ def build_2d(sp: Spec2D):
     ys = -sp.tear_m + np.arange(Ny) * dx
     col = column_average(ys, dx, st.eps_of_y(1.0, core=False))
     col_core = column_average(ys, dx, st.eps_of_y(1.0, core=True))
-    xs = np.arange(Nx) * dx
+    x0 = sp.x_start_um * 1e-6 if sp.x_start_um is not None else 0.0
+    xs = x0 + np.arange(Nx) * dx
     in_wg = (xs >= x_facet_um * 1e-6) & (xs <= (sp.length_m if sp.length_m is not None else Nx * dx * 1e6 * 1e-6))
     eps = np.empty((Nx, Ny), dtype=np.complex128 if lossy else F32)
     eps[:, :] = col[None, :]
@@ -287,7 +292,7 @@ def build_2d(sp: Spec2D):
         xc = sp.bead.x_um * 1e-6
         yc = sp.bead.y_um * 1e-6 if sp.bead.y_um is not None else -r
         if not (xc + r < xs[0] or xc - r > xs[-1]):
-            i0, i1 = max(0, int((xc - r) / dx) - 2), min(Nx, int((xc + r) / dx) + 2)
+            i0, i1 = max(0, int((xc - r - x0) / dx) - 2), min(Nx, int((xc + r - x0) / dx) + 2)
             j0, j1 = max(0, int((yc - r - ys[0]) / dx) - 2), min(Ny, int((yc + r - ys[0]) / dx) + 3)
             if i1 > i0 and j1 > j0:
                 bead_patch = dict(bg=eps[i0:i1, j0:j1].real.astype(np.float64), i0=i0, j0=j0,
@@ -323,7 +328,8 @@ def build_2d(sp: Spec2D):
         a, p1, p2 = h * (a[:-1] + a[1:]), h * (p1[:-1] + p1[1:]), h * (p2[:-1] + p2[1:])
     out['src'] = dict(ix=sp.src_ix, amp=a, ph1=p1, ph2=p2, omega=2 * np.pi * sp.f0, air_um=air,
                       iy_src=int(round((yc_src + sp.tear_m) / dx)))
-    out['cx'] = cpml_axis(Nx, sp.npml, sp.npml, dx, dt, lam_m)
+    nlo, nhi = sp.npml_x if sp.npml_x is not None else (sp.npml, sp.npml)
+    out['cx'] = cpml_axis(Nx, nlo, nhi, dx, dt, lam_m)
     out['cy'] = cpml_axis(Ny, sp.npml, sp.npml, dx, dt, lam_m)
     return out
 

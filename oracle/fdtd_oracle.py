@@ -393,7 +393,9 @@ class Grid2D:
         Q = {k: up(v) for k, v in cy.items()}
         self.P, self.Q = P, Q
 
-    def step(self, n, env):
+    def step(self, n, env, before_pec=None):
+        """One leapfrog step; before_pec(field) runs after the source and before the
+        PEC termination (the stitch drive, fdtd2d_core.py:1439-1441, 1462-1464)."""
         t = n * self.dt
         P, Q, ch = self.P, self.Q, self.ch
         if self.pol == 's':
@@ -412,6 +414,8 @@ class Grid2D:
                               + self.ce_h[1:-1, 1:-1] * (dhy / P['ke'][1:-1, None] + self.p_ezx
                                                          - dhx / Q['ke'][None, 1:-1] - self.p_ezy))
             self.src.inject(Ez, t, env, self.fp64)
+            if before_pec is not None:
+                before_pec(Ez)
             xl, xh, yl, yh = self.pec
             if xl: Ez[0, :] = 0.0
             if xh: Ez[-1, :] = 0.0
@@ -434,6 +438,8 @@ class Grid2D:
             self.p_eyx = P['be'][1:-1, None] * self.p_eyx + P['ce'][1:-1, None] * d
             Ey[1:-1, :] += -self.ca_y[1:-1, :] * (d / P['ke'][1:-1, None] + self.p_eyx)
             self.src.inject(Ey, t, env, self.fp64)
+            if before_pec is not None:
+                before_pec(Ey)
             xl, xh, yl, yh = self.pec
             if xl: Ey[0, :] = 0.0
             if xh: Ey[-1, :] = 0.0
@@ -474,6 +480,16 @@ class Grid2D:
         if self.pol == 's':
             return ((-1.0, self.Ez[il], self.Hy[il - 1], self.Hy[il]),)
         return ((+1.0, self.Ey[il], self.Hz[il - 1], self.Hz[il]),)
+
+
+def tm_ex2_node(Ex):
+    """_tm_ex2_node (fdtd2d_core.py:477-486): Ex^2 squared-averaged onto the nodes."""
+    s = Ex * Ex
+    out = np.zeros((Ex.shape[0] + 1, Ex.shape[1]), dtype=np.float32)
+    out[1:-1, :] = 0.5 * (s[:-1, :] + s[1:, :])
+    out[0, :] = s[0, :]
+    out[-1, :] = s[-1, :]
+    return out
 
 
 class PlaneFlux:

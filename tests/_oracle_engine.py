@@ -30,24 +30,45 @@ class Grid2D:
     def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None):
         self.pol = 'p' if str(pol).lower() in ('p', 'tm') else 's'
         self.nx, self.ny, self.dx, self.dt = nx, ny, dx, dt
-        h = O.Huygens.__new__(O.Huygens)
-        h.ix, h.omega = int(src['ix']), float(src['omega'])
-        h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
+        if src is None:
+            h = _NoSource()
+        else:
+            h = O.Huygens.__new__(O.Huygens)
+            h.ix, h.omega = int(src['ix']), float(src['omega'])
+            h.amp, h.ph1, h.ph2 = (np.asarray(src[k], F32) for k in ('amp', 'ph1', 'ph2'))
         self.g = O.Grid2D(self.pol, nx, ny, dx, dt, cx, cy, h, coef, F32, pec)
 
     def view(self, name):
         return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
 
-    def step(self, table, n0, nsteps, epi=None, stream=None):
+    def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
+        if self.g.src.omega is None:
+            self.g.src.omega = table.omega
         for n in range(n0, n0 + nsteps):
             t = n * self.dt
-            self.g.step(n, float(table.envelope(t)))
+            env = float(table.envelope(t))
+            hook = (lambda F, t=t, env=env: drive.apply(F, table.omega, t, env)) if drive is not None else None
+            self.g.step(n, env, before_pec=hook)
             if epi is not None:
                 epi.after(n, t, self.g)
 
 
+class Drive2D:
+    """2D overlap drive exactly as fdtd2d_core.py:1439-1440 / 1462-1463 writes it."""
+
+    def __init__(self, grid, hand, taper, env=None, cos_wt=None, sin_wt=None):
+        self.D = np.asarray(torch.as_tensor(hand).numpy(), np.complex64)
+        self.O = self.D.shape[0]
+        self.w = np.asarray(taper, F32)[:, None]
+
+    def apply(self, F, omega, t, env):
+        din = env * np.real(self.D * np.exp(1j * omega * t))
+        F[:self.O, :] = self.w * din + (1.0 - self.w) * F[:self.O, :]
+
+
 class Epi2D:
-    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=()):
+    def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=(),
+                 dft_raw=False, ex2=False):
         nx, ny = grid.nx, grid.ny
         self.grid = grid
         self.boxes = [tuple(b) for b in boxes]
@@ -61,6 +82,12 @@ class Epi2D:
         self.planes = dict(planes)
         self.flux_acc = None
         self._omega = None
+        # run_beads_stitched's own complex64 sums (fdtd2d_core.py:1441-1446, 1471):
+        # TE Ez / TM Ey on its grid, TM Ex on the nodes, TM <Ex^2> on the nodes
+        self.acc_st = np.zeros((nx, ny) if grid.pol == 's' else (nx, ny - 1), np.complex64)
+        self.acc_exa = np.zeros((nx, ny), np.complex64)
+        self.acc_ex2 = np.zeros((nx, ny), F32)
+        self.ex2 = torch.from_numpy(self.acc_ex2) if ex2 else None
 
     def after(self, n, t, g):
         if self.flux_acc is None:
@@ -75,6 +102,13 @@ class Epi2D:
             self.acc += field.astype(np.complex64) * ph
             if self.acc_ex is not None:
                 self.acc_ex += g.ex_node().astype(np.complex64) * ph
+            p64 = np.complex64(ph)
+            if g.pol == 's':
+                self.acc_st += g.Ez.astype(np.complex64) * p64
+            else:
+                self.acc_st += g.Ey.astype(np.complex64) * p64
+                self.acc_ex2 += O.tm_ex2_node(g.Ex)
+                self.acc_exa += g.ex_node().astype(np.complex64) * p64
             for k, il in self.planes.items():
                 self.flux_acc.add(k, t, g.flux_pairs(il))
         elif self.win_prev[0] <= n < self.win_prev[1]:
@@ -90,9 +124,16 @@ class Epi2D:
     def iavg(self):
         return torch.from_numpy(self.acc_I.copy())
 
-    def phasor(self, which='dft'):
-        a = dict(dft=self.acc, prev=self.acc_prev, dft_ex=self.acc_ex)[which]
+    def phasor(self, which='dft', kind=None):
+        if kind == 'stitch':
+            a = self.acc_exa if which == 'dft_ex' else self.acc_st
+        else:
+            a = dict(dft=self.acc, prev=self.acc_prev, dft_ex=self.acc_ex)[which]
         return torch.from_numpy(a.astype(np.complex128))
+
+    def plane_dft(self, name):
+        return [(sg, torch.from_numpy(aE.astype(np.complex128)), torch.from_numpy(aH.astype(np.complex128)))
+                for sg, aE, aH in self.flux_acc.acc[name]]
 
     def restart_dft(self, window):
         self.acc_prev, self.acc = self.acc, np.zeros_like(self.acc)

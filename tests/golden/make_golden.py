@@ -19,10 +19,12 @@ Outputs:
                                        summaries) of three whole-driver cases
   dropin_3d.json                       the same for run_3d + save_results_3d
   dropin_3d_stitch.json                the same for run_3d_stitched + save_results_3d
+  dropin_2d_stitch.json                the same for run_beads(method='stitch') + save_results
 
 `python tests/golden/make_golden.py dropin` stops after the two JSON files;
-`python tests/golden/make_golden.py stitch` writes only the stitch fixtures
-(adds case_3d_stitch to characterization.json, writes dropin_3d_stitch.json).
+`python tests/golden/make_golden.py stitch` writes only the 3D stitch fixtures
+(adds case_3d_stitch to characterization.json, writes dropin_3d_stitch.json);
+`python tests/golden/make_golden.py stitch2d` writes dropin_2d_stitch.json.
 """
 import json
 import os
@@ -459,7 +461,70 @@ def dropin_3d_stitch():
     return out
 
 
+# ------------------------------------------------------ drop-in run_beads_stitched
+# Whole-driver cases: fdtd2d_core.run_beads(method='stitch') + save_results.  'te' runs 3
+# windows on the characterization stack (the last one flush with the domain end); 'tm'
+# 4 windows on an absorbing custom stack with KAPPA on the core, an input gap, a tilted
+# offset source and a bead across a seam (TM: Ey handoff, <Ex^2> and Ex amplitude).
+DROPIN_2D_STITCH = dict(
+    te=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.5, dx_nm=100.0, save_frames=True,
+                    n_snapshots=2, wg_thickness_um=1.0, lambda_nm=850.0, method='stitch', length_um=12.0,
+                    bead_x_um=5.0, window_w_um=5.0, slide_um=3.5), kappa={}),
+    tm=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.6, dx_nm=100.0, save_frames=True,
+                    n_snapshots=3, wg_thickness_um=1.2, lambda_nm=850.0, method='stitch', length_um=14.0,
+                    bead_x_um=6.3, window_w_um=5.0, slide_um=3.2, polarization='p', input_gap_um=1.5,
+                    vcsel_tilt=2.0, vcsel_offset=0.1, vcsel_waist=1.2,
+                    stack=[dict(name='Aqueous', t_um=2.0, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                           dict(name='Mucin', t_um=0.5, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+            kappa=dict(wg=0.0005)),
+)
+
+
+def dropin_2d_stitch():
+    """Run the reference 2D stitch end to end for DROPIN_2D_STITCH and summarise its outputs."""
+    import glob
+    import pickle
+    import re
+    out = {}
+    for name, c in DROPIN_2D_STITCH.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_stitch2d_')
+        old_k = d2.KAPPA
+        try:
+            os.chdir(tmp)
+            d2.KAPPA = dict(c['kappa'])
+            r = d2.run_beads(**c['kw'])
+            res = dict(transmission=float(r['transmission']), P_in=float(r['P_in']), P_out=float(r['P_out']),
+                       transmission_intensity=float(r['transmission_intensity']))
+            arrays = {}
+            for key in ('Iavg', 'Ex_cw_amp'):
+                if r.get(key) is not None:
+                    arrays[key] = _summ(np.asarray(r[key]))
+            d2.save_results(r)
+            z = np.load(glob.glob('results/*_frames.npz')[0])
+            npz = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+            left = sorted(re.sub(r'_\d+_\d+\.npy$', '_{tag}.npy', f) for f in os.listdir('results'))
+        finally:
+            d2.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        out[name] = dict(kw={k: v for k, v in c['kw'].items() if k != 'stack'}, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         result=res, arrays=arrays, npz=npz, pkl=scal, files_left=left)
+    return out
+
+
 def main():
+    if 'stitch2d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_2d_stitch.json'), 'w') as f:
+            json.dump(dropin_2d_stitch(), f, indent=1)
+        print('wrote dropin_2d_stitch.json')
+        return
     if 'stitch' in sys.argv[1:]:
         path = os.path.join(OUT, 'characterization.json')
         ch = json.load(open(path))

@@ -64,6 +64,8 @@ def test_invalid_arguments_are_rejected_without_launch(lib):
     assert lib.lens_batch2d_plan(inst, 2, 8, blk, None) == -1    # empty descriptors
     assert lib.lens_batch2d_step(inst, None, None, None, 2, 0, 8, None, 0, 1, None) == -1
     assert lib.lens_fdtd3d_accum_e2(ctypes.byref(g), 1, 0, None, None) == -1
+    assert lib.lens_te2d_step_driven(None, None, None, None, 0, 1, None) == -1
+    assert lib.lens_tm2d_step_driven(None, None, None, None, 0, 1, None) == -1
     d = N.Drive3D()
     assert lib.lens_fdtd3d_step_driven(ctypes.byref(g), None, None, None, 0, 1, None) == -1
     assert lib.lens_fdtd3d_step_driven(ctypes.byref(g), None, None, ctypes.byref(d), 0, 1, None) == -1

@@ -48,6 +48,8 @@ def _run(name, engine, tmp_path, monkeypatch):
     if engine is not None:
         monkeypatch.setattr(D2, 'E', engine)
     r = D2.run_beads(**_kwargs(case))
+    # the frame stream file is removed by save_results (as the reference does): keep its frames
+    r['_frames_before_save'] = np.array(np.load(r['frames_memmap'], mmap_mode='r')[:len(r['frames'])])
     npz = D2.save_results(r)
     with open(glob.glob('results/*.pkl')[0], 'rb') as f:
         pk = pickle.load(f)
@@ -99,7 +101,7 @@ def test_characterization_known_answer(tmp_path, monkeypatch):
     r, z, pk = _run('te', _oracle_engine, tmp_path, monkeypatch)
     for k in ('transmission', 'P_in', 'P_out'):
         np.testing.assert_allclose(r[k], ch[k], rtol=1e-6)
-    ez = np.asarray(np.load(r['frames_memmap'], mmap_mode='r')[:len(r['frames'])], np.float64)
+    ez = np.asarray(r['_frames_before_save'], np.float64)
     assert list(ez.shape) == ch['frames']['shape']
     np.testing.assert_allclose([ez.sum(), np.abs(ez).max(), ez.mean()],
                                [ch['frames']['sum'], ch['frames']['absmax'], ch['frames']['mean']], rtol=1e-6)

@@ -126,6 +126,12 @@ typedef struct {
                                     layout as dft, during the dft window, or NULL */
     float *ex2;                  /* TM: Ex^2 on the nodes summed during the dft
                                     window (nx, pitch), or NULL                */
+    int nsx;                     /* time-domain Poynting planes (every step)   */
+    int sx_plane[LENS_MAX_PLANE];/* x-planes il (1 <= il <= nx-2)              */
+    double *sx_acc;              /* per plane: pitch doubles, acc[j] += the
+                                    FP32 product E(il,j) * (H(il-1,j) + H(il,j))/2
+                                    (TE Ez*Hy, TM Ey*Hz; the TE flux is minus the
+                                    sum, fdtd2d_core.py:489-497)              */
 } LensEpi2D;
 
 /* Advance `nsteps` steps starting at step n0 (t = n*dt, n = n0 ... n0+nsteps-1). */

@@ -59,7 +59,8 @@ class Epi2D(ctypes.Structure):
                 ('prev_n0', c_int), ('prev_n1', c_int), ('dft_prev', c_void_p),
                 ('iavg_n0', c_int), ('iavg', c_void_p),
                 ('nplane', c_int), ('plane', c_int * MAX_PLANE), ('plane_acc', c_void_p),
-                ('dft_raw', c_void_p), ('ex2', c_void_p)]
+                ('dft_raw', c_void_p), ('ex2', c_void_p),
+                ('nsx', c_int), ('sx_plane', c_int * MAX_PLANE), ('sx_acc', c_void_p)]
 
 
 NPSI = 12

@@ -72,6 +72,13 @@ __device__ __forceinline__ void plane_node(const LensEpi2D &ep, const LensStepTa
     a[3 * pitch] += (double)h * hi;
 }
 
+// Time-domain Poynting term of one plane cell (fdtd2d_core.py:489-497): the
+// FP32 product of E and H averaged onto the E plane, summed in FP64.
+__device__ __forceinline__ void sx_node(const LensEpi2D &ep, int p, int pitch, int j, float e, float h0, float h1) {
+    const float h = __fmul_rn(0.5f, __fadd_rn(h0, h1));
+    ep.sx_acc[(size_t)p * pitch + j] += (double)__fmul_rn(e, h);
+}
+
 __device__ __forceinline__ bool in_window(const LensEpi2D &ep, int n) {
     return n >= ep.dft_n0 && n < ep.dft_n1;
 }
@@ -161,6 +168,8 @@ __global__ void __launch_bounds__(BX *BY)
                 if (i == ep.plane[p])
                     plane_node(ep, tab, n, p, P, j, ez, 0.5f * (g.hy[o - P] + g.hy[o]));
         }
+        for (int p = 0; p < ep.nsx; ++p)
+            if (i == ep.sx_plane[p]) sx_node(ep, p, P, j, ez, g.hy[o - P], g.hy[o]);
     }
     epilogue_node(ep, tab, n, i, j, valid, o, ez, ez * ez, 0.f);
 }
@@ -276,13 +285,16 @@ __global__ void __launch_bounds__(BX *BY)
                 if (i == ep.plane[p])
                     plane_node(ep, tab, n, p, P, j, g.ey[o], 0.5f * (g.hz[o - P] + g.hz[o]));
         }
+        if (j < ny - 1)
+            for (int p = 0; p < ep.nsx; ++p)
+                if (i == ep.sx_plane[p]) sx_node(ep, p, P, j, g.ey[o], g.hz[o - P], g.hz[o]);
     }
     epilogue_node(ep, tab, n, i, j, valid, o, field, inten, exn);
 }
 
 bool epi2d_active(const LensEpi2D *ep, int n) {
     if (!ep) return false;
-    if (ep->nbox > 0) return true;
+    if (ep->nbox > 0 || ep->nsx > 0) return true;
     if ((ep->dft || ep->dft_ex || ep->dft_raw || ep->ex2 || ep->nplane > 0) && n >= ep->dft_n0 && n < ep->dft_n1)
         return true;
     if (ep->dft_prev && n >= ep->prev_n0 && n < ep->prev_n1) return true;
@@ -296,6 +308,9 @@ bool epi2d_ok(const LensEpi2D *ep, const LensStepTable *t, int nx) {
         return false;
     for (int p = 0; p < ep->nplane; ++p)  // H is averaged over rows il-1 and il
         if (ep->plane[p] < 1 || ep->plane[p] > nx - 2) return false;
+    if (ep->nsx < 0 || ep->nsx > LENS_MAX_PLANE || (ep->nsx > 0 && !ep->sx_acc)) return false;
+    for (int p = 0; p < ep->nsx; ++p)
+        if (ep->sx_plane[p] < 1 || ep->sx_plane[p] > nx - 2) return false;
     const bool dft = ep->dft || ep->dft_ex || ep->dft_prev || ep->dft_raw || ep->nplane > 0;
     return !dft || (t->pe && t->ph);
 }

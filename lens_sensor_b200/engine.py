@@ -63,9 +63,12 @@ def strip_widths(c):
 
 
 class _Axis:
-    """Device copy of one CPML axis (b, c, 1/kappa on integer and half nodes)."""
+    """Device copy of one CPML axis (b, c, 1/kappa on integer and half nodes).
+    full: psi over the whole axis (every node a strip node: b = 1, c = 0 keeps
+    psi constant outside the absorber, as the reference's full-domain psi
+    arrays do, boundaries.py:172-175)."""
 
-    def __init__(self, prof, n, dev):
+    def __init__(self, prof, n, dev, full=False):
         self.keep = []
         self.ax = N.Axis()
         for tag, length in (('e', n), ('h', n - 1)):
@@ -75,7 +78,7 @@ class _Axis:
             assert len(b) == length, (tag, len(b), length)
             tb, tc, ti = (torch.from_numpy(v.copy()).to(dev) for v in (b, c, ik))
             self.keep += [tb, tc, ti]
-            lo, hi = strip_widths(c)
+            lo, hi = (length, 0) if full else strip_widths(c)
             setattr(self.ax, tag, N.Profile(_ptr(tb), _ptr(tc), _ptr(ti), length, lo, hi))
 
     def w(self, tag):
@@ -127,9 +130,11 @@ class Grid2D:
     coef: TE {'ce_e','ce_h'} (nx,ny); TM {'ca_x' (nx-1,ny), 'ca_y' (nx,ny-1),
     optional 'da_x','da_y'} - the arrays of fdtd2d_core._coeffs / _tm_coeffs /
     _tm_loss.  cx, cy: CPML profiles {'ke','be','ce','kh','bh','ch'} along x and y.
-    src: dict(ix, amp, ph1, ph2) of the Huygens pair (TM: on the Ey grid)."""
+    src: dict(ix, amp, ph1, ph2) of the Huygens pair (TM: on the Ey grid).
+    full_x: x psi over every row (the co-moving window, whose rolled psi keeps
+    its values outside the absorber)."""
 
-    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None):
+    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None, full_x=False):
         self.lib = N.load()
         dev = self.dev = _device(device)
         self.pol = 'p' if str(pol).lower() in ('p', 'tm') else 's'
@@ -138,7 +143,7 @@ class Grid2D:
         shp = (nx, P)
         z = lambda *s: torch.zeros(s if s else shp, dtype=torch.float32, device=dev)
         self.ch = F32(dt / (MU0 * dx))
-        self.axx, self.axy = _Axis(cx, nx, dev), _Axis(cy, ny, dev)
+        self.axx, self.axy = _Axis(cx, nx, dev, full=full_x), _Axis(cy, ny, dev)
         wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
         if src is None:                # no source (a stitch window driven by its predecessor)
             self.src_t = {}
@@ -182,6 +187,21 @@ class Grid2D:
         a, b = shapes[name]
         return getattr(self, name)[:a, :b]
 
+    def state(self):
+        """The fields and psi arrays, each with its rows along x."""
+        names = ('ez', 'hx', 'hy') if self.pol == 's' else ('ex', 'ey', 'hz')
+        return [getattr(self, q) for q in names] + list(self.psi.values())
+
+    def take_shifted(self, other, n):
+        """Fields and psi of `other` (same sizes and strips) moved n rows towards
+        x = 0, the last n rows zero: the co-moving window's roll
+        (fdtd2d_core.py:1093-1102, boundaries.py:217-221)."""
+        for a, b in zip(self.state(), other.state()):
+            assert a.shape == b.shape, (a.shape, b.shape)
+            a.zero_()
+            if 0 < n < a.shape[0]:
+                a[:a.shape[0] - n].copy_(b[n:])
+
     def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
         e = ctypes.byref(epi.s) if epi is not None else None
         if drive is None:
@@ -221,9 +241,14 @@ class Epi2D:
     """Epilogue buffers of a 2D solve (detector boxes, DFTs, Iavg, flux planes)."""
 
     def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=(),
-                 dft_raw=False, ex2=False):
+                 dft_raw=False, ex2=False, sx_planes=(), box_split=False):
         """dft_raw / ex2 (TM): the DFT of Ey on its own grid and the sum of Ex^2 on
-        the nodes over the dft window (run_beads_stitched, fdtd2d_core.py:1441-1446)."""
+        the nodes over the dft window (run_beads_stitched, fdtd2d_core.py:1441-1446).
+        sx_planes: {name: il} planes whose time-domain Poynting flux is summed
+        over every step (the pulse energies of run_beads_sliding,
+        fdtd2d_core.py:1139-1158).  box_split names the reference's separate
+        FP64 sums of field^2 and <Ex^2> in a TM box (fdtd2d_core.py:1148-1150);
+        the device sums their FP32 sum per cell in FP64 either way."""
         dev, nx, P = grid.dev, grid.nx, grid.pitch
         self.grid = grid
         self.boxes = [tuple(int(v) for v in b) for b in boxes]
@@ -253,7 +278,21 @@ class Epi2D:
             s.plane[q] = int(il)
         s.plane_acc = _ptr(self.plane_acc)
         s.dft_raw, s.ex2 = _ptr(self.dft_raw), _ptr(self.ex2)
+        self.sx_planes = dict(sx_planes)
+        self.sx_acc = torch.zeros((max(1, len(self.sx_planes)), P), dtype=torch.float64, device=dev)
+        s.nsx = len(self.sx_planes)
+        for q, il in enumerate(self.sx_planes.values()):
+            s.sx_plane[q] = int(il)
+        s.sx_acc = _ptr(self.sx_acc)
         self.s = s
+
+    def sx(self, name):
+        """Sum over the steps run of the instantaneous +x flux through plane
+        `name`: TE -sum Ez Hy, TM sum Ey Hz, H averaged onto the plane
+        (_sx_plane_2d, fdtd2d_core.py:489-497)."""
+        q = list(self.sx_planes).index(name)
+        tot = float(torch.sum(self.sx_acc[q]))
+        return -tot if self.grid.pol == 's' else tot
 
     def phasor(self, which='dft', kind=None):
         """Accumulated sum(F e^{-i w t}) on the nodes (nx, ny) ('dft_raw': on the

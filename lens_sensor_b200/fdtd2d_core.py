@@ -36,6 +36,19 @@ CW_MAX_EXTEND = 2.0
 N_LIPID = 1.480
 
 
+def _set_tear(stack, tear_buffer_um, dx_nm, cad=None):
+    """The reference's run_beads preamble (fdtd2d_core.py:547-560): a custom stack
+    deepens the domain below the core when the fixed buffer is too shallow; an
+    explicit tear_buffer_um sets it.  The caller restores TEAR_BUFFER."""
+    global TEAR_BUFFER
+    if stack is not None and tear_buffer_um is None and cad is None:
+        need = sum(float(Ly['t_um']) for Ly in stack) + 1.5 + 10 * dx_nm * 1e-3
+        if need * 1e-6 > TEAR_BUFFER + 1e-12:
+            tear_buffer_um = need
+    if tear_buffer_um is not None:
+        TEAR_BUFFER = float(tear_buffer_um) * 1e-6
+
+
 def _guard_in_plane(i_in, src_ix, n_max, margin=5):
     lo = int(src_ix) + int(margin)
     return int(i_in) if i_in >= lo else min(lo, int(n_max) - 2)
@@ -85,6 +98,20 @@ def run_beads(wg_mat, bead_mat, bead_d_um, dx_nm=20.0, save_frames=True, n_snaps
                                       boundary=boundary, cad=cad, stack=stack)
         finally:
             TEAR_BUFFER = old
+    if method == 'sliding':
+        global_old = TEAR_BUFFER
+        try:
+            _set_tear(stack, tear_buffer_um, dx_nm, cad)
+            return run_beads_sliding(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
+                                     wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt, vcsel_offset,
+                                     source_type, window_w_um, slide_um, place_bead, t_aqueous_um,
+                                     t_mucin_um=t_mucin_um, t_lipid_um=t_lipid_um, input_gap_um=input_gap_um,
+                                     length_um=length_um, bead_x_um=bead_x_um, bead_y_um=bead_y_um, wg_n=wg_n,
+                                     bead_n=bead_n, n_aqueous=n_aqueous, n_mucin=n_mucin, n_cornea=n_cornea,
+                                     n_lipid=n_lipid, polarization=polarization, curved=curved,
+                                     boundary=boundary, pulse_cycles=pulse_cycles, cad=cad, stack=stack)
+        finally:
+            globals()['TEAR_BUFFER'] = global_old
     if method != 'full' or str(boundary).lower() != 'cpml' or source_type != 'cw' or cad is not None or curved:
         raise NotImplementedError(f'lens_sensor_b200.run_beads: method={method!r} boundary={boundary!r} '
                                   f'source_type={source_type!r} cad={cad is not None} curved={curved}: '
@@ -468,6 +495,158 @@ def run_beads_stitched(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapsh
         res['Ex_cw_amp'] = ExA_full
     if return_efull:
         res['Efull'] = Efull
+    return res
+
+
+def run_beads_sliding(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
+                      wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt,
+                      vcsel_offset, source_type, window_w_um, slide_um, place_bead=True,
+                      t_aqueous_um=None, t_mucin_um=None, t_lipid_um=0.0, input_gap_um=0.0,
+                      length_um=None, bead_x_um=None, bead_y_um=None, wg_n=None, bead_n=None,
+                      n_aqueous=None, n_mucin=None, n_cornea=None, n_lipid=None,
+                      polarization='s', curved=False, boundary='cpml', pulse_cycles=30.0,
+                      cad=None, stack=None):
+    """2D co-moving window (fdtd2d_core.py:930-1194): a window of window_w_um
+    follows the wave down the guide in slides of slide_um.  Each slide rebuilds
+    the window's materials at its x position, moves the fields and the psi of
+    the CPML (all four edges) back by the slide (the last rows zero) and runs
+    the slide's steps on the engine; the VCSEL (CW or Gaussian pulse) drives
+    the first slide only.  The detector boxes and the time-domain Poynting
+    planes count while their x lies in the window, so transmission is a ratio
+    of pulse energies.  The reference keeps psi over the whole window, and the
+    rolled psi keeps its value outside the absorber (b = 1, c = 0 there): the
+    engine's window grid does the same (psi over every row along x).
+    Supported: boundary='cpml', no CAD, flat geometry."""
+    if str(boundary or 'cpml').lower() != 'cpml' or cad is not None or curved:
+        raise NotImplementedError(f'lens_sensor_b200.run_beads_sliding: boundary={boundary!r} '
+                                  f'cad={cad is not None} curved={curved}: only the CPML co-moving window '
+                                  f'runs on the B200 engine')
+    pol = 'p' if str(polarization).lower() in ('p', 'tm') else 's'
+    t_total = time.time()
+    t_aq_um = t_aqueous_um if t_aqueous_um is not None else T_AQ * 1e6
+    wg_n = wg_n if wg_n is not None else n_at(wg_mat, lambda_nm)
+    bead_n = bead_n if bead_n is not None else n_at(bead_mat, lambda_nm)
+    n_aq_l = n_aqueous if n_aqueous is not None else n_at('aqueous', lambda_nm)
+    n_mu_l = n_mucin if n_mucin is not None else n_at('mucin', lambda_nm)
+    n_co_l = n_cornea if n_cornea is not None else cornea_default(lambda_nm)
+    n_lip_l = n_lipid if n_lipid is not None else n_at('lipid', lambda_nm)
+    L = (length_um * 1e-6) if length_um is not None else L_DEMO
+    L_um = L * 1e6
+    T_WG = wg_thickness_um * 1e-6
+    LAM = lambda_nm * 1e-9
+    label = f'WG-{wg_mat}_Bead-{bead_mat}_d{bead_d_um:g}_L{lambda_nm:g}' + ('' if place_bead else '_ref')
+    dx = dx_nm * 1e-9
+    dt = 0.5 * dx / (C0 * np.sqrt(2))
+    NPML = 10
+    src_ix = NPML + 2
+    vd = float(input_gap_um or 0.0)
+    air = air_path_um(vd, dx * 1e6)
+    x_facet_um = src_ix * dx * 1e6 + air
+    tear_m = TEAR_BUFFER
+    y0_m = -tear_m
+    H_total = T_WG + AIR_BUFFER + tear_m
+    Nx, Ny = int(round(window_w_um * 1e-6 / dx)), int(round(H_total / dx))
+    bx_um = bead_x_um if bead_x_um is not None else L_um / 2.0
+    n_slides = int(np.ceil(L_um / slide_um))
+    N_shift = int(round(slide_um * 1e-6 / dx))
+    st, lossy, k = _stack_2d(wg_n, wg_thickness_um, t_lipid_um, n_lip_l, t_aq_um, n_aq_l, t_mucin_um, n_mu_l,
+                             n_co_l, stack)
+    bead = None
+    if place_bead and bead_d_um:
+        bead = Bead2D(bx_um, bead_d_um, complex(bead_n, k.get('bead', 0.0)) if lossy else bead_n, bead_y_um)
+    f0 = C0 / LAM
+    omega = 2 * np.pi * f0
+    if source_type == 'pulse':       # exp(-((t - 3 s)/s)^2), s = pulse_cycles / f0 (fdtd2d_core.py:1107-1109)
+        s_p = pulse_cycles / f0
+        env = lambda t: np.exp(-(((t - 3 * s_p) / s_p) ** 2))
+    else:
+        env = E.cw_envelope(f0)
+    iy_lo, iy_hi = int(round(tear_m / dx)), int(round((T_WG + tear_m) / dx))
+    # detectors in global x (um); the input plane kept downstream of the source (flux.py:64-74)
+    xi_g = _guard_in_plane(int(round(0.1 * L_um / (dx * 1e6))), max(src_ix, int(round(x_facet_um / (dx * 1e6)))),
+                           int(round(L / dx))) * dx * 1e6
+    det = ((xi_g, 'in'), (0.9 * L_um, 'out'))
+    hw = max(1, int(round(min(DET_LEN / 2, 0.05 * L_um * 1e-6) / dx)))
+    frames, mm_path, ez_mm, k_fr = [], None, None, 0
+    safe = ''.join(c if (c.isalnum() or c in '-_.') else '_' for c in label)
+    if save_frames:
+        os.makedirs('results', exist_ok=True)
+        mm_path = os.path.join('results', f'_stream_beads_{safe}_sliding.npy')
+        ez_mm = np.lib.format.open_memmap(mm_path, mode='w+', dtype=np.float32,
+                                          shape=(max(1, n_snapshots + n_slides + 4), Nx, Ny))
+    sums = dict(in_P=0.0, out_P=0.0, **{q: 0.0 for q in ('in', 'out', 'src_up', 'src_dn')})
+    grid = None
+    t_start = time.time()
+    for slide_i in range(n_slides):
+        x_start_um = slide_i * slide_um
+        if x_start_um >= L_um:
+            break
+        x_end_um = x_start_um + window_w_um
+        src_active = slide_i == 0
+        sp = Spec2D(pol, Nx, Ny, dx, st, tear_m, bead, npml=NPML, lam_nm=lambda_nm, waist_um=vcsel_waist,
+                    length_m=L, vcsel_distance_um=vd, vcsel_offset_um=vcsel_offset, vcsel_tilt_deg=vcsel_tilt,
+                    src_core_only=SRC_CORE_ONLY, x_start_um=x_start_um)
+        geo = build_2d(sp)
+        coef = {q: geo[q] for q in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if q in geo}
+        new = E.Grid2D(pol, Nx, Ny, dx, dt, coef, geo['cx'], geo['cy'], geo['src'] if src_active else None,
+                       full_x=True)
+        if grid is not None:         # fields and psi move with the window (fdtd2d_core.py:1093-1102)
+            new.take_shifted(grid, N_shift if 0 < N_shift < Nx else 0)
+        grid = new
+        steps_slide = (int(window_w_um * 1e-6 * wg_n / C0 / dt) if src_active
+                       else int(slide_um * 1e-6 * wg_n / C0 / dt)) + 200
+        snap_every = max(1, steps_slide // max(1, n_snapshots // n_slides + 1))
+        boxes, names, sxp = [], [], {}
+        for xg, which in det:
+            if x_start_um <= xg <= x_end_um:
+                cl = int(round((xg - x_start_um) * 1e-6 / dx))
+                boxes.append((max(0, cl - hw), min(Nx, cl + hw), iy_lo, iy_hi))
+                names.append(which)
+                if 1 <= cl < Nx - 1:
+                    sxp[which] = cl
+        if src_active:               # energy around the VCSEL pair (vcsel.py:158-166)
+            sxp.update(src_up=src_ix - 1, src_dn=src_ix + 3)
+        ep = E.Epi2D(grid, boxes=boxes, sx_planes=sxp, box_split=True)
+        tab = E.StepTable(0, steps_slide, dt, geo['src']['omega'], omega, env)
+        n = 0
+        while n < steps_slide:
+            nxt = min(steps_slide, (n // snap_every + 1) * snap_every)
+            grid.step(tab, n, nxt - n, ep)
+            n = nxt
+            if save_frames and n % snap_every == 0 and k_fr < ez_mm.shape[0]:
+                ez_mm[k_fr] = _field_2d(grid)
+                frames.append({'x_start': x_start_um, 'x_end': x_end_um, 'y_start': y0_m * 1e6,
+                               'y_end': (y0_m + H_total) * 1e6, 'slide_i': slide_i, 'step': n,
+                               'time': time.time() - t_start})
+                k_fr += 1
+        box = ep.box_acc.double().cpu().numpy()
+        for q, which in enumerate(names):
+            sums[which + '_P'] += float(box[q])
+        for which in sxp:
+            sums[which] += ep.sx(which)
+        del ep
+    if ez_mm is not None:
+        ez_mm.flush()
+        del ez_mm
+    total_time = time.time() - t_total
+    P_in, P_out = sums['in_P'] * dx * dx, sums['out_P'] * dx * dx
+    Tr_I = P_out / max(P_in, 1e-30)
+    S_in, S_out, S_up, S_dn = sums['in'], sums['out'], sums['src_up'], sums['src_dn']
+    Tr = S_out / S_in if abs(S_in) > 0 else Tr_I
+    tr_def = 'poynting' if abs(S_in) > 0 else 'intensity'
+    res = _result_dict(label, P_in, P_out, Tr, frames, total_time, bead_d_um, wg_mat, bead_mat, wg_n, bead_n,
+                       wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt, vcsel_offset, source_type, 'sliding',
+                       place_bead, n_aq_l, n_mu_l, n_co_l, mm_path, t_aq_um, t_mucin_um, t_lipid_um, bx_um,
+                       x_facet_um, L_um, pol, stack, n_lip_l)
+    res['transmission_intensity'] = Tr_I
+    res['transmission_def'] = tr_def
+    # VCSEL pulse energies [J/m]: coupling only, no power scaling (fdtd2d_core.py:415-435, 1187-1188)
+    p_emit, p_refl = (S_dn - S_up) * dx, -S_up * dx
+    res.update(laser_power_mw=LASER_POWER_MW, vcsel_distance_um=vd, vcsel_air_um=float(air),
+               vcsel_waist_um=float(vcsel_waist), x_facet_um=float(x_facet_um), p_src_si=None)
+    if p_emit and p_emit > 0:
+        res['coupling_efficiency'] = (S_in * dx) / p_emit
+        res['facet_reflection'] = p_refl / p_emit
     return res
 
 

@@ -27,7 +27,7 @@ class StepTable:
 
 
 class Grid2D:
-    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None):
+    def __init__(self, pol, nx, ny, dx, dt, coef, cx, cy, src, pec=(1, 1, 1, 1), device=None, full_x=False):
         self.pol = 'p' if str(pol).lower() in ('p', 'tm') else 's'
         self.nx, self.ny, self.dx, self.dt = nx, ny, dx, dt
         if src is None:
@@ -40,6 +40,19 @@ class Grid2D:
 
     def view(self, name):
         return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
+
+    def _state(self):
+        names = (('Ez', 'Hx', 'Hy', 'p_hxy', 'p_hyx', 'p_ezx', 'p_ezy') if self.pol == 's' else
+                 ('Ex', 'Ey', 'Hz', 'p_hzx', 'p_hzy', 'p_exy', 'p_eyx'))
+        return names
+
+    def take_shifted(self, other, n):
+        """The reference's roll of the fields and the full-domain psi with the
+        trailing rows zeroed (fdtd2d_core.py:1093-1102, boundaries.py:217-221)."""
+        for q in self._state():
+            a = np.roll(getattr(other.g, q), -n, axis=0)
+            a[a.shape[0] - n:, :] = 0
+            setattr(self.g, q, a)
 
     def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
         if self.g.src.omega is None:
@@ -68,12 +81,16 @@ class Drive2D:
 
 class Epi2D:
     def __init__(self, grid, boxes=(), dft=None, dft_ex=False, prev=None, iavg_n0=None, planes=(),
-                 dft_raw=False, ex2=False):
+                 dft_raw=False, ex2=False, sx_planes=(), box_split=False):
         nx, ny = grid.nx, grid.ny
         self.grid = grid
         self.boxes = [tuple(b) for b in boxes]
         self.box = np.zeros(len(self.boxes), np.float64)
-        self.win, self.win_prev = tuple(dft), tuple(prev) if prev is not None else (0, 0)
+        self.box_split = box_split
+        self.sx_planes = dict(sx_planes)
+        self.sx_tot = {k: np.float64(0.0) for k in self.sx_planes}
+        self.win = tuple(dft) if dft is not None else (0, 0)
+        self.win_prev = tuple(prev) if prev is not None else (0, 0)
         self.acc = np.zeros((nx, ny), np.complex64)
         self.acc_ex = np.zeros((nx, ny), np.complex64) if dft_ex else None
         self.acc_prev = np.zeros((nx, ny), np.complex64)
@@ -96,7 +113,20 @@ class Epi2D:
         field = g.field()
         I_E = g.intensity(field)
         for q, (x0, x1, y0, y1) in enumerate(self.boxes):
-            self.box[q] += np.sum(I_E[x0:x1, y0:y1], dtype=np.float64)
+            if self.box_split:      # fdtd2d_core.py:1148-1150: field^2 and <Ex^2> summed apart
+                v = np.sum(field[x0:x1, y0:y1] ** 2, dtype=np.float64)
+                if g.pol == 'p':
+                    v = v + np.sum(O.tm_ex2_node(g.Ex)[x0:x1, y0:y1], dtype=np.float64)
+                self.box[q] += v
+            else:
+                self.box[q] += np.sum(I_E[x0:x1, y0:y1], dtype=np.float64)
+        for k, il in self.sx_planes.items():   # _sx_plane_2d (fdtd2d_core.py:489-497)
+            if g.pol == 's':
+                hy = 0.5 * (g.Hy[il - 1] + g.Hy[il])
+                self.sx_tot[k] += -np.sum(g.Ez[il] * hy, dtype=np.float64)
+            else:
+                hz = 0.5 * (g.Hz[il - 1] + g.Hz[il])
+                self.sx_tot[k] += np.sum(g.Ey[il] * hz, dtype=np.float64)
         if self.win[0] <= n < self.win[1]:
             ph = np.exp(-1j * self._omega * t)
             self.acc += field.astype(np.complex64) * ph
@@ -119,6 +149,9 @@ class Epi2D:
     @property
     def box_acc(self):
         return torch.from_numpy(self.box.copy())
+
+    def sx(self, name):
+        return float(self.sx_tot[name])
 
     @property
     def iavg(self):
@@ -202,6 +235,19 @@ class Grid3D:
     def view(self, name):
         return torch.from_numpy(getattr(self.g, name[0].upper() + name[1:]).copy())
 
+    def _state(self):
+        names = (('Ez', 'Hx', 'Hy', 'p_hxy', 'p_hyx', 'p_ezx', 'p_ezy') if self.pol == 's' else
+                 ('Ex', 'Ey', 'Hz', 'p_hzx', 'p_hzy', 'p_exy', 'p_eyx'))
+        return names
+
+    def take_shifted(self, other, n):
+        """The reference's roll of the fields and the full-domain psi with the
+        trailing rows zeroed (fdtd2d_core.py:1093-1102, boundaries.py:217-221)."""
+        for q in self._state():
+            a = np.roll(getattr(other.g, q), -n, axis=0)
+            a[a.shape[0] - n:, :] = 0
+            setattr(self.g, q, a)
+
     def step(self, table, n0, nsteps, epi=None, stream=None, drive=None):
         if self.g.src.omega is None:
             self.g.src.omega = table.omega
@@ -279,6 +325,9 @@ class Epi3D:
     @property
     def box_acc(self):
         return torch.from_numpy(self.box.copy())
+
+    def sx(self, name):
+        return float(self.sx_tot[name])
 
     def phasor(self, comp=1, kind=None):
         if kind == 'split':

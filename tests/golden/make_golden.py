@@ -25,6 +25,7 @@ Outputs:
 `python tests/golden/make_golden.py stitch` writes only the 3D stitch fixtures
 (adds case_3d_stitch to characterization.json, writes dropin_3d_stitch.json);
 `python tests/golden/make_golden.py stitch2d` writes dropin_2d_stitch.json.
+`python tests/golden/make_golden.py sliding2d` writes dropin_2d_sliding.json.
 """
 import json
 import os
@@ -519,7 +520,72 @@ def dropin_2d_stitch():
     return out
 
 
+# ------------------------------------------------------- drop-in 2D sliding window
+# run_beads(method='sliding') -> run_beads_sliding + save_results: 'te_pulse' a
+# Gaussian pulse (3 cycles) through 4 slides of an 8 um window with a bead;
+# 'tm_cw' a CW VCSEL through 4 slides on an absorbing stack with KAPPA on the
+# core, an input gap and a tilted offset source.  Both with a 2 um air buffer
+# (module AIR_BUFFER) and a 3 um tear buffer to keep the runs small.
+DROPIN_2D_SLIDING = dict(
+    te_pulse=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.5, dx_nm=25.0, save_frames=True,
+                          n_snapshots=4, wg_thickness_um=1.0, lambda_nm=850.0, method='sliding', length_um=16.0,
+                          bead_x_um=7.0, window_w_um=8.0, slide_um=4.0, source_type='pulse', pulse_cycles=3.0,
+                          tear_buffer_um=3.0),
+                  kappa={}, air_um=2.0),
+    tm_cw=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.6, dx_nm=25.0, save_frames=True,
+                       n_snapshots=3, wg_thickness_um=1.2, lambda_nm=850.0, method='sliding', length_um=14.0,
+                       bead_x_um=6.3, window_w_um=7.0, slide_um=3.5, polarization='p', input_gap_um=1.5,
+                       vcsel_tilt=2.0, vcsel_offset=0.1, vcsel_waist=1.2, tear_buffer_um=4.5,
+                       stack=[dict(name='Aqueous', t_um=2.0, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                              dict(name='Mucin', t_um=0.5, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+               kappa=dict(wg=0.0005), air_um=2.0),
+)
+
+
+def dropin_2d_sliding():
+    """Run the reference co-moving window end to end for DROPIN_2D_SLIDING and summarise its outputs."""
+    import glob
+    import pickle
+    out = {}
+    for name, c in DROPIN_2D_SLIDING.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_sliding2d_')
+        old_k, old_air = d2.KAPPA, d2.AIR_BUFFER
+        try:
+            os.chdir(tmp)
+            d2.KAPPA = dict(c['kappa'])
+            d2.AIR_BUFFER = c['air_um'] * 1e-6
+            r = d2.run_beads(**c['kw'])
+            res = {k: float(r[k]) for k in ('transmission', 'P_in', 'P_out', 'transmission_intensity')}
+            res.update({k: float(r[k]) for k in ('coupling_efficiency', 'facet_reflection') if k in r})
+            fr = np.load(r['frames_memmap'], mmap_mode='r')[:len(r['frames'])]
+            frames = _summ(np.asarray(fr))
+            d2.save_results(r)
+            z = np.load(glob.glob('results/*_frames.npz')[0])
+            npz = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+            left = sorted(os.listdir('results'))
+        finally:
+            d2.KAPPA, d2.AIR_BUFFER = old_k, old_air
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        out[name] = dict(kw={k: v for k, v in c['kw'].items() if k != 'stack'}, kappa=c['kappa'],
+                         air_um=c['air_um'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         result=res, frames=frames, npz=npz, pkl=scal, files_left=left)
+    return out
+
+
 def main():
+    if 'sliding2d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_2d_sliding.json'), 'w') as f:
+            json.dump(dropin_2d_sliding(), f, indent=1)
+        print('wrote dropin_2d_sliding.json')
+        return
     if 'stitch2d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_2d_stitch.json'), 'w') as f:
             json.dump(dropin_2d_stitch(), f, indent=1)

@@ -98,6 +98,24 @@ def run_beads(wg_mat, bead_mat, bead_d_um, dx_nm=20.0, save_frames=True, n_snaps
                                       boundary=boundary, cad=cad, stack=stack)
         finally:
             TEAR_BUFFER = old
+    if method == 'stitch' and str(source_type).lower() == 'pulse':
+        if pulse_mode == 'td':
+            raise NotImplementedError("lens_sensor_b200.run_beads: the time-domain pulse stitch "
+                                      "(pulse_mode='td') is not built; the Fourier stitch is")
+        global_old = TEAR_BUFFER
+        try:
+            _set_tear(stack, tear_buffer_um, dx_nm, cad)
+            return run_beads_stitched_pulse(
+                wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots, wg_thickness_um, lambda_nm,
+                vcsel_waist, vcsel_tilt, vcsel_offset, window_w_um, slide_um, place_bead,
+                t_aqueous_um=t_aqueous_um, t_mucin_um=t_mucin_um, t_lipid_um=t_lipid_um, input_gap_um=input_gap_um,
+                length_um=length_um, bead_x_um=bead_x_um, bead_y_um=bead_y_um, wg_n=wg_n, bead_n=bead_n,
+                n_aqueous=n_aqueous, n_mucin=n_mucin, n_cornea=n_cornea, n_lipid=n_lipid,
+                polarization=polarization, curved=curved, boundary=boundary, cad=cad, pulse_cycles=pulse_cycles,
+                pulse_tmax_fs=pulse_tmax_fs, pulse_nfreq=pulse_nfreq, pulse_dispersion=pulse_dispersion,
+                n_aq_tear_offset=n_aq_tear_offset, stack=stack)
+        finally:
+            globals()['TEAR_BUFFER'] = global_old
     if method == 'sliding':
         global_old = TEAR_BUFFER
         try:
@@ -498,6 +516,145 @@ def run_beads_stitched(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapsh
     return res
 
 
+def stack_at_lambda(stack, lam_nm):
+    """The stack at another wavelength (fdtd2d_core.py:83-95): a layer that names
+    its material takes that material's n at lam_nm and keeps its absorption;
+    layers given by number stay as they are."""
+    if stack is None:
+        return None
+    out = []
+    for Ly in stack:
+        q = dict(Ly)
+        if q.get('mat'):
+            nc = complex(n_at(q['mat'], lam_nm), complex(q['n']).imag)
+            q['n'], q['kappa'] = nc, nc.imag
+        out.append(q)
+    return out
+
+
+def run_beads_stitched_pulse(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
+                             wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt, vcsel_offset,
+                             window_w_um, slide_um, place_bead, pulse_cycles=30.0,
+                             pulse_tmax_fs=None, pulse_nfreq=None, pulse_dispersion=True,
+                             cad=None, t_eval_s=None, n_aq_tear_offset=None, stack=None, **kw):
+    """Transient 2D stitch by Fourier synthesis (fdtd2d_core.py:1866-2017).
+
+    The source pulse exp(-((t - 3s)/s)^2) sin(w0 t), s = pulse_cycles / f0, is
+    split into frequencies w_k = w0 + k dw inside |w - w0| < 5.26 / s (the band
+    where its spectrum exceeds 1e-3 of the peak), dw = 2 pi / (1.6 t_max) or set
+    by pulse_nfreq.  Every w_k runs a CW stitch on the engine (materials at
+    lambda_k unless pulse_dispersion is off); its assembled amplitude E_k answers
+    sin(w t) = Re(-i e^{iwt}), so the field at t is
+    (1/pi) Re sum_k i E_k S(w_k) e^{i w_k t} dw with
+    S(w) = (G(w - w0) - G(w + w0)) / 2i, G(v) = sqrt(pi) s e^{-(v s)^2/4} e^{-i v tc}.
+    The time frames are summed frequency by frequency on the device (one FP32
+    accumulator per frame); the CW set of the centre frequency and the
+    transmission spectrum come with the result.  No CAD."""
+    if cad is not None:
+        raise NotImplementedError('lens_sensor_b200.run_beads_stitched_pulse: CAD geometry is not built')
+    t_total = time.time()
+    f0 = C0 / (lambda_nm * 1e-9)
+    w0 = 2 * np.pi * f0
+    s_p = pulse_cycles / f0
+    tc = 3 * s_p
+    pol = 'p' if str(kw.get('polarization', 's')).lower() in ('p', 'tm') else 's'
+    L_um = kw.get('length_um') or L_DEMO * 1e6
+    n_core = kw.get('wg_n') or n_at(wg_mat, lambda_nm)
+    y0_um, y1_um = -TEAR_BUFFER * 1e6, (wg_thickness_um * 1e-6 + AIR_BUFFER) * 1e6
+    t_max = (pulse_tmax_fs * 1e-15) if pulse_tmax_fs else tc + 3 * s_p + L_um * 1e-6 * n_core * 1.15 / C0
+    half = 5.26 / s_p
+    dw = 2 * half / max(int(pulse_nfreq) - 1, 1) if pulse_nfreq else 2 * np.pi / (1.6 * t_max)
+    m = int(np.ceil(half / dw))
+    w_k = w0 + np.arange(-m, m + 1) * dw
+    w_k = w_k[w_k > 0]
+    lam_k = 2 * np.pi * C0 / w_k * 1e9
+    G = lambda v: np.sqrt(np.pi) * s_p * np.exp(-(v * s_p) ** 2 / 4.0) * np.exp(-1j * v * tc)
+    S_k = (G(w_k - w0) - G(w_k + w0)) / (2j)
+    fixed = {}
+    if not pulse_dispersion:           # every index held at lambda0
+        fixed = dict(wg_n=kw.get('wg_n') or n_at(wg_mat, lambda_nm),
+                     bead_n=kw.get('bead_n') or n_at(bead_mat, lambda_nm),
+                     n_aqueous=kw.get('n_aqueous') or n_at('aqueous', lambda_nm),
+                     n_mucin=kw.get('n_mucin') or n_at('mucin', lambda_nm),
+                     n_cornea=kw.get('n_cornea') or cornea_default(lambda_nm),
+                     n_lipid=kw.get('n_lipid') or n_at('lipid', lambda_nm))
+    rest = {q: v for q, v in kw.items() if q not in fixed}
+    tear_disp = pulse_dispersion and n_aq_tear_offset is not None
+    n_t = max(int(n_snapshots), 24)
+    t_j = np.linspace(0.0, t_max, n_t)
+    if t_eval_s is not None:
+        t_j = np.asarray(t_eval_s, dtype=np.float64)
+        n_t = len(t_j)
+    label = f'WG-{wg_mat}_Bead-{bead_mat}_d{bead_d_um:g}_L{lambda_nm:g}' + ('' if place_bead else '_ref')
+    safe = ''.join(c if (c.isalnum() or c in '-_.') else '_' for c in label)
+    dev = torch.device('cuda') if torch.cuda.is_available() else torch.device('cpu')
+    acc, spec_T, spec_P = None, [], []
+    k_c = int(np.argmin(np.abs(w_k - w0)))
+    r_c = E_c = None
+    for k, (wk, lk, Sk) in enumerate(zip(w_k, lam_k, S_k)):
+        kwk = dict(rest)
+        if tear_disp:
+            kwk['n_aqueous'] = n_at('aqueous', float(lk)) + float(n_aq_tear_offset)
+        stk = stack_at_lambda(stack, float(lk)) if (stack is not None and pulse_dispersion) else stack
+        r = run_beads_stitched(wg_mat, bead_mat, bead_d_um, dx_nm, False, 4, wg_thickness_um, float(lk),
+                               vcsel_waist, vcsel_tilt, vcsel_offset, 'cw', window_w_um, slide_um, place_bead,
+                               cad=None, return_efull=True, stack=stk, **fixed, **kwk)
+        Ek = np.asarray(r.pop('Efull'))
+        if pol == 'p':                 # Ey (nx, ny-1) onto the nodes (nx, ny)
+            En = np.empty((Ek.shape[0], Ek.shape[1] + 1), dtype=np.complex64)
+            En[:, 1:-1] = 0.5 * (Ek[:, :-1] + Ek[:, 1:])
+            En[:, 0], En[:, -1] = Ek[:, 0], Ek[:, -1]
+            Ek = En
+        if acc is None:
+            acc = torch.zeros((n_t,) + Ek.shape, dtype=torch.float32, device=dev)
+        # i E_k S(w_k) dw / pi, then its real part at every frame time
+        c = (torch.from_numpy(Ek).to(dev) * 1j).to(torch.complex128) * complex(Sk * dw / np.pi)
+        for j, tj in enumerate(t_j):
+            acc[j] += torch.real(c * complex(np.exp(1j * wk * tj))).to(torch.float32)
+        spec_T.append(float(r['transmission']))
+        spec_P.append(float(r['P_out']))
+        if k == k_c:
+            r_c, E_c = r, Ek
+    os.makedirs('results', exist_ok=True)
+    mm_path = os.path.join('results', f'_stream_beads_{safe}_pulse_{os.getpid()}.npy')
+    fr_mm = np.lib.format.open_memmap(mm_path, mode='w+', dtype=np.float32, shape=tuple(acc.shape))
+    for j in range(n_t):
+        fr_mm[j] = acc[j].cpu().numpy()
+    fr_mm.flush()
+    del fr_mm, acc
+    frames = [{'x_start': 0.0, 'x_end': L_um, 'y_start': y0_um, 'y_end': y1_um, 'slide_i': 0, 'step': j,
+               'time': float(tj)} for j, tj in enumerate(t_j)]
+    # the steady set at the centre frequency (the analyzer's second view)
+    cw_path = os.path.join('results', f'_stream_beads_{safe}_pulse_cw_{os.getpid()}.npy')
+    nfr_cw = max(1, n_snapshots)
+    cw_mm = np.lib.format.open_memmap(cw_path, mode='w+', dtype=np.float32, shape=(nfr_cw,) + E_c.shape)
+    cw_frames = []
+    for q in range(nfr_cw):
+        tk = (q / nfr_cw) * (1.0 / (w_k[k_c] / 2 / np.pi))
+        cw_mm[q] = np.real(E_c * np.exp(1j * w_k[k_c] * tk)).astype(np.float32)
+        cw_frames.append({'x_start': 0.0, 'x_end': L_um, 'y_start': y0_um, 'y_end': y1_um, 'slide_i': 0,
+                          'step': q, 'time': tk})
+    cw_mm.flush()
+    del cw_mm
+    res = dict(r_c)
+    res.update(scenario=label, method='stitch-pulse', frames=frames, frames_memmap=mm_path, cw_frames=cw_frames,
+               cw_frames_memmap=cw_path, view_primary='transient', cw_only=False, Iavg=None, source_type='pulse',
+               lambda_nm=lambda_nm, total_time=time.time() - t_total,
+               spectrum=dict(lam_nm=lam_k, T=np.array(spec_T), P_out=np.array(spec_P),
+                             weight=np.abs(S_k) / np.abs(S_k).max()),
+               pulse=dict(cycles=pulse_cycles, s_fs=s_p * 1e15, tmax_fs=t_max * 1e15, nfreq=len(w_k),
+                          dispersion=bool(pulse_dispersion)))
+    if stack is not None:              # the stack at lambda0
+        st = [dict(Ly) for Ly in stack]
+        res['stack'], res['stack_custom'] = st, True
+        res['layers'] = tuple([st[q]['t_um'] * 1e-6 if q < len(st) else 0.0 for q in range(3)] +
+                              [complex(st[1]['n']).real if len(st) > 1 else
+                               (complex(st[0]['n']).real if st else 1.333)])
+    wgt = np.abs(S_k) ** 2
+    res['transmission'] = float(np.sum(wgt * np.array(spec_T)) / np.sum(wgt))   # spectrally weighted
+    return res
+
+
 def run_beads_sliding(wg_mat, bead_mat, bead_d_um, dx_nm, save_frames, n_snapshots,
                       wg_thickness_um, lambda_nm, vcsel_waist, vcsel_tilt,
                       vcsel_offset, source_type, window_w_um, slide_um, place_bead=True,
@@ -790,6 +947,14 @@ def save_results(result, out_dir='results'):
         v = result.get(q)
         if v is not None and np.isfinite(float(v)):
             kw[q] = np.array([float(v)])
+    spec = result.get('spectrum')
+    if spec:                           # Fourier stitch: spectrum and pulse (fdtd2d_core.py:2229-2236)
+        pu = result.get('pulse') or {}
+        kw.update(spec_lam_nm=np.asarray(spec['lam_nm'], dtype=np.float64),
+                  spec_T=np.asarray(spec['T'], dtype=np.float64),
+                  spec_weight=np.asarray(spec['weight'], dtype=np.float64),
+                  pulse_cycles=np.array([pu.get('cycles', 0.0)]), pulse_tmax_fs=np.array([pu.get('tmax_fs', 0.0)]),
+                  pulse_dispersion=np.array([int(bool(pu.get('dispersion', True)))]))
     npz = f'{out_dir}/beads_{tag}_frames.npz'
     np.savez_compressed(npz, **kw)
     # the temporary frame stream files go once the NPZ is written (fdtd2d_core.py:2243-2265)

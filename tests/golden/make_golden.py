@@ -26,6 +26,7 @@ Outputs:
 (adds case_3d_stitch to characterization.json, writes dropin_3d_stitch.json);
 `python tests/golden/make_golden.py stitch2d` writes dropin_2d_stitch.json.
 `python tests/golden/make_golden.py sliding2d` writes dropin_2d_sliding.json.
+`python tests/golden/make_golden.py pulse2d` writes dropin_2d_pulse.json.
 """
 import json
 import os
@@ -580,7 +581,70 @@ def dropin_2d_sliding():
     return out
 
 
+# ------------------------------------------------- drop-in 2D Fourier pulse stitch
+# run_beads(method='stitch', source_type='pulse') -> run_beads_stitched_pulse +
+# save_results: 'te_disp' 5 frequencies with material dispersion (the core's n
+# follows n(lambda_k)) on the characterization stack; 'tm_fixed' 4 frequencies
+# with every index held at lambda0, an absorbing stack, KAPPA on the core, an
+# input gap and a tilted offset source, frames at a set t_max.
+DROPIN_2D_PULSE = dict(
+    te_disp=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.5, dx_nm=100.0, save_frames=True,
+                         n_snapshots=2, wg_thickness_um=1.0, lambda_nm=850.0, method='stitch', length_um=12.0,
+                         bead_x_um=5.0, window_w_um=5.0, slide_um=3.5, source_type='pulse', pulse_cycles=3.0,
+                         pulse_nfreq=5), kappa={}),
+    tm_fixed=dict(kw=dict(wg_mat='pmma', bead_mat='polystyrol', bead_d_um=0.6, dx_nm=100.0, save_frames=True,
+                          n_snapshots=3, wg_thickness_um=1.2, lambda_nm=850.0, method='stitch', length_um=11.0,
+                          bead_x_um=5.3, window_w_um=5.0, slide_um=3.2, polarization='p', input_gap_um=1.5,
+                          vcsel_tilt=2.0, vcsel_offset=0.1, vcsel_waist=1.2, source_type='pulse', pulse_cycles=4.0,
+                          pulse_nfreq=4, pulse_dispersion=False, pulse_tmax_fs=120.0,
+                          stack=[dict(name='Aqueous', t_um=2.0, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                                 dict(name='Mucin', t_um=0.5, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+                  kappa=dict(wg=0.0005)),
+)
+
+
+def dropin_2d_pulse():
+    """Run the reference Fourier pulse stitch end to end for DROPIN_2D_PULSE and summarise its outputs."""
+    import glob
+    import pickle
+    import re
+    out = {}
+    for name, c in DROPIN_2D_PULSE.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_pulse2d_')
+        old_k = d2.KAPPA
+        try:
+            os.chdir(tmp)
+            d2.KAPPA = dict(c['kappa'])
+            r = d2.run_beads(**c['kw'])
+            res = {k: float(r[k]) for k in ('transmission', 'P_in', 'P_out', 'transmission_intensity')}
+            spec = {k: [float(v) for v in np.asarray(r['spectrum'][k])] for k in ('lam_nm', 'T', 'P_out', 'weight')}
+            fr = _summ(np.asarray(np.load(r['frames_memmap'], mmap_mode='r')[:len(r['frames'])]))
+            d2.save_results(r)
+            z = np.load(glob.glob('results/*_frames.npz')[0])
+            npz = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+            left = sorted(re.sub(r'_\d+_\d+\.npy$', '_{tag}.npy', f) for f in os.listdir('results'))
+        finally:
+            d2.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        out[name] = dict(kw={k: v for k, v in c['kw'].items() if k != 'stack'}, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         result=res, spectrum=spec, frames=fr, npz=npz, pkl=scal, files_left=left)
+    return out
+
+
 def main():
+    if 'pulse2d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_2d_pulse.json'), 'w') as f:
+            json.dump(dropin_2d_pulse(), f, indent=1)
+        print('wrote dropin_2d_pulse.json')
+        return
     if 'sliding2d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_2d_sliding.json'), 'w') as f:
             json.dump(dropin_2d_sliding(), f, indent=1)

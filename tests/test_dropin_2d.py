@@ -109,7 +109,7 @@ def test_characterization_known_answer(tmp_path, monkeypatch):
 
 def test_unsupported_paths_refuse():
     with pytest.raises(NotImplementedError):
-        D2.run_beads('pmma', 'polystyrol', 0.5, method='stitch', source_type='pulse')
+        D2.run_beads('pmma', 'polystyrol', 0.5, method='stitch', source_type='pulse', pulse_mode='td')
     with pytest.raises(NotImplementedError):
         D2.run_beads('pmma', 'polystyrol', 0.5, boundary='mur')
 

@@ -19,7 +19,7 @@ import torch
 
 from . import engine as E
 from .geometry import Sphere, Spec3D, Stack, build_3d
-from .physics import C0
+from .physics import C0, cornea_default, n_at
 from .stitch3d import StitchPlan, StitchSolve
 
 # module switches the reference's driver sets (fdtd3d_core.py:52-60)
@@ -423,6 +423,123 @@ def run_3d_stitched(label, wg_n, window_w_um=20.0, slide_um=12.0,
                 transmission_intensity=Tr_I, transmission_def=tr_def)
 
 
+def _drop_streams(res):
+    """Close and delete the temporary memmaps of a result (fdtd3d_core.py:2071-2085)."""
+    for q in ('vols_array', 'vols_ex', 'vols_ey', 'cw_vol', 'Iavg'):
+        m = getattr(res.get(q), '_mmap', None)
+        if m is not None:
+            m.close()
+        res[q] = None
+    for pth in res.get('_stream_paths') or []:
+        if os.path.exists(pth):
+            os.remove(pth)
+
+
+def run_3d_stitched_pulse(label, wg_n, window_w_um=20.0, slide_um=12.0, pulse_cycles=30.0,
+                          pulse_tmax_fs=None, pulse_nfreq=None, pulse_dispersion=True,
+                          disp_map=None, t_eval_s=None, cad=None, stack=None, **kw):
+    """Transient 3D stitch by Fourier synthesis (fdtd3d_core.py:2087-2215).
+
+    The pulse exp(-((t - 3s)/s)^2) sin(w0 t), s = pulse_cycles / f0, is taken
+    apart into frequencies w_k = w0 + k dw (|w - w0| < 5.26 / s; dw =
+    2 pi / (1.6 t_max) or from pulse_nfreq); each runs a CW run_3d_stitched on
+    the engine and its assembled amplitude E_k (the driven component) adds
+    Re(i E_k S(w_k) e^{i w_k t_j}) dw / pi to the frame at t_j, in complex64 as
+    the reference does, on the device.  disp_map {parameter: material} sets
+    those indices from n(lambda_k) (a (material, offset) pair adds the offset;
+    'cornea_layered' the layered cornea; 'bead' the bead's n); stack layers that
+    name a material follow n(lambda_k).  Results: the frames, the CW set of the
+    centre frequency (8 phases), <E^2> over the frames and the transmission
+    spectrum.  No CAD."""
+    from .fdtd2d_core import stack_at_lambda
+    if cad is not None:
+        raise NotImplementedError('lens_sensor_b200.run_3d_stitched_pulse: CAD geometry is not built')
+    t_total = time.time()
+    lam_nm = kw.pop('lam_nm', 850.0)
+    f0 = C0 / (lam_nm * 1e-9)
+    w0 = 2 * np.pi * f0
+    s_p = pulse_cycles / f0
+    tc = 3 * s_p
+    lx = kw.get('lx_um', 40.0)
+    t_max = (pulse_tmax_fs * 1e-15) if pulse_tmax_fs else tc + 3 * s_p + lx * 1e-6 * wg_n * 1.15 / C0
+    half = 5.26 / s_p
+    dw = 2 * half / max(int(pulse_nfreq) - 1, 1) if pulse_nfreq else 2 * np.pi / (1.6 * t_max)
+    m = int(np.ceil(half / dw))
+    w_k = w0 + np.arange(-m, m + 1) * dw
+    w_k = w_k[w_k > 0]
+    lam_k = 2 * np.pi * C0 / w_k * 1e9
+    G = lambda v: np.sqrt(np.pi) * s_p * np.exp(-(v * s_p) ** 2 / 4.0) * np.exp(-1j * v * tc)
+    S_k = (G(w_k - w0) - G(w_k + w0)) / (2j)
+    n_snap = int(kw.pop('n_snapshots', 8))
+    t_j = (np.asarray(t_eval_s, dtype=np.float64) if t_eval_s is not None
+           else np.linspace(0.0, t_max, max(n_snap, 8)))
+    dmap = dict(disp_map or {}) if pulse_dispersion else {}
+    dev = torch.device('cuda') if torch.cuda.is_available() else torch.device('cpu')
+    acc, spec_T = None, []
+    r_c = E_c = None
+    k_c = int(np.argmin(np.abs(w_k - w0)))
+    os.makedirs('results', exist_ok=True)
+    safe = ''.join(c if (c.isalnum() or c in '-_.') else '_' for c in str(label))
+    for k, (wk, lk, Sk) in enumerate(zip(w_k, lam_k, S_k)):
+        kwk, wg_k = dict(kw), wg_n
+        for par, mat in dmap.items():
+            if par == 'wg_n':
+                wg_k = n_at(mat, lk)
+            elif par == 'bead':
+                if kwk.get('bead'):
+                    kwk['bead'] = dict(kwk['bead'], n=n_at(mat, lk))
+            elif mat == 'cornea_layered':
+                kwk[par] = cornea_default(lk)
+            elif isinstance(mat, (tuple, list)):
+                kwk[par] = n_at(mat[0], lk) + float(mat[1])
+            else:
+                kwk[par] = n_at(mat, lk)
+        stk = stack_at_lambda(stack, float(lk)) if (stack is not None and pulse_dispersion) else stack
+        r = run_3d_stitched(f'{label}_f{k}', wg_k, window_w_um=window_w_um, slide_um=slide_um, lam_nm=float(lk),
+                            n_snapshots=1, return_efull=True, cad=None, stack=stk, **kwk)
+        Ek = r.pop('Efull')
+        if acc is None:
+            acc = torch.zeros((len(t_j),) + Ek.shape, dtype=torch.float32, device=dev)
+        c = (torch.from_numpy(np.ascontiguousarray(Ek)).to(dev) * 1j) * complex(np.complex64(Sk * dw / np.pi))
+        for j, tj in enumerate(t_j):
+            acc[j] += torch.real(c * complex(np.complex64(np.exp(1j * wk * tj))))
+        spec_T.append(float(r['transmission']))
+        if k == k_c:
+            r_c, E_c = r, Ek
+        _drop_streams(r)
+    fr_path = os.path.join('results', f'_stream3d_{safe}_fourier_ez.npy')
+    fr = np.lib.format.open_memmap(fr_path, mode='w+', dtype=np.float32, shape=tuple(acc.shape))
+    for j in range(len(t_j)):
+        fr[j] = acc[j].cpu().numpy()
+    fr.flush()
+    # the steady set at the centre frequency and <E^2> over the frames
+    nfr_cw = 8
+    cw_path = os.path.join('results', f'_stream3d_{safe}_fourier_cwvol.npy')
+    cw_vol = np.lib.format.open_memmap(cw_path, mode='w+', dtype=np.float32, shape=(nfr_cw,) + E_c.shape)
+    for q in range(nfr_cw):
+        cw_vol[q] = np.real(E_c * np.complex64(np.exp(2j * np.pi * q / nfr_cw))).astype(np.float32)
+    cw_vol.flush()
+    ia_path = os.path.join('results', f'_stream3d_{safe}_fourier_Iavg.npy')
+    Iavg = np.lib.format.open_memmap(ia_path, mode='w+', dtype=np.float32, shape=E_c.shape)
+    for x0 in range(0, E_c.shape[0], 64):
+        Iavg[x0:x0 + 64] = np.mean(np.asarray(fr[:, x0:x0 + 64], dtype=np.float32) ** 2, axis=0)
+    Iavg.flush()
+    del acc
+    res = dict(r_c)
+    wgt = np.abs(S_k) ** 2
+    res.update(scenario=label, vols_array=fr, vols_ex=None, vols_ey=None, vector=False,
+               _stream_paths=[fr_path, cw_path, ia_path], snap_steps=[int(round(t / r_c['dt'])) for t in t_j],
+               snap_times=[float(t) for t in t_j], Iavg=Iavg, cw_vol=cw_vol, view_primary='transient',
+               cw_only=False, source_type='pulse', lam_nm=lam_nm, total_time=time.time() - t_total,
+               transmission=float(np.sum(wgt * np.array(spec_T)) / np.sum(wgt)),
+               spectrum=dict(lam_nm=lam_k, T=np.array(spec_T), weight=np.abs(S_k) / np.abs(S_k).max()),
+               pulse=dict(cycles=pulse_cycles, tmax_fs=t_max * 1e15, nfreq=len(w_k),
+                          dispersion=bool(pulse_dispersion)))
+    if stack is not None:              # the stack at lambda0
+        res.update(stack=[dict(Ly) for Ly in stack], stack_custom=True, layers=_layers_tuple(stack))
+    return res
+
+
 def save_results_3d(result, out_dir='results', prefix='fdtd3d', material_names=None):
     """PKL summary, z mid-plane frames NPZ and full-volume NPZ (fdtd3d_core.py:2218-2461)."""
     os.makedirs(out_dir, exist_ok=True)
@@ -475,6 +592,14 @@ def save_results_3d(result, out_dir='results', prefix='fdtd3d', material_names=N
                  has_cw=np.array([1 if (cw_only or cw_vol is not None) else 0]),
                  cw_only=np.array([1 if cw_only else 0]),
                  view_primary=np.array([str(result.get('view_primary', 'transient'))]))
+    spec = result.get('spectrum')
+    if spec:                           # Fourier stitch: the spectrum in both NPZ (fdtd3d_core.py:2301-2308)
+        pu = result.get('pulse') or {}
+        flags.update(spec_lam_nm=np.asarray(spec['lam_nm'], dtype=np.float64),
+                     spec_T=np.asarray(spec['T'], dtype=np.float64),
+                     spec_weight=np.asarray(spec['weight'], dtype=np.float64),
+                     pulse_cycles=np.array([pu.get('cycles', 0.0)]),
+                     pulse_dispersion=np.array([int(bool(pu.get('dispersion', True)))]))
     bead = result.get('bead') or {}
     bd = bead.get('d_um', 0.0)
     bead_yc, bead_zc = bead.get('y_um', -bd / 2.0), bead.get('z_um', 0.0)

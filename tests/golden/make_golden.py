@@ -27,6 +27,7 @@ Outputs:
 `python tests/golden/make_golden.py stitch2d` writes dropin_2d_stitch.json.
 `python tests/golden/make_golden.py sliding2d` writes dropin_2d_sliding.json.
 `python tests/golden/make_golden.py pulse2d` writes dropin_2d_pulse.json.
+`python tests/golden/make_golden.py pulse3d` writes dropin_3d_pulse.json.
 """
 import json
 import os
@@ -639,7 +640,74 @@ def dropin_2d_pulse():
     return out
 
 
+# ------------------------------------------------- drop-in 3D Fourier pulse stitch
+# fdtd3d_core.run_3d_stitched_pulse + save_results_3d: 'te_disp' the
+# characterization stitch geometry, 3 frequencies, the core's n from n(lambda_k)
+# (disp_map); 'tm_fixed' the absorbing-stack channel case, 3 frequencies with the
+# indices held, a set t_max and 8 frames.
+DROPIN_3D_PULSE = dict(
+    te_disp=dict(kw=dict(label='te_disp', wg_n=1.491, window_w_um=2.0, slide_um=1.2, lx_um=4.0, air_um=1.0,
+                         tear_um=2.0, lz_um=2.0, dx_nm=100.0, t_wg_um=1.0, t_aq_um=1.0, t_mu_um=0.5, lam_nm=850.0,
+                         n_snapshots=2, vcsel_waist_um=1.0, vcsel_waist_z_um=1.0,
+                         bead=dict(x_um=2.0, d_um=0.5, n=1.59), n_sponge=8, pulse_cycles=3.0, pulse_nfreq=3,
+                         disp_map=dict(wg_n='pmma')), kappa={}),
+    tm_fixed=dict(kw=dict(label='tm_fixed', wg_n=1.49, window_w_um=2.2, slide_um=1.0, lx_um=5.0, air_um=0.6,
+                          tear_um=2.0, lz_um=2.0, dx_nm=100.0, t_wg_um=0.9, lam_nm=850.0, n_snapshots=3,
+                          vcsel_waist_um=0.9, vcsel_waist_z_um=0.7, vcsel_tilt_deg=2.0, vcsel_offset_y_um=0.05,
+                          vcsel_offset_z_um=-0.1, input_gap_um=1.5, wg_width_um=1.2, n_clad_side=1.33,
+                          bead=dict(x_um=2.1, d_um=0.6, n=1.59, z_um=0.15), n_sponge=8, polarization='p',
+                          pulse_cycles=4.0, pulse_nfreq=3, pulse_dispersion=False, pulse_tmax_fs=90.0,
+                          stack=[dict(name='Aqueous', t_um=1.0, n=complex(1.333, 0.002), kappa=0.002, mat=None),
+                                 dict(name='Mucin', t_um=0.3, n=complex(1.342, 0.0), kappa=0.0, mat=None)]),
+                  kappa={}),
+)
+
+
+def dropin_3d_pulse():
+    """Run the reference 3D Fourier pulse stitch end to end for DROPIN_3D_PULSE and summarise."""
+    import glob
+    import pickle
+    out = {}
+    for name, c in DROPIN_3D_PULSE.items():
+        prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_pulse3d_')
+        old_k = d3.KAPPA
+        try:
+            os.chdir(tmp)
+            d3.KAPPA = dict(c['kappa'])
+            r = d3.run_3d_stitched_pulse(**c['kw'])
+            res = dict(transmission=float(r['transmission']), P_in=float(r['P_in']), P_out=float(r['P_out']))
+            spec = {k: [float(v) for v in np.asarray(r['spectrum'][k])] for k in ('lam_nm', 'T', 'weight')}
+            arrays = dict(vols=_summ(np.asarray(r['vols_array'])), Iavg=_summ(np.asarray(r['Iavg'])),
+                          cw_vol=_summ(np.asarray(r['cw_vol'])))
+            d3.save_results_3d(r)
+            files = {}
+            for f in sorted(glob.glob('results/*.npz')):
+                z = np.load(f)
+                files[os.path.basename(f).replace(c['kw']['label'], '{label}')] = {k: _summ(z[k]) for k in z.files}
+            with open(glob.glob('results/*.pkl')[0], 'rb') as f:
+                pk = pickle.load(f)
+            left = sorted(os.listdir('results'))
+        finally:
+            d3.KAPPA = old_k
+            os.chdir(prev)
+            shutil.rmtree(tmp, ignore_errors=True)
+        scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
+                    [float(np.real(v)), float(np.imag(v))] if isinstance(v, complex) else float(v))
+                for k, v in pk.items() if isinstance(v, (str, bool, int, float, complex, np.floating))
+                or v is None}
+        kw = {k: v for k, v in c['kw'].items() if k != 'stack'}
+        out[name] = dict(kw=kw, kappa=c['kappa'],
+                         stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
+                         result=res, spectrum=spec, arrays=arrays, npz=files, pkl=scal, files_left=left)
+    return out
+
+
 def main():
+    if 'pulse3d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_3d_pulse.json'), 'w') as f:
+            json.dump(dropin_3d_pulse(), f, indent=1)
+        print('wrote dropin_3d_pulse.json')
+        return
     if 'pulse2d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_2d_pulse.json'), 'w') as f:
             json.dump(dropin_2d_pulse(), f, indent=1)

@@ -628,6 +628,25 @@ __device__ __forceinline__ void stage_hpsi(uint32_t dst, const K3 &g, IX o, unsi
         if (M & ax[q]) cp_async4(dst + q * NT3 * 4, on[q] ? g.pr[q] + o : g.pr[q], on[q]);
 }
 
+// A CPML tile that carries the psi of one axis only.
+template <unsigned M>
+constexpr bool single_axis() {
+    return M == AXZ || M == AXY || M == AXX;
+}
+
+// Stage the E-psi of one cell of a single-axis tile beside its H-psi: E component e
+// (ex_y, ex_z, ey_z, ey_x, ez_x, ez_y) into slot e, a slot the H-psi of that one
+// axis leaves free (z: H 0, 3 / E 1, 2; y: H 1, 4 / E 0, 5; x: H 2, 5 / E 3, 4).
+template <unsigned M, typename IX>
+__device__ __forceinline__ void stage_epsi(uint32_t dst, const K3 &g, IX o, unsigned f, bool xe) {
+    const bool in = f & F_IN, z = in && (f & F_ZE), y = in && (f & F_YE), x = in && xe;
+    const bool on[6] = {y, z, z, x, x, y};
+    constexpr unsigned ax[6] = {AXY, AXZ, AXZ, AXX, AXX, AXY};
+#pragma unroll
+    for (int e = 0; e < 6; ++e)
+        if (M & ax[e]) cp_async4(dst + e * NT3 * 4, on[e] ? g.pr[6 + e] + o : g.pr[6 + e], on[e]);
+}
+
 // psi values of one cell (E-psi: ex_y, ex_z, ey_z, ey_x, ez_x, ez_y)
 struct P6 {
     float v[6];
@@ -896,6 +915,11 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         const uint32_t d = hs_s + (((unsigned)(p - xs) & 1u) * HS_STAGE) * 4;
         stage_hpsi<M>(d, g, base + oa, fa, xh);
         stage_hpsi<M>(d + 6 * NT3 * 4, g, base + ob, fb, xh);
+        if (single_axis<M>() && owner && p >= x0) {  // E-psi of plane p, read in its E phase
+            const bool xe = (M & AXX) && in_strip(g.ax.e, p);
+            stage_epsi<M>(d, g, base + oa, fa, xe);
+            stage_epsi<M>(d + 6 * NT3 * 4, g, base + ob, fb, xe);
+        }
         cp_async_commit();
     };
     auto load_ep = [&](int p) {
@@ -906,7 +930,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     };
     if (!owner) load_hold(xs);
     if (ST && M) stage_hp(xs);
-    if (ST && M && owner) load_ep(x0);
+    if (ST && M && !single_axis<M>() && owner) load_ep(x0);
     // coefficient column types: the tile's rows of the type table into shared
     // memory; each owner lane's column type one plane ahead
     float *sCT = reinterpret_cast<float *>(smem + OFF_CT);
@@ -1020,6 +1044,13 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
             cs += nb;
             const C6 cb{cs[0], cs[st], cs[2 * st], lossy ? cs[3 * st] : 1.f, lossy ? cs[4 * st] : 1.f,
                         lossy ? cs[5 * st] : 1.f};
+            if (ST && single_axis<M>()) {  // E-psi staged beside the H-psi of this plane
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    epa.v[e] = hs[e * NT3];
+                    epb.v[e] = hs[(6 + e) * NT3];
+                }
+            }
             const F3 Ea = e_new<ST, M, IX>(g, F3{exa, cya, cza}, ha, hxka, hyka, hxja, hzja, hyma, hzma, ca, fa,
                                         pl, ja, k, zta, yta, px, epa, base + oa);
             const F3 Eb = e_new<ST, M, IX>(g, F3{exb, cyb, czb}, hb, hxkb, hykb, ha.x, ha.z, hymb, hzmb, cb, fb,
@@ -1035,7 +1066,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
                 g.wex[o] = Eb.x; g.wey[o] = Eb.y; g.wez[o] = Eb.z;
             }
         }
-        if (ST && M && owner && i + 1 < x1) load_ep(i + 1);
+        if (ST && M && !single_axis<M>() && owner && i + 1 < x1) load_ep(i + 1);
         // carry; advance the ring counters
         cya = nya; cza = nza; cyb = nyb; czb = nzb;
         hyma = ha.y; hzma = ha.z; hymb = hb.y; hzmb = hb.z;

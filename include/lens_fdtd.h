@@ -191,6 +191,14 @@ typedef struct {
                                     runs: its own step is n - n_start (source
                                     time, DFT window, table row), so instances
                                     can join a batch that is already running    */
+    /* Optional row form of the coefficients (NULL rtype: every row from c[]).
+       A layered instance repeats a few coefficient rows (over y) on almost
+       every x row: rtype[i] < ntype names row i's type in ctab, laid out
+       (type, coefficient q, pitch); 255 reads row i from c[].  Values are
+       c[]'s own, bit for bit.                                                */
+    const unsigned char *rtype;  /* (nx) or NULL                                */
+    const float *ctab;           /* (ntype, ncoef, pitch), ncoef = TE 2 / TM 2
+                                    or 4 (with damping)                       */
 } LensInst2D;
 
 /* Block plan of a batch for tiles of 128 columns x 2*by rows: writes blk[0..ninst]

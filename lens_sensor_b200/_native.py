@@ -93,7 +93,8 @@ class Inst2D(ctypes.Structure):
     _fields_ = [('pol', c_int), ('nx', c_int), ('ny', c_int), ('pitch', c_int),
                 ('f', c_void_p * 3), ('c', c_void_p * 4), ('ch', c_float),
                 ('ax', Axis), ('ay', Axis), ('psi', c_void_p * 4), ('pec', c_int * 4),
-                ('src', Source), ('dft_n0', c_int), ('dft_n1', c_int), ('dft', c_void_p), ('n_start', c_int)]
+                ('src', Source), ('dft_n0', c_int), ('dft_n1', c_int), ('dft', c_void_p), ('n_start', c_int),
+                ('rtype', c_void_p), ('ctab', c_void_p)]
 
 
 class Drive3D(ctypes.Structure):

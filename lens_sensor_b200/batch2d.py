@@ -30,6 +30,33 @@ from .geometry import build_2d
 DTYPES = {'f32': (N.F32, torch.float32), 'f16': (N.F16, torch.float16), 'bf16': (N.BF16, torch.bfloat16)}
 
 
+MAX_RTYPE = 4
+
+
+def row_types(coefs, min_rows=8):
+    """Row form of an instance's padded (nx, pitch) coefficient arrays
+    (LensInst2D.rtype / ctab): the x rows are grouped by their exact bytes over
+    all coefficient arrays; the up to 4 most frequent groups of at least
+    min_rows rows become row types (rtype = type, 255 for the other rows) and
+    their rows form the table (ntype, ncoef, pitch).  Returns (None, None)
+    when no group qualifies."""
+    dev = coefs[0].device
+    a = torch.stack(coefs, dim=1).cpu().numpy()            # (nx, ncoef, pitch)
+    rows = np.ascontiguousarray(a.reshape(a.shape[0], -1)).view(np.uint8).reshape(a.shape[0], -1)
+    uniq, inv, cnt = np.unique(rows, axis=0, return_inverse=True, return_counts=True)
+    inv = inv.reshape(-1)
+    order = [u for u in np.argsort(-cnt, kind='stable')[:MAX_RTYPE] if cnt[u] >= min_rows]
+    if not order:
+        return None, None
+    rt = np.full(a.shape[0], 255, np.uint8)
+    tab = np.zeros((len(order),) + a.shape[1:], np.float32)
+    for t, u in enumerate(order):
+        sel = np.nonzero(inv == u)[0]
+        rt[sel] = t
+        tab[t] = a[sel[0]]
+    return torch.from_numpy(rt).to(dev), torch.from_numpy(tab).to(dev)
+
+
 class Instance:
     """Device state of one 2D solve in a batch."""
 
@@ -47,6 +74,7 @@ class Instance:
         else:
             cn = ['ca_x', 'ca_y'] + (['da_x', 'da_y'] if geo.get('da_x') is not None else [])
         self.c = [E._pad_upload(geo[k], shp, dev) for k in cn]
+        self.rtype, self.ctab = row_types(self.c)
         self.axx, self.axy = E._Axis(geo['cx'], nx, dev), E._Axis(geo['cy'], ny, dev)
         wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
         z = lambda a, b: torch.zeros((a, b), dtype=torch.float32, device=dev)
@@ -78,10 +106,12 @@ class Instance:
                          E._ptr(self.src_t['ph2']), len(src['amp']), 1, len(src['amp']))
         s.dft_n0, s.dft_n1 = self.window
         s.dft = self.dft.data_ptr()
+        if self.rtype is not None:
+            s.rtype, s.ctab = self.rtype.data_ptr(), self.ctab.data_ptr()
         self.s = s
 
     def nbytes(self):
-        t = self.f + self.c + self.psi + [self.dft]
+        t = self.f + self.c + self.psi + [self.dft] + ([self.ctab] if self.ctab is not None else [])
         return sum(x.numel() * x.element_size() for x in t)
 
     def reset(self):

@@ -127,6 +127,16 @@ struct V {
         return reinterpret_cast<float *>(__ldg(reinterpret_cast<const unsigned long long *>(&p->psi[q])));
     }
     __device__ __forceinline__ float ch() const { return __ldg(&p->ch); }
+    // coefficient q of row i from column j0 on: the row-type table where row i
+    // has a type, else the instance's own array
+    __device__ __forceinline__ const float *crow(int q, int ncoef, int i, int j0, size_t o) const {
+        const unsigned char *rt = reinterpret_cast<const unsigned char *>(
+            __ldg(reinterpret_cast<const unsigned long long *>(&p->rtype)));
+        const unsigned t = rt ? __ldg(rt + i) : 255u;
+        if (t == 255u) return c(q) + o;
+        const float *tab = reinterpret_cast<const float *>(__ldg(reinterpret_cast<const unsigned long long *>(&p->ctab)));
+        return tab + ((size_t)t * ncoef + q) * (size_t)pitch() + j0;
+    }
     __device__ __forceinline__ const LensProfile &prof(bool x, bool e) const {
         return x ? (e ? p->ax.e : p->ax.h) : (e ? p->ay.e : p->ay.h);
     }
@@ -277,7 +287,6 @@ __global__ void __launch_bounds__(256, 4)
     if (g.pol() == 0) {  // TE: Ez (boundaries.py:196-215), source, PEC, node DFT
         void *ezp = g.f(0);
         const void *hxp = g.f(1), *hyp = g.f(2);
-        const float *ce = g.c(0), *chh = g.c(1);
         float hy[RB + 1][VEC], hx[RB][VEC], hxp1[RB], ez[RB][VEC];
 #pragma unroll
         for (int r = 0; r <= RB; ++r) {  // hy[r] = Hy(i0 + r - 1)
@@ -301,8 +310,8 @@ __global__ void __launch_bounds__(256, 4)
             const int s = (i > 0 && i < nx - 1) ? strip_of(i, xe.lo, xe.hi, xe.n) : -1;
             const float ki = __ldg(xe.ik + i);
             float c0[VEC], c1[VEC], v4[VEC];
-            f4_to(__ldg(reinterpret_cast<const float4 *>(ce + o)), c0);
-            f4_to(__ldg(reinterpret_cast<const float4 *>(chh + o)), c1);
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(0, 2, i, j0, o))), c0);
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(1, 2, i, j0, o))), c1);
 #pragma unroll
             for (int c = 0; c < VEC; ++c) {
                 const int j = j0 + c;
@@ -328,7 +337,7 @@ __global__ void __launch_bounds__(256, 4)
     // TM: loss damping, Ex / Ey (boundaries.py:249-268), source, PEC
     void *exp_ = g.f(0), *eyp = g.f(1);
     const void *hzp = g.f(2);
-    const float *cax = g.c(0), *cay = g.c(1), *dax = g.c(2), *day = g.c(3);
+    const float *dax = g.c(2), *day = g.c(3);
     float hz[RB + 1][VEC], hzp1[RB], ex[RB][VEC], ey[RB][VEC];
 #pragma unroll
     for (int r = 0; r <= RB; ++r) {  // hz[r] = Hz(i0 + r - 1)
@@ -348,10 +357,13 @@ __global__ void __launch_bounds__(256, 4)
         const int i = i0 + r;
         if (i >= nx) break;
         const size_t o = (size_t)i * P + j0;
-        const float4 ax4 = __ldg(reinterpret_cast<const float4 *>(cax + o));
-        const float4 ay4 = __ldg(reinterpret_cast<const float4 *>(cay + o));
-        const float4 dx4 = dax ? __ldg(reinterpret_cast<const float4 *>(dax + o)) : make_float4(1.f, 1.f, 1.f, 1.f);
-        const float4 dy4 = day ? __ldg(reinterpret_cast<const float4 *>(day + o)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        const int nq = dax ? 4 : 2;
+        const float4 ax4 = __ldg(reinterpret_cast<const float4 *>(g.crow(0, nq, i, j0, o)));
+        const float4 ay4 = __ldg(reinterpret_cast<const float4 *>(g.crow(1, nq, i, j0, o)));
+        const float4 dx4 = dax ? __ldg(reinterpret_cast<const float4 *>(g.crow(2, nq, i, j0, o)))
+                               : make_float4(1.f, 1.f, 1.f, 1.f);
+        const float4 dy4 = day ? __ldg(reinterpret_cast<const float4 *>(g.crow(3, nq, i, j0, o)))
+                               : make_float4(1.f, 1.f, 1.f, 1.f);
         float ax_[VEC], ay_[VEC], dx_[VEC], dy_[VEC];
         f4_to(ax4, ax_); f4_to(ay4, ay_); f4_to(dx4, dx_); f4_to(dy4, dy_);
         const int s = (i > 0 && i < nx - 1) ? strip_of(i, xe.lo, xe.hi, xe.n) : -1;
@@ -427,6 +439,7 @@ bool inst_ok(const LensInst2D &g) {
     if ((g.pol != 0 && g.pol != 1) || g.nx < 3 || g.ny < 3 || g.pitch < g.ny || (g.pitch % 32)) return false;
     if (!g.f[0] || !g.f[1] || !g.f[2] || !g.c[0] || !g.c[1]) return false;
     if (g.pol == 1 && (!g.c[2]) != (!g.c[3])) return false;
+    if (g.rtype && !g.ctab) return false;
     if (!lens_profile_ok(g.ax.e, g.nx) || !lens_profile_ok(g.ax.h, g.nx - 1) || !lens_profile_ok(g.ay.e, g.ny) ||
         !lens_profile_ok(g.ay.h, g.ny - 1))
         return false;

@@ -33,27 +33,31 @@ DTYPES = {'f32': (N.F32, torch.float32), 'f16': (N.F16, torch.float16), 'bf16': 
 MAX_RTYPE = 4
 
 
-def row_types(coefs, min_rows=8):
-    """Row form of an instance's padded (nx, pitch) coefficient arrays
-    (LensInst2D.rtype / ctab): the x rows are grouped by their exact bytes over
-    all coefficient arrays; the up to 4 most frequent groups of at least
-    min_rows rows become row types (rtype = type, 255 for the other rows) and
-    their rows form the table (ntype, ncoef, pitch).  Returns (None, None)
+def row_types(arrays, shape, dev, min_rows=8):
+    """Row form of an instance's coefficient arrays (LensInst2D.rtype / ctab),
+    from the host arrays (no device round trip): each array sits in the leading
+    corner of a zero (nx, pitch) block, as on the device; the x rows are grouped
+    by their exact bytes over all arrays, and the up to 4 most frequent groups of
+    at least min_rows rows become row types (rtype = type, 255 for the other
+    rows) whose rows form the table (ntype, ncoef, pitch).  Returns (None, None)
     when no group qualifies."""
-    dev = coefs[0].device
-    a = torch.stack(coefs, dim=1).cpu().numpy()            # (nx, ncoef, pitch)
-    rows = np.ascontiguousarray(a.reshape(a.shape[0], -1)).view(np.uint8).reshape(a.shape[0], -1)
-    uniq, inv, cnt = np.unique(rows, axis=0, return_inverse=True, return_counts=True)
-    inv = inv.reshape(-1)
-    order = [u for u in np.argsort(-cnt, kind='stable')[:MAX_RTYPE] if cnt[u] >= min_rows]
-    if not order:
+    nx, P = shape
+    a = np.zeros((nx, len(arrays), P), np.float32)
+    for q, v in enumerate(arrays):
+        v = np.asarray(v, np.float32)
+        a[:v.shape[0], q, :v.shape[1]] = v
+    groups = {}
+    for i in range(nx):
+        groups.setdefault(a[i].tobytes(), []).append(i)
+    best = sorted(groups.values(), key=len, reverse=True)[:MAX_RTYPE]
+    best = [g for g in best if len(g) >= min_rows]
+    if not best:
         return None, None
-    rt = np.full(a.shape[0], 255, np.uint8)
-    tab = np.zeros((len(order),) + a.shape[1:], np.float32)
-    for t, u in enumerate(order):
-        sel = np.nonzero(inv == u)[0]
-        rt[sel] = t
-        tab[t] = a[sel[0]]
+    rt = np.full(nx, 255, np.uint8)
+    tab = np.zeros((len(best), len(arrays), P), np.float32)
+    for t, g in enumerate(best):
+        rt[g] = t
+        tab[t] = a[g[0]]
     return torch.from_numpy(rt).to(dev), torch.from_numpy(tab).to(dev)
 
 
@@ -74,7 +78,7 @@ class Instance:
         else:
             cn = ['ca_x', 'ca_y'] + (['da_x', 'da_y'] if geo.get('da_x') is not None else [])
         self.c = [E._pad_upload(geo[k], shp, dev) for k in cn]
-        self.rtype, self.ctab = row_types(self.c)
+        self.rtype, self.ctab = row_types([geo[k] for k in cn], shp, dev)
         self.axx, self.axy = E._Axis(geo['cx'], nx, dev), E._Axis(geo['cy'], ny, dev)
         wxe, wxh, wye, wyh = self.axx.w('e'), self.axx.w('h'), self.axy.w('e'), self.axy.w('h')
         z = lambda a, b: torch.zeros((a, b), dtype=torch.float32, device=dev)

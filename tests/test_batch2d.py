@@ -51,6 +51,32 @@ def test_plan_of_uneven_instances():
     assert lib.lens_batch2d_plan(bad, 1, 4, blk, None) == -1
 
 
+def test_row_types_are_exact_rows_of_the_coefficients():
+    """The row form (LensInst2D.rtype / ctab) holds each typed row's bytes exactly
+    and covers the layered rows of config-2 instances (TE, lossless and lossy TM)."""
+    from lens_sensor_b200 import batch2d as B
+    from lens_sensor_b200 import engine as E
+    from lens_sensor_b200.geometry import build_2d
+    from lens_sensor_b200.workloads import config2
+    specs, _ = config2(count=4)
+    for sp in specs:
+        g = build_2d(sp)
+        cn = ['ce_e', 'ce_h'] if sp.pol == 's' else ['ca_x', 'ca_y'] + (['da_x', 'da_y'] if g.get('da_x') is not None else [])
+        P = E.pitch_of(sp.ny)
+        rt, tab = B.row_types([g[k] for k in cn], (sp.nx, P), 'cpu')
+        full = np.zeros((sp.nx, len(cn), P), np.float32)
+        for q, k in enumerate(cn):
+            v = np.asarray(g[k], np.float32)
+            full[:v.shape[0], q, :v.shape[1]] = v
+        rt, tab = rt.numpy(), tab.numpy()
+        assert tab.shape[0] <= B.MAX_RTYPE and (rt != 255).mean() > 0.9
+        for i in range(sp.nx):
+            if rt[i] != 255:
+                assert full[i].tobytes() == tab[rt[i]].tobytes(), i
+    flat = [np.arange(12, dtype=np.float32).reshape(3, 4)]       # three different rows: no type
+    assert B.row_types(flat, (3, 32), 'cpu') == (None, None)
+
+
 def _small_sweep():
     from lens_sensor_b200.workloads import config2
     specs, _ = config2(count=6)

@@ -41,6 +41,22 @@ def dist_env():
     return ws, int(os.environ.get('RANK', '0')), int(os.environ.get('LOCAL_RANK', '0'))
 
 
+def max_over_ranks(x, pg, device='cuda'):
+    """The slowest rank's figure (every rank must call it, in the same order);
+    x itself without a process group."""
+    if not pg:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(cells, steps, ws, seconds):
+    """Whole-job cell updates per second: ws replicas, each `steps` steps of `cells`."""
+    return cells * steps * ws / seconds
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
@@ -156,13 +172,9 @@ def run_e2e(spec, steps_total, cells, ws, pg):
     ph = [s2.phasor(c).cpu() for c in (0, 1, 2)]
     res = s2.results()
     torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([t_e2e], device='cuda')
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(time.perf_counter() - t0, pg)
     d2h = sum(p.numel() * 16 for p in ph) + 64
-    out = dict(value=cells * steps_total * ws / t_e2e, unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
+    out = dict(value=job_rate(cells, steps_total, ws, t_e2e), unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
                d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
                transmission=res['transmission'], cw_rel_change=res['cw_rel_change'])
     del s2
@@ -355,12 +367,8 @@ def ours_arm(args):
     ck = clocks.stop()
     launches = solve.launches - l0
     ms_a = ev[0].elapsed_time(ev[1])
-    ms = ms_a + ev[1].elapsed_time(ev[2])
-    if pg:
-        t = torch.tensor([ms], device='cuda')
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = cells * K * ws / (ms * 1e-3)
+    ms = max_over_ranks(ms_a + ev[1].elapsed_time(ev[2]), pg)
+    value = job_rate(cells, K, ws, ms * 1e-3)
     # algorithmic bytes of the whole mix: 72 B per cell update (6 fields R+W, 3 ce + 3 D
     # read), +12 B (E re-read) +16 B per accumulated component (complex float32 R+W) on
     # window steps, +20 B per |E|^2 accumulation pass

@@ -182,7 +182,7 @@ def run_e2e(spec, steps_total, cells, ws, pg):
     return out
 
 
-def run_batched(plain_sample=16):
+def run_batched(plain_sample=16, count=256):
     """Config 2: the 256-instance uneven 2D TE/TM sweep (4000 steps each).
 
     plain   instances one at a time through the single-grid engine (the drop-in
@@ -196,7 +196,7 @@ def run_batched(plain_sample=16):
     from lens_sensor_b200 import batch2d as B
     from lens_sensor_b200 import engine as E
     from lens_sensor_b200.workloads import config2
-    specs, steps = config2()
+    specs, steps = config2(count=count)
     ev = lambda: torch.cuda.Event(enable_timing=True)
     sw = B.Sweep(specs, steps, 'f32')
     tuned = sw.autotune()
@@ -243,7 +243,7 @@ def run_batched(plain_sample=16):
     plain = pc * steps / t_p
     f32 = cells * steps / t_b
     f16 = cells * steps / t_h
-    return dict(workload='config2: 256 uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
+    return dict(workload=f'config2: {len(specs)} uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
                          '12-cell CPML, 4000 steps, seeded tear-film / lipid / bead sweep',
                 unit=UNIT, cells_total=cells, steps=steps, plain=plain,
                 plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time',
@@ -391,7 +391,7 @@ def ours_arm(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(spec, steps_total, cells, ws, pg)
-    batched = run_batched() if (ws == 1 and not args.no_batch) else None
+    batched = run_batched(count=args.batch_instances) if (ws == 1 and not args.no_batch) else None
     stitch = run_stitch(args.stitch_windows) if (ws == 1 and not args.no_stitch) else None
     serving = run_serving(args.serve_requests) if (ws == 1 and not args.no_serve) else None
     cpu = None
@@ -430,6 +430,8 @@ def main():
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
     ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (config 2)')
     ap.add_argument('--no-stitch', action='store_true', help='skip the 3D stitch (config 3 windows)')
+    ap.add_argument('--batch-instances', type=int, default=256,
+                    help='instances of the config-2 sweep (fewer: a small case for profiling)')
     ap.add_argument('--stitch-windows', type=int, default=3, help='stitch windows (0: all 19 of config 3)')
     ap.add_argument('--no-serve', action='store_true', help='skip the serving stream (config 4)')
     ap.add_argument('--serve-requests', type=int, default=32, help='requests of the config-4 stream')

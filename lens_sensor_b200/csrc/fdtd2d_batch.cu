@@ -160,6 +160,21 @@ __device__ __forceinline__ void dft_node(const LensInst2D *g, const LensStepTabl
     }
 }
 
+// A zero the compiler cannot see through: the lean passes add it where the
+// general passes add a psi term, so both evaluate the same expression shapes.
+__device__ __forceinline__ float opaque_zero() {
+    float z;
+    asm volatile("mov.b32 %0, 0;" : "=f"(z));
+    return z;
+}
+
+// Rows [i0, i0 + RB) / columns [j0, j0 + VEC) of a thread clear of a profile's
+// psi strips ([lo, n - hi) is strip-free), of the faces and of the source rows:
+// such cells take the lean passes below (no per-cell tests).
+__device__ __forceinline__ bool clear_of(const LensProfile &p, int a, int b, int lo_min, int hi_max) {
+    return a >= max(p.lo, lo_min) && b <= min(p.n - p.hi, hi_max);
+}
+
 // psi update at profile entry m: psi = b*psi + c*d, stored; returns the new psi.
 __device__ __forceinline__ float psi_step(const LensProfile &pf, int m, float *q, float d) {
     const float p = __ldg(pf.b + m) * (*q) + __ldg(pf.c + m) * d;
@@ -193,6 +208,26 @@ __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const in
             ezn[r] = (in && j0 + VEC < ny) ? S::ld(ezp, o + VEC) : 0.f;
             f4_to(in ? S::ld4(hxp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hx[r]);
             f4_to(in ? S::ld4(hyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hy[r]);
+        }
+        if (clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1)) {
+            const float z = opaque_zero();  // lean: every Hx and Hy updates, no psi
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+                const int i = i0 + r;
+                const size_t o = (size_t)i * P + j0;
+                const float ki = __ldg(xh.ik + i);
+                float nhx[VEC], nhy[VEC];
+#pragma unroll
+                for (int c = 0; c < VEC; ++c) {
+                    const float d = (c + 1 < VEC ? ez[r][c + 1] : ezn[r]) - ez[r][c];
+                    nhx[c] = hx[r][c] - ch * (d * __ldg(yh.ik + j0 + c) + z);
+                    const float d2 = ez[r + 1][c] - ez[r][c];
+                    nhy[c] = hy[r][c] + ch * (d2 * ki + z);
+                }
+                S::st4(hxp, o, to_f4(nhx));
+                S::st4(hyp, o, to_f4(nhy));
+            }
+            return;
         }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
@@ -243,6 +278,23 @@ __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const in
         f4_to(in ? S::ld4(exp_, o) : make_float4(0.f, 0.f, 0.f, 0.f), ex[r]);
         exn[r] = (in && j0 + VEC < ny) ? S::ld(exp_, o + VEC) : 0.f;
         f4_to(in ? S::ld4(hzp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hz[r]);
+    }
+    if (clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1)) {
+        const float z = opaque_zero();  // lean: every Hz updates, no psi
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            const size_t o = (size_t)i * P + j0;
+            const float ki = __ldg(xh.ik + i);
+            float nhz[VEC];
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+                const float dyx = ey[r + 1][c] - ey[r][c], dxy = (c + 1 < VEC ? ex[r][c + 1] : exn[r]) - ex[r][c];
+                nhz[c] = hz[r][c] - ch * ((dyx * ki + z) - (dxy * __ldg(yh.ik + j0 + c) + z));
+            }
+            S::st4(hzp, o, to_f4(nhz));
+        }
+        return;
     }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {
@@ -302,6 +354,38 @@ __global__ void __launch_bounds__(256, 4)
             hxp1[r] = (in && j0 >= 1) ? S::ld(hxp, o - 1) : 0.f;       // Hx(i, j0-1)
             f4_to(in ? S::ld4(ezp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ez[r]);
         }
+        if (clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
+            (six < 0 || six + 1 < i0 || six >= i0 + RB)) {
+            const float z = opaque_zero();  // lean: interior cells, no psi, source or PEC
+            float *dft = reinterpret_cast<float *>(__ldg(reinterpret_cast<const unsigned long long *>(&tl.g->dft)));
+            const bool win = dft && n >= __ldg(&tl.g->dft_n0) && n < __ldg(&tl.g->dft_n1);
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+                const int i = i0 + r;
+                const size_t o = (size_t)i * P + j0;
+                const float ki = __ldg(xe.ik + i);
+                float c0[VEC], c1[VEC], v4[VEC];
+                f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(0, 2, i, j0, o))), c0);
+                f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(1, 2, i, j0, o))), c1);
+#pragma unroll
+                for (int c = 0; c < VEC; ++c) {
+                    const float dhy = hy[r + 1][c] - hy[r][c], dhx = hx[r][c] - (c > 0 ? hx[r][c - 1] : hxp1[r]);
+                    v4[c] = c0[c] * ez[r][c] + c1[c] * (dhy * ki + z - dhx * __ldg(ye.ik + j0 + c) - z);
+                }
+                S::st4(ezp, o, to_f4(v4));
+                if (win) {  // dft_node on the four cells
+                    const int k = n - tab.t0;
+                    const float pr = tab.pe[2 * k], pim = tab.pe[2 * k + 1];
+                    float4 *a = reinterpret_cast<float4 *>(dft + 2 * o);
+                    float4 s0 = a[0], s1 = a[1];
+                    s0.x += v4[0] * pr; s0.y += v4[0] * pim; s0.z += v4[1] * pr; s0.w += v4[1] * pim;
+                    s1.x += v4[2] * pr; s1.y += v4[2] * pim; s1.z += v4[3] * pr; s1.w += v4[3] * pim;
+                    a[0] = s0;
+                    a[1] = s1;
+                }
+            }
+            return;
+        }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
             const int i = i0 + r;
@@ -351,6 +435,39 @@ __global__ void __launch_bounds__(256, 4)
         f4_to(i < nx - 1 ? S::ld4(exp_, o) : make_float4(0.f, 0.f, 0.f, 0.f), ex[r]);
         hzp1[r] = (i < nx - 1 && j0 >= 1) ? S::ld(hzp, o - 1) : 0.f;   // Hz(i, j0-1)
         f4_to(i < nx ? S::ld4(eyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ey[r]);
+    }
+    if (clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
+        (six < 0 || six + 1 < i0 || six >= i0 + RB)) {
+        const float z = opaque_zero();  // lean: interior cells, no psi, source or PEC
+        const int nq = dax ? 4 : 2;
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            const size_t o = (size_t)i * P + j0;
+            float ax_[VEC], ay_[VEC], dx_[VEC], dy_[VEC];
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(0, nq, i, j0, o))), ax_);
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(1, nq, i, j0, o))), ay_);
+            f4_to(dax ? __ldg(reinterpret_cast<const float4 *>(g.crow(2, nq, i, j0, o))) : make_float4(1.f, 1.f, 1.f, 1.f),
+                  dx_);
+            f4_to(day ? __ldg(reinterpret_cast<const float4 *>(g.crow(3, nq, i, j0, o))) : make_float4(1.f, 1.f, 1.f, 1.f),
+                  dy_);
+            const float ki = __ldg(xe.ik + i);
+            float nex[VEC], ney[VEC];
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+                float e = ex[r][c];
+                if (dax) e = e * dx_[c];
+                const float d = hz[r + 1][c] - (c > 0 ? hz[r + 1][c - 1] : hzp1[r]);
+                nex[c] = e + ax_[c] * (d * __ldg(ye.ik + j0 + c) + z);
+                float e2 = ey[r][c];
+                if (day) e2 = e2 * dy_[c];
+                const float d2 = hz[r + 1][c] - hz[r][c];
+                ney[c] = e2 + (-ay_[c]) * (d2 * ki + z);
+            }
+            S::st4(exp_, o, to_f4(nex));
+            S::st4(eyp, o, to_f4(ney));
+        }
+        return;
     }
 #pragma unroll
     for (int r = 0; r < RB; ++r) {

@@ -170,7 +170,8 @@ __device__ __forceinline__ float opaque_zero() {
 
 // Rows [i0, i0 + RB) / columns [j0, j0 + VEC) of a thread clear of a profile's
 // psi strips ([lo, n - hi) is strip-free), of the faces and of the source rows:
-// such cells take the lean passes below (no per-cell tests).
+// a warp whose threads are all clear takes the lean passes below (no per-cell
+// tests); a warp with one thread at a face or in a strip takes the general pass.
 __device__ __forceinline__ bool clear_of(const LensProfile &p, int a, int b, int lo_min, int hi_max) {
     return a >= max(p.lo, lo_min) && b <= min(p.n - p.hi, hi_max);
 }
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const in
             f4_to(in ? S::ld4(hxp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hx[r]);
             f4_to(in ? S::ld4(hyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hy[r]);
         }
-        if (clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1)) {
+        if (__all_sync(__activemask(), clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1))) {
             const float z = opaque_zero();  // lean: every Hx and Hy updates, no psi
 #pragma unroll
             for (int r = 0; r < RB; ++r) {
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const in
         exn[r] = (in && j0 + VEC < ny) ? S::ld(exp_, o + VEC) : 0.f;
         f4_to(in ? S::ld4(hzp, o) : make_float4(0.f, 0.f, 0.f, 0.f), hz[r]);
     }
-    if (clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1)) {
+    if (__all_sync(__activemask(), clear_of(xh, i0, i0 + RB, 0, nx - 1) && clear_of(yh, j0, j0 + VEC, 0, ny - 1))) {
         const float z = opaque_zero();  // lean: every Hz updates, no psi
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
@@ -354,8 +355,8 @@ __global__ void __launch_bounds__(256, 4)
             hxp1[r] = (in && j0 >= 1) ? S::ld(hxp, o - 1) : 0.f;       // Hx(i, j0-1)
             f4_to(in ? S::ld4(ezp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ez[r]);
         }
-        if (clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
-            (six < 0 || six + 1 < i0 || six >= i0 + RB)) {
+        if (__all_sync(__activemask(), clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
+                                           (six < 0 || six + 1 < i0 || six >= i0 + RB))) {
             const float z = opaque_zero();  // lean: interior cells, no psi, source or PEC
             float *dft = reinterpret_cast<float *>(__ldg(reinterpret_cast<const unsigned long long *>(&tl.g->dft)));
             const bool win = dft && n >= __ldg(&tl.g->dft_n0) && n < __ldg(&tl.g->dft_n1);
@@ -436,8 +437,8 @@ __global__ void __launch_bounds__(256, 4)
         hzp1[r] = (i < nx - 1 && j0 >= 1) ? S::ld(hzp, o - 1) : 0.f;   // Hz(i, j0-1)
         f4_to(i < nx ? S::ld4(eyp, o) : make_float4(0.f, 0.f, 0.f, 0.f), ey[r]);
     }
-    if (clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
-        (six < 0 || six + 1 < i0 || six >= i0 + RB)) {
+    if (__all_sync(__activemask(), clear_of(xe, i0, i0 + RB, 1, nx - 1) && clear_of(ye, j0, j0 + VEC, 1, ny - 1) &&
+                                       (six < 0 || six + 1 < i0 || six >= i0 + RB))) {
         const float z = opaque_zero();  // lean: interior cells, no psi, source or PEC
         const int nq = dax ? 4 : 2;
 #pragma unroll

@@ -387,6 +387,38 @@ __global__ void __launch_bounds__(256, 4)
             }
             return;
         }
+        if (__all_sync(__activemask(), clear_of(xe, i0, i0 + RB, 1, nx - 1) &&
+                                           (six < 0 || six + 1 < i0 || six >= i0 + RB))) {
+            // rows clear of x strips, x faces and the source: the y tests only
+            const float z = opaque_zero();
+#pragma unroll
+            for (int r = 0; r < RB; ++r) {
+                const int i = i0 + r;
+                const size_t o = (size_t)i * P + j0;
+                const float ki = __ldg(xe.ik + i);
+                float c0[VEC], c1[VEC], v4[VEC];
+                f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(0, 2, i, j0, o))), c0);
+                f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(1, 2, i, j0, o))), c1);
+#pragma unroll
+                for (int c = 0; c < VEC; ++c) {
+                    const int j = j0 + c;
+                    float v = ez[r][c];
+                    if (j > 0 && j < ny - 1) {
+                        const float dhy = hy[r + 1][c] - hy[r][c], dhx = hx[r][c] - (c > 0 ? hx[r][c - 1] : hxp1[r]);
+                        float qy = z;
+                        const int sj = strip_of(j, ye.lo, ye.hi, ye.n);
+                        if (sj >= 0) qy = psi_step(ye, j, g.psi(3) + (size_t)i * wy + sj, dhx);
+                        v = c0[c] * v + c1[c] * (dhy * ki + z - dhx * __ldg(ye.ik + j) - qy);
+                    }
+                    if ((pec2 && j == 0) || (pec3 && j == ny - 1)) v = 0.f;
+                    if (j >= ny) v = 0.f;
+                    v4[c] = v;
+                    if (j < ny) dft_node(tl.g, tab, n, o + c, v);
+                }
+                S::st4(ezp, o, to_f4(v4));
+            }
+            return;
+        }
 #pragma unroll
         for (int r = 0; r < RB; ++r) {
             const int i = i0 + r;
@@ -464,6 +496,54 @@ __global__ void __launch_bounds__(256, 4)
                 if (day) e2 = e2 * dy_[c];
                 const float d2 = hz[r + 1][c] - hz[r][c];
                 ney[c] = e2 + (-ay_[c]) * (d2 * ki + z);
+            }
+            S::st4(exp_, o, to_f4(nex));
+            S::st4(eyp, o, to_f4(ney));
+        }
+        return;
+    }
+    if (__all_sync(__activemask(), clear_of(xe, i0, i0 + RB, 1, nx - 1) &&
+                                       (six < 0 || six + 1 < i0 || six >= i0 + RB))) {
+        // rows clear of x strips, x faces and the source: the y tests only
+        const float z = opaque_zero();
+        const int nq = dax ? 4 : 2;
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            const int i = i0 + r;
+            const size_t o = (size_t)i * P + j0;
+            float ax_[VEC], ay_[VEC], dx_[VEC], dy_[VEC];
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(0, nq, i, j0, o))), ax_);
+            f4_to(__ldg(reinterpret_cast<const float4 *>(g.crow(1, nq, i, j0, o))), ay_);
+            f4_to(dax ? __ldg(reinterpret_cast<const float4 *>(g.crow(2, nq, i, j0, o))) : make_float4(1.f, 1.f, 1.f, 1.f),
+                  dx_);
+            f4_to(day ? __ldg(reinterpret_cast<const float4 *>(g.crow(3, nq, i, j0, o))) : make_float4(1.f, 1.f, 1.f, 1.f),
+                  dy_);
+            const float ki = __ldg(xe.ik + i);
+            float nex[VEC], ney[VEC];
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+                const int j = j0 + c;
+                nex[c] = ex[r][c];
+                ney[c] = ey[r][c];
+                if (j < ny) {  // Ex at (i+1/2, j)
+                    float e = ex[r][c];
+                    if (dax) e = e * dx_[c];
+                    if (j > 0 && j < ny - 1) {
+                        const float d = hz[r + 1][c] - (c > 0 ? hz[r + 1][c - 1] : hzp1[r]);
+                        float p = z;
+                        const int sj = strip_of(j, ye.lo, ye.hi, ye.n);
+                        if (sj >= 0) p = psi_step(ye, j, g.psi(2) + (size_t)i * wy + sj, d);
+                        e = e + ax_[c] * (d * __ldg(ye.ik + j) + p);
+                    }
+                    if ((pec2 && j == 0) || (pec3 && j == ny - 1)) e = 0.f;
+                    nex[c] = e;
+                }
+                if (j < ny - 1) {  // Ey at (i, j+1/2)
+                    float e = ey[r][c];
+                    if (day) e = e * dy_[c];
+                    const float d = hz[r + 1][c] - hz[r][c];
+                    ney[c] = e + (-ay_[c]) * (d * ki + z);
+                }
             }
             S::st4(exp_, o, to_f4(nex));
             S::st4(eyp, o, to_f4(ney));

@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark: Yee cell-updates/s of the 3D CPML time-stepping hot path.
 
-Workload (config 1): 3D TM planar waveguide 480 x 192 x 256 cells @ 30 nm,
+Workload: 3D TM planar waveguide 480 x 192 x 256 cells @ 30 nm,
 float32 fields, 10-cell CPML, absorbing aqueous (1.333+0.001i), two seeded
 polystyrene beads, 4000-step CW schedule with Ex/Ey/Ez phasors.  One "step" is
 one leapfrog time step over the whole grid.  The K timed steps sample the
@@ -32,7 +32,7 @@ import numpy as np  # noqa: E402
 
 METRIC = 'yee_cell_updates_per_s'
 UNIT = 'cell-updates/s'
-WORKLOAD = ('config1: 3D TM planar waveguide 480x192x256 @ 30 nm, fp32, 10-cell CPML, '
+WORKLOAD = ('waveguide3d_tm: 3D TM planar waveguide 480x192x256 @ 30 nm, fp32, 10-cell CPML, '
             'lossy aqueous 1.333+0.001i, 2 seeded PS beads, 4000-step CW schedule, Ex/Ey/Ez phasors')
 
 
@@ -126,7 +126,7 @@ def cpu_baseline(spec, steps=8):
         g.box_e2(*box)
     dt = time.perf_counter() - t0
     cells = spec.nx * spec.ny * spec.nz
-    return cells * steps / dt, dict(sample=f'{steps} consecutive full-grid steps of the config-1 3D CPML '
+    return cells * steps / dt, dict(sample=f'{steps} consecutive full-grid steps of the 480x192x256 3D CPML '
                                            f'step + detector box sums on the NumPy oracle (float32), '
                                            f'{dt:.1f} s', cores=1)
 
@@ -143,8 +143,8 @@ def reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    from lens_sensor_b200.workloads import config1
-    spec, steps_total = config1()
+    from lens_sensor_b200.workloads import waveguide3d_tm
+    spec, steps_total = waveguide3d_tm()
     # each step: one full-grid oracle step; bounded so the arm ends within minutes
     k = max(1, min(args.steps, 12))
     value, info = cpu_baseline(spec, steps=k)
@@ -195,8 +195,8 @@ def run_batched(plain_sample=16, count=256):
     import torch
     from lens_sensor_b200 import batch2d as B
     from lens_sensor_b200 import engine as E
-    from lens_sensor_b200.workloads import config2
-    specs, steps = config2(count=count)
+    from lens_sensor_b200.workloads import sweep2d
+    specs, steps = sweep2d(count=count)
     ev = lambda: torch.cuda.Event(enable_timing=True)
     sw = B.Sweep(specs, steps, 'f32')
     tuned = sw.autotune()
@@ -243,7 +243,7 @@ def run_batched(plain_sample=16, count=256):
     plain = pc * steps / t_p
     f32 = cells * steps / t_b
     f16 = cells * steps / t_h
-    return dict(workload=f'config2: {len(specs)} uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
+    return dict(workload=f'sweep2d: {len(specs)} uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
                          '12-cell CPML, 4000 steps, seeded tear-film / lipid / bead sweep',
                 unit=UNIT, cells_total=cells, steps=steps, plain=plain,
                 plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time',
@@ -265,9 +265,9 @@ def run_stitch(windows=3):
     import torch
     from lens_sensor_b200 import engine as E
     from lens_sensor_b200.stitch3d import StitchSolve
-    from lens_sensor_b200.workloads import config3
+    from lens_sensor_b200.workloads import stitch3d_plan
     windows = 19 if windows <= 0 else windows
-    pl = config3(nx_full=480 + (windows - 1) * 440)
+    pl = stitch3d_plan(nx_full=480 + (windows - 1) * 440)
     Ef = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.complex64)
     Ia = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.float32)
 
@@ -287,7 +287,7 @@ def run_stitch(windows=3):
     T = job.transmission()
     del job
     torch.cuda.empty_cache()
-    return dict(workload=f'config3: 3D stitch, {pl.n_win} windows of {pl.Nx_win} x {pl.Ny} x {pl.Nz} @ 30 nm '
+    return dict(workload=f'stitch3d_plan: 3D stitch, {pl.n_win} windows of {pl.Nx_win} x {pl.Ny} x {pl.Nz} @ 30 nm '
                          f'(+{pl.EXT}-cell absorber on interior windows), {pl.O}-cell overlap, '
                          f'{pl.steps_win} steps per window; {pl.Nx_full} cells = {pl.lx_um:.1f} um',
                 unit=UNIT, value=cu / wall, wall_s=wall, cell_updates=cu, windows=pl.n_win,
@@ -303,13 +303,13 @@ def run_serving(count=32, seed=4):
     minus arrival."""
     import torch
     from lens_sensor_b200.serve import Request, Server, summary
-    from lens_sensor_b200.workloads import config4
-    reqs = [Request(i, k, sp, n, t) for i, (k, sp, n, t) in enumerate(config4(seed=seed, count=count))]
+    from lens_sensor_b200.workloads import serving_stream
+    reqs = [Request(i, k, sp, n, t) for i, (k, sp, n, t) in enumerate(serving_stream(seed=seed, count=count))]
     srv = Server()
     done = srv.run(reqs)
     out = summary(done)
     torch.cuda.empty_cache()
-    out.update(workload=f'config4: first {count} requests of the seeded Poisson stream (50 req/s): '
+    out.update(workload=f'serving_stream: first {count} requests of the seeded Poisson stream (50 req/s): '
                         f'{sum(r.kind == "2d" for r in reqs)} 2D, {sum(r.kind == "3d" for r in reqs)} 3D, '
                         f'{sum(r.kind == "stitch" for r in reqs)} stitch',
                unit=UNIT, value=out['cell_updates_per_s'], budget_bytes=srv.budget, slots3d=srv.slots3d,
@@ -329,8 +329,8 @@ def ours_arm(args):
                                 device_id=torch.device('cuda', local))
         pg = dist
     from lens_sensor_b200.solver3d import Solve3D
-    from lens_sensor_b200.workloads import config1
-    spec, steps_total = config1()
+    from lens_sensor_b200.workloads import waveguide3d_tm
+    spec, steps_total = waveguide3d_tm()
     cells = spec.nx * spec.ny * spec.nz
     solve = Solve3D(spec, steps_total, comps=(0, 1, 2))
     W = max(3, args.warmup)
@@ -381,7 +381,7 @@ def ours_arm(args):
     achieved = 72.0 * cells / t_launch / 1e9
     traffic = None
     try:
-        with open(os.path.join(ROOT, 'profiles', 'yee3d_config1_traffic.json')) as f:
+        with open(os.path.join(ROOT, 'profiles', 'yee3d_waveguide3d_tm_traffic.json')) as f:
             traffic = json.load(f).get('bytes_per_launch')
     except Exception:
         pass
@@ -428,13 +428,13 @@ def main():
     ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
-    ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (config 2)')
-    ap.add_argument('--no-stitch', action='store_true', help='skip the 3D stitch (config 3 windows)')
+    ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (sweep2d)')
+    ap.add_argument('--no-stitch', action='store_true', help='skip the 3D stitch (stitch3d_plan windows)')
     ap.add_argument('--batch-instances', type=int, default=256,
-                    help='instances of the config-2 sweep (fewer: a small case for profiling)')
-    ap.add_argument('--stitch-windows', type=int, default=3, help='stitch windows (0: all 19 of config 3)')
-    ap.add_argument('--no-serve', action='store_true', help='skip the serving stream (config 4)')
-    ap.add_argument('--serve-requests', type=int, default=32, help='requests of the config-4 stream')
+                    help='instances of the sweep2d sweep (fewer: a small case for profiling)')
+    ap.add_argument('--stitch-windows', type=int, default=3, help='stitch windows (0: all 19 of stitch3d_plan)')
+    ap.add_argument('--no-serve', action='store_true', help='skip the serving stream (serving_stream)')
+    ap.add_argument('--serve-requests', type=int, default=32, help='requests of the serving stream')
     args = ap.parse_args()
     if args.impl == 'reference':
         reference_arm(args)

@@ -1,14 +1,14 @@
 """The benchmark workloads, built from seeded parameters.
 
-config 0  2D TE planar waveguide 1600 x 480 @ 25 nm, 12-cell CPML, 6000 steps,
-          CW ramped over 20 periods, one bead (n 1.59, r 0.4 um) at a seeded x.
-config 1  3D TM (Ey) planar waveguide 480 x 192 x 256 @ 30 nm, 10-cell CPML,
-          4000 steps, absorbing aqueous 1.333+0.001i, two seeded beads
-          (r ~ U(0.3, 0.6) um), phasors of Ex/Ey/Ez.
-config 2  256 uneven 2D TE/TM solves (tear-film thickness / bead sweep).
-config 3  3D stitch of a 240 um waveguide: windows of 480 x 192 x 256 @ 30 nm,
-          40-cell overlap (19 windows by the reference's window formula).
-config 4  serving stream: Poisson arrivals of mixed 2D / 3D / stitch requests.
+planar2d_te     2D TE planar waveguide 1600 x 480 @ 25 nm, 12-cell CPML, 6000 steps,
+                CW ramped over 20 periods, one bead (n 1.59, r 0.4 um) at a seeded x.
+waveguide3d_tm  3D TM (Ey) planar waveguide 480 x 192 x 256 @ 30 nm, 10-cell CPML,
+                4000 steps, absorbing aqueous 1.333+0.001i, two seeded beads
+                (r ~ U(0.3, 0.6) um), phasors of Ex/Ey/Ez.
+sweep2d         256 uneven 2D TE/TM solves (tear-film thickness / bead sweep).
+stitch3d_plan   3D stitch of a 240 um waveguide: windows of 480 x 192 x 256 @ 30 nm,
+                40-cell overlap (19 windows by the reference's window formula).
+serving_stream  serving stream: Poisson arrivals of mixed 2D / 3D / stitch requests.
 
 Layer stack (core downward): PMMA core n=1.49 (2 um) / aqueous n=1.333
 (1.5 um) / mucin n=1.34 (0.5 um) / cornea n=1.376 substrate; air above.  In 3D
@@ -23,7 +23,7 @@ from .stitch3d import StitchPlan
 N_PMMA, N_AQ, N_MUCIN, N_CORNEA, N_PS, N_LIPID = 1.49, 1.333, 1.34, 1.376, 1.59, 1.48
 
 
-def config0(seed=0):
+def planar2d_te(seed=0):
     rng = np.random.default_rng(seed)
     st = Stack(N_PMMA, 2.0, [(1.5, N_AQ), (0.5, N_MUCIN)], N_CORNEA)
     x = float(rng.uniform(15.0, 30.0))
@@ -31,7 +31,7 @@ def config0(seed=0):
                   ramp_periods=20.0), 6000
 
 
-def config1(seed=1):
+def waveguide3d_tm(seed=1):
     rng = np.random.default_rng(seed)
     r = rng.uniform(0.3, 0.6, 2)
     beads = [Sphere(float(rng.uniform(4.5, 7.0)), float(2 * r[0]), N_PS, -float(r[0]), float(rng.uniform(-2, 2))),
@@ -40,7 +40,7 @@ def config1(seed=1):
     return Spec3D('p', 480, 192, 256, 30.0, st, 3.0, beads, npml=10), 4000
 
 
-def config2(seed=2, count=256):
+def sweep2d(seed=2, count=256):
     """256 uneven 2D solves: aqueous U(0.5, 5) um, mucin U(0.2, 1), lipid
     U(0, 0.1) (n 1.48), bead r U(0.2, 0.8) um at a random x; widths U{600..2400},
     heights U{300..560} cells at 25 nm; TE and TM alternate; 4000 steps each."""
@@ -69,10 +69,10 @@ def _stack3d(rng, ly_um, air_um=0.5):
     return st, ly_um - t_wg - air_um
 
 
-def config3(seed=3, nx_full=8000, nx_win=480, overlap=40, ny=192, nz=256):
+def stitch3d_plan(seed=3, nx_full=8000, nx_win=480, overlap=40, ny=192, nz=256):
     """3D stitch of a 240 um planar waveguide at 30 nm (nx_full = 8000 cells) in
     windows of nx_win x ny x nz cells overlapping by `overlap` cells (slide
-    nx_win - overlap), config-1 stack (2 um core, absorbing aqueous), two seeded
+    nx_win - overlap), waveguide3d_tm stack (2 um core, absorbing aqueous), two seeded
     beads.  The reference's window count ceil((8000 - 480) / 440) + 1 = 19, the
     last window flush with the domain end (fdtd3d_core.py:1382-1386)."""
     rng = np.random.default_rng(seed)
@@ -88,15 +88,15 @@ def config3(seed=3, nx_full=8000, nx_win=480, overlap=40, ny=192, nz=256):
                       beads=beads, waist_um=1.5, waist_z_um=1.5)
 
 
-def config4(seed=4, count=64, rate=50.0):
+def serving_stream(seed=4, count=64, rate=50.0):
     """Serving stream: Poisson arrivals (mean `rate` req/s, seeded) of
-    70 % 2D TE/TM solves of the config-2 size distribution (4000 steps),
+    70 % 2D TE/TM solves of the sweep2d size distribution (4000 steps),
     25 % 3D solves of 256-512 x 128-192 x 160-256 cells at 30 nm with 2000-4000
     steps and 5 % 3D stitch jobs of 4-10 windows (windows of 256-384 x 128-160 x
     160-192 cells, 40-cell overlap).  Returns [(kind, spec, steps, arrival)]."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, count))
-    specs2d, steps2d = config2(seed + 100, count)
+    specs2d, steps2d = sweep2d(seed + 100, count)
     out = []
     for q in range(count):
         u = rng.uniform()

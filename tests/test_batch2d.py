@@ -53,12 +53,12 @@ def test_plan_of_uneven_instances():
 
 def test_row_types_are_exact_rows_of_the_coefficients():
     """The row form (LensInst2D.rtype / ctab) holds each typed row's bytes exactly
-    and covers the layered rows of config-2 instances (TE, lossless and lossy TM)."""
+    and covers the layered rows of sweep2d instances (TE, lossless and lossy TM)."""
     from lens_sensor_b200 import batch2d as B
     from lens_sensor_b200 import engine as E
     from lens_sensor_b200.geometry import build_2d
-    from lens_sensor_b200.workloads import config2
-    specs, _ = config2(count=4)
+    from lens_sensor_b200.workloads import sweep2d
+    specs, _ = sweep2d(count=4)
     for sp in specs:
         g = build_2d(sp)
         cn = ['ce_e', 'ce_h'] if sp.pol == 's' else ['ca_x', 'ca_y'] + (['da_x', 'da_y'] if g.get('da_x') is not None else [])
@@ -78,8 +78,8 @@ def test_row_types_are_exact_rows_of_the_coefficients():
 
 
 def _small_sweep():
-    from lens_sensor_b200.workloads import config2
-    specs, _ = config2(count=6)
+    from lens_sensor_b200.workloads import sweep2d
+    specs, _ = sweep2d(count=6)
     return [replace(sp, nx=min(sp.nx, 150 + 23 * q), ny=min(sp.ny, 300 - 11 * q)) for q, sp in enumerate(specs)]
 
 

@@ -21,8 +21,8 @@ from lens_sensor_b200.stitch3d import StitchPlan
 TOL_SCALAR = 1e-9
 
 
-def test_config4_stream_is_seeded_poisson_mix():
-    a, b = W.config4(seed=7, count=200), W.config4(seed=7, count=200)
+def test_serving_stream_is_seeded_poisson_mix():
+    a, b = W.serving_stream(seed=7, count=200), W.serving_stream(seed=7, count=200)
     assert [(k, s, t) for k, _, s, t in a] == [(k, s, t) for k, _, s, t in b]
     t = np.array([x[3] for x in a])
     assert np.all(np.diff(t) > 0)

@@ -22,9 +22,9 @@ def test_noalloc_matches_batched_step_twice():
     import torch
     from lens_sensor_b200 import _native as N
     from lens_sensor_b200 import batch2d as B
-    from lens_sensor_b200.workloads import config2
+    from lens_sensor_b200.workloads import sweep2d
     lib = N.load()
-    specs, _ = config2(count=5)
+    specs, _ = sweep2d(count=5)
     specs = [replace(sp, nx=min(sp.nx, 140 + 19 * q), ny=min(sp.ny, 260 - 9 * q)) for q, sp in enumerate(specs)]
     steps = 200
     ref = B.Sweep(specs, steps, 'f32', by=4)
@@ -49,9 +49,9 @@ def test_noalloc_rejects_oversized_batches():
     import torch
     from lens_sensor_b200 import _native as N
     from lens_sensor_b200 import batch2d as B
-    from lens_sensor_b200.workloads import config2
+    from lens_sensor_b200.workloads import sweep2d
     lib = N.load()
-    specs, _ = config2(count=1)
+    specs, _ = sweep2d(count=1)
     sw = B.Sweep([replace(specs[0], nx=120, ny=100)], 10, 'f32')
     many = (N.Inst2D * 513)(*([sw.insts[0].s] * 513))              # more than 512 instances
     st = lib.lens_batch2d_step_noalloc(many, 513, N.F32, 4, ctypes.byref(sw.table.s), 0, 1, None)

@@ -504,6 +504,7 @@ __device__ __forceinline__ PX px_at(const K3 &g, int i) {
 }
 
 constexpr int MAXCH = 96;
+constexpr int MAXPERM = 4096;  // CPML tiles that can be reordered (more: the plain order)
 // Work of one step: every (z-tile, y-tile, x-chunk).  The CPML tiles (outside
 // the lean core [lo, hi): CPML-free, interior) come first, the longer CTAs
 // starting early; within each group the order is chunk, y-tile, z-tile (z
@@ -513,6 +514,8 @@ struct Work {
     int lo[3], hi[3];  // lean core: z-tiles, y-tiles, chunks
     int plo[3], phi[3];  // z-tiles, y-tiles, chunks without z / y / x CPML psi
     int x[MAXCH + 1];  // chunk c covers planes [x[c], x[c+1])
+    int nperm;                    // CTAs [0, nperm) take tile perm[id] (0: the order above)
+    unsigned short perm[MAXPERM];  // CPML tiles ordered by the pass they run, most axes first
 };
 
 // Tile of CTA `id` (see Work); returns true for a lean tile.
@@ -1087,7 +1090,7 @@ __global__ void __launch_bounds__(NW3 * 32, 2)
     yee3d(const __grid_constant__ EMaps tm, const K3 g, const LensStepTable tab, const LensEpi3D ep, int n,
           int epi, const __grid_constant__ Work wk) {
     int tz, ty, c;
-    const bool lean = work_tile(wk, blockIdx.x, tz, ty, c);
+    const bool lean = work_tile(wk, blockIdx.x < wk.nperm ? (int)wk.perm[blockIdx.x] : (int)blockIdx.x, tz, ty, c);
     extern __shared__ __align__(128) unsigned char smem[];
     const int k0 = tz * TK, j0 = ty * TJ, x0 = wk.x[c], x1 = wk.x[c + 1];
     if (lean) {
@@ -1473,6 +1476,28 @@ Work make_work(const LensGrid3D *g, int slots) {
     wk.lo[0] = z0; wk.hi[0] = z1;
     wk.lo[1] = y0; wk.hi[1] = y1;
     wk.lo[2] = c0; wk.hi[2] = c1;
+    // CPML tiles grouped by the specialised pass they run (tiles of more axes first), so
+    // that CTAs resident together mostly share their code
+    const int nlean = (z1 - z0) * (y1 - y0) * (c1 - c0);
+    const int nstrip = ntz * nty * nc - nlean;
+    wk.nperm = 0;
+    if (nstrip > 0 && nstrip <= MAXPERM) {
+        unsigned char mk[MAXPERM];
+        for (int id = 0; id < nstrip; ++id) {
+            int tz, ty, c;
+            work_tile(wk, id, tz, ty, c);
+            const unsigned m = ((tz < wk.plo[0] || tz >= wk.phi[0]) ? AXZ : 0u) |
+                               ((ty < wk.plo[1] || ty >= wk.phi[1]) ? AXY : 0u) |
+                               ((c < wk.plo[2] || c >= wk.phi[2]) ? AXX : 0u);
+            const int axes = (m & 1u) + ((m >> 1) & 1u) + ((m >> 2) & 1u);
+            mk[id] = (unsigned char)((3 - axes) * 8 + (7 - m));  // sort key: more axes first, then the mask
+        }
+        int n = 0;
+        for (int key = 0; key < 32; ++key)
+            for (int id = 0; id < nstrip; ++id)
+                if (mk[id] == key) wk.perm[n++] = (unsigned short)id;
+        wk.nperm = n;
+    }
     return wk;
 }
 

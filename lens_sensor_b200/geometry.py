@@ -463,11 +463,15 @@ class Spec3D:
 
 
 def _stagger(a, ax):
+    """Mean of neighbouring nodes along ax (0.5 * (a[i] + a[i+1])), in a's precision,
+    returned as float32."""
     lo = [slice(None)] * 3
     hi = [slice(None)] * 3
     lo[ax] = slice(None, -1)
     hi[ax] = slice(1, None)
-    return (F32(0.5) * (a[tuple(lo)] + a[tuple(hi)])).astype(F32)
+    out = a[tuple(lo)] + a[tuple(hi)]
+    out *= out.dtype.type(0.5)
+    return out.astype(F32, copy=False)
 
 
 def build_3d(sp: Spec3D):
@@ -567,8 +571,13 @@ def build_3d(sp: Spec3D):
     ce = [_stagger(inv, 0), None, _stagger(inv, 2)]
     hinv = (dt / (EPS0 * dx) / hcols).astype(F32)
     cy = np.ascontiguousarray(hinv[T].transpose(0, 2, 1))       # every column type overrides ce_y
+    # the loss factor (1 + D) / 2 at the staggered positions of each axis, made once
+    half_d = [None, None, None]
     if lossy:
-        cy *= _stagger(F32(0.5) * (1 + D), 1)
+        hD = F32(0.5) * (1 + D)
+        half_d = [_stagger(hD, ax) for ax in range(3)]
+        del hD
+        cy *= half_d[1]
     ce[1] = cy
     c = dt / (EPS0 * dx)
     for bp in patches:                                            # Farjadpour tensor at the bead edge
@@ -606,7 +615,7 @@ def build_3d(sp: Spec3D):
             blk = tgt[sl].astype(np.float64)
             val = c * np.broadcast_to(inv_t3, f.shape)
             if lossy:
-                val = val * _stagger(F32(0.5) * (1 + D), ax)[sl].astype(np.float64)
+                val = val * half_d[ax][sl].astype(np.float64)
             blk[sel] = val[sel]
             tgt[sl] = blk.astype(F32)
     da = None if not lossy else tuple(_stagger(D, ax) for ax in range(3))

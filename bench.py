@@ -168,14 +168,25 @@ def run_e2e(spec, steps_total, cells, ws, pg):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    torch.cuda.synchronize()          # the uploads are synchronous already; marks the phase end
+    t1 = time.perf_counter()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    s2.stage_host((0, 1, 2))          # the read-back's host buffers are made while the device steps
     s2.run()
-    ph = [s2.phasor(c).cpu() for c in (0, 1, 2)]
+    ev[1].record()
+    s2.phasors_host((0, 1, 2))
     res = s2.results()
     torch.cuda.synchronize()
-    t_e2e = max_over_ranks(time.perf_counter() - t0, pg)
-    d2h = sum(p.numel() * 16 for p in ph) + 64
+    t3 = time.perf_counter()
+    t_e2e = max_over_ranks(t3 - t0, pg)
+    d2h = s2.d2h_bytes + 64
+    t_run = ev[0].elapsed_time(ev[1]) * 1e-3
+    phases = dict(setup_host=s2.t_setup_host, setup_device=t1 - t0 - s2.t_setup_host, run_device=t_run,
+                  after_run=t3 - t1 - t_run)
     out = dict(value=job_rate(cells, steps_total, ws, t_e2e), unit=UNIT, h2d_bytes_per_step=s2.h2d_bytes / steps_total,
                d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
+               phase_seconds={k: round(v, 4) for k, v in phases.items()},
                transmission=res['transmission'], cw_rel_change=res['cw_rel_change'])
     del s2
     torch.cuda.empty_cache()

@@ -18,6 +18,8 @@ entry facet, ...); beads are local patches.  Coefficient volumes are expanded
 from per-type columns, then the bead boxes are patched.
 """
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import List, Optional, Tuple
 
@@ -462,16 +464,54 @@ class Spec3D:
         return C0 / (self.lam_nm * 1e-9)
 
 
+HOST_THREADS = max(1, min(16, len(os.sched_getaffinity(0))))
+
+
+def _slabs(n, fn, min_rows=16):
+    """fn(i0, i1) over contiguous slabs of [0, n) on up to HOST_THREADS threads
+    (the volume builders are NumPy element-wise work, which runs without the GIL)."""
+    k = min(HOST_THREADS, n // min_rows)
+    if k <= 1:
+        fn(0, n)
+        return
+    b = [n * q // k for q in range(k + 1)]
+    with ThreadPoolExecutor(k) as ex:
+        for f in [ex.submit(fn, b[q], b[q + 1]) for q in range(k)]:
+            f.result()
+
+
 def _stagger(a, ax):
-    """Mean of neighbouring nodes along ax (0.5 * (a[i] + a[i+1])), in a's precision,
+    """Mean of neighbouring nodes along ax, 0.5 * (a[i] + a[i+1]) in a's precision,
     returned as float32."""
-    lo = [slice(None)] * 3
-    hi = [slice(None)] * 3
-    lo[ax] = slice(None, -1)
-    hi[ax] = slice(1, None)
-    out = a[tuple(lo)] + a[tuple(hi)]
-    out *= out.dtype.type(0.5)
+    shp = list(a.shape)
+    shp[ax] -= 1
+    out = np.empty(shp, dtype=a.dtype)
+    half = a.dtype.type(0.5)
+
+    def part(i0, i1):
+        if ax == 0:
+            lo, hi = a[i0:i1], a[i0 + 1:i1 + 1]
+        else:
+            s_lo, s_hi = [slice(i0, i1), slice(None), slice(None)], [slice(i0, i1), slice(None), slice(None)]
+            s_lo[ax], s_hi[ax] = slice(None, -1), slice(1, None)
+            lo, hi = a[tuple(s_lo)], a[tuple(s_hi)]
+        o = out[i0:i1]
+        np.add(lo, hi, out=o)
+        o *= half
+    _slabs(shp[0], part)
     return out.astype(F32, copy=False)
+
+
+def _columns_volume(T, tab):
+    """(Nx, Ny, Nz) float32 volume whose (i, :, k) column is tab[T[i, k]]
+    (tab: (ntype, Ny) float32, one row per column type)."""
+    Nx, Nz = T.shape
+    out = np.empty((Nx, tab.shape[1], Nz), F32)
+
+    def part(i0, i1):
+        out[i0:i1] = tab[T[i0:i1]].transpose(0, 2, 1)
+    _slabs(Nx, part)
+    return out
 
 
 def build_3d(sp: Spec3D):
@@ -534,17 +574,18 @@ def build_3d(sp: Spec3D):
         inv /= (1 + a)
         return inv, ((1 - a) / (1 + a)).astype(F32)
 
-    # volumes from the per-type columns
+    # volumes from the per-type columns (every column type of T has a column)
     inv_t = {t: inv_damp(c) for t, c in cols_node.items()}
-    inv = np.empty((Nx, Nz, Ny), F32)
-    D = np.empty((Nx, Nz, Ny), F32) if lossy else None
+    assert set(np.unique(T).tolist()) <= set(inv_t), (np.unique(T), sorted(inv_t))
+    nty = max(inv_t) + 1
+    tab_inv = np.zeros((nty, Ny), F32)
+    tab_d = np.zeros((nty, Ny), F32)
     for t, (iv, dv) in inv_t.items():
-        sel = T == t
-        inv[sel] = iv
+        tab_inv[t] = iv
         if lossy:
-            D[sel] = dv
-    inv = np.ascontiguousarray(inv.transpose(0, 2, 1))
-    D = np.ascontiguousarray(D.transpose(0, 2, 1)) if lossy else None
+            tab_d[t] = dv
+    inv = _columns_volume(T, tab_inv)
+    D = _columns_volume(T, tab_d) if lossy else None
     # beads: blended eps in their boxes, background kept for the tensor
     patches = []
     for bd in sp.beads:
@@ -570,11 +611,17 @@ def build_3d(sp: Spec3D):
             D[i0:i1, j0:j1, k0:k1] = dv
     ce = [_stagger(inv, 0), None, _stagger(inv, 2)]
     hinv = (dt / (EPS0 * dx) / hcols).astype(F32)
-    cy = np.ascontiguousarray(hinv[T].transpose(0, 2, 1))       # every column type overrides ce_y
+    cy = _columns_volume(T, hinv)                                 # every column type overrides ce_y
     # the loss factor (1 + D) / 2 at the staggered positions of each axis, made once
     half_d = [None, None, None]
     if lossy:
-        hD = F32(0.5) * (1 + D)
+        hD = np.empty_like(D)
+
+        def half_part(i0, i1):
+            h = hD[i0:i1]
+            np.add(D[i0:i1], F32(1), out=h)
+            h *= F32(0.5)
+        _slabs(Nx, half_part)
         half_d = [_stagger(hD, ax) for ax in range(3)]
         del hD
         cy *= half_d[1]

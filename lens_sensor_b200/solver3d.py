@@ -12,12 +12,17 @@ results.  This is the engine behind fdtd3d_core.run_3d's full-domain CPML path
 """
 import math
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
 
 from . import engine as E
 from .geometry import Spec3D, build_3d
+
+
+# one worker that prepares host read-back buffers while the device steps
+_HOST_POOL = ThreadPoolExecutor(1, thread_name_prefix='lens-host-stage')
 
 
 def guard_in_plane(i_in, src_ix, n_max, margin=5):
@@ -120,6 +125,48 @@ class Solve3D:
         """Complex CW amplitude (2/N) sum F e^{-i w t} (fdtd3d_core.py:1271)."""
         comp = self.spec.src_comp if comp is None else comp
         return (2.0 / self.n_acc) * self.epi.phasor(comp)
+
+    def _host_buffers(self, comps):
+        """Host complex64 destinations (nx, ny, pitch) of the phasor read-back,
+        written once so that their pages are resident before the copy."""
+        out = {}
+        for c in comps:
+            a = np.empty(tuple(self.epi.dft[c].shape[:3]), np.complex64)
+            a.view(np.float32).fill(0.0)
+            out[c] = a
+        return out
+
+    def stage_host(self, comps=None):
+        """Prepare the host destinations of phasors_host(comps) on a background
+        thread, so that it overlaps the stepping (call before run(); the
+        launches run without the GIL)."""
+        comps = self.comps if comps is None else tuple(comps)
+        self._staged = (comps, _HOST_POOL.submit(self._host_buffers, comps))
+        return self
+
+    def phasors_host(self, comps=None, stream=None):
+        """{comp: (2/N) sum F e^{-i w t}} as host complex64 arrays in each
+        component's shape, the dtype of the reference's CW amplitude
+        (fdtd3d_core.py:1271, (2/n) times a complex64 accumulator).
+
+        Each component is scaled on the device and copied back in one transfer
+        on `stream` (default: the current stream), into the buffers stage_host()
+        prepared if it was called for these components, else into new ones.
+        Returns once the copies have ended."""
+        comps = self.comps if comps is None else tuple(comps)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        staged, self._staged = getattr(self, '_staged', None), None
+        host = staged[1].result() if staged is not None and set(comps) <= set(staged[0]) else {}
+        host.update(self._host_buffers([c for c in comps if c not in host]))
+        scale = 2.0 / self.n_acc
+        with torch.cuda.stream(st):
+            for c in comps:
+                torch.from_numpy(host[c]).copy_(torch.view_as_complex(self.epi.dft[c]) * scale)
+        st.synchronize()
+        self.d2h_bytes = sum(host[c].nbytes for c in comps)
+        nx, ny, nz = self.spec.nx, self.spec.ny, self.spec.nz
+        shape = {0: (nx - 1, ny, nz), 1: (nx, ny - 1, nz), 2: (nx, ny, nz - 1)}
+        return {c: host[c][:shape[c][0], :shape[c][1], :shape[c][2]] for c in comps}
 
     def results(self, stream=None):
         """Scalars of the finished solve; waits for `stream` (default: the device)."""

@@ -1,0 +1,133 @@
+"""Size-independent properties of the engine at the full sizes of the two
+single-grid workloads, where the oracle is too slow to compare with:
+
+  planar2d_te     2D TE 1600 x 480 @ 25 nm, 12-cell CPML, one bead, 6000 steps
+  waveguide3d_tm  3D TM 480 x 192 x 256 @ 30 nm, 10-cell CPML, lossy aqueous,
+                  two beads, the 4000-step schedule with Ex/Ey/Ez phasors
+
+* chunking: the same steps issued in uneven pieces (odd step counts, so the
+  fused 3D pass also ends on its second field buffer mid-run) give bit-identical
+  fields and phasors;
+* linearity: the update is linear in the source (the Yee, CPML, loss and DFT
+  arithmetic multiplies fields only by coefficients), so doubling the Huygens
+  amplitudes doubles every field, phasor and flux and quadruples every |E|^2
+  sum.  Not bit for bit: ahead of the wave the numerical precursor passes
+  through subnormal values, whose rounding does not scale with the source, and
+  the wavefront carries that ~1-ulp relative difference along as it grows.
+  The NumPy oracle (the reference algorithm in float32, subnormals kept) shows
+  the same: 600 x 160 cells, 900 steps, relative L2 5e-7 in Ez; at the full 2D
+  size after 6000 steps the GPU gives 1.4e-6 (Ez) to 5e-6 (Hx), at the full 3D
+  size 5.5e-5 in Hy relative to its own norm (a weak component of this drive;
+  the 3D check divides by the norm of the whole E or H field).  REL_LIN leaves
+  a margin over that; a term missing the source factor would miss it by orders
+  of magnitude;
+* 2D: the batched kernels on the full-size instance agree with the single-grid
+  kernels, as on the small sweep.
+"""
+import numpy as np
+import pytest
+
+from lens_sensor_b200.workloads import planar2d_te, waveguide3d_tm
+
+REL_LIN = 5e-5       # linearity: relative L2 (subnormal rounding at the precursor, see above)
+
+
+def _rel(a, b):
+    return float((a - b).abs().norm()) / max(float(b.abs().norm()), 1e-300)
+
+
+def _doubled_source(src):
+    return dict(src, amp=(2 * np.asarray(src['amp'], np.float32)).astype(np.float32))
+
+
+@pytest.mark.gpu
+def test_planar2d_full_size_chunking_linearity_and_batch():
+    import torch
+    from lens_sensor_b200 import batch2d as B
+    from lens_sensor_b200 import engine as E
+    sp, steps = planar2d_te()
+    assert (sp.nx, sp.ny, steps) == (1600, 480, 6000)
+    sw = B.Sweep([sp], steps, 'f32')
+    sw.run()
+    torch.cuda.synchronize()
+    batched = sw.results()[0]['phasor']
+    inst = sw.insts[0]
+    geo = inst.geo
+    coef = {k: geo[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if k in geo}
+
+    def single(src, chunks):
+        g = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, geo['cx'], geo['cy'], src)
+        ep = E.Epi2D(g, dft=inst.window)
+        n = 0
+        for n1 in chunks:
+            g.step(sw.table, n, n1 - n, ep)
+            n = n1
+        torch.cuda.synchronize()
+        return g, ep
+
+    g1, e1 = single(geo['src'], (steps,))
+    g2, e2 = single(geo['src'], (1, 1999, 4321, steps))
+    for nm in ('ez', 'hx', 'hy'):
+        assert torch.equal(getattr(g1, nm), getattr(g2, nm)), nm
+    p1, p2 = e1.phasor(), e2.phasor()
+    assert torch.equal(p1, p2)
+    assert float(p1.abs().max()) > 0 and bool(torch.isfinite(p1).all())
+    g3, e3 = single(_doubled_source(geo['src']), (steps,))
+    for nm in ('ez', 'hx', 'hy'):
+        assert _rel(getattr(g3, nm), 2 * getattr(g1, nm)) <= REL_LIN, (nm, _rel(getattr(g3, nm), 2 * getattr(g1, nm)))
+    assert _rel(e3.phasor(), 2 * p1) <= REL_LIN
+    ph = (2.0 / inst.n_acc) * p1
+    assert _rel(batched, ph) < 1e-5
+
+
+@pytest.mark.gpu
+def test_waveguide3d_full_size_chunking_and_linearity():
+    import torch
+    from lens_sensor_b200.geometry import build_3d
+    from lens_sensor_b200.solver3d import Solve3D
+    sp, steps = waveguide3d_tm()
+    assert (sp.nx, sp.ny, sp.nz, steps) == (480, 192, 256, 4000)
+    geo = build_3d(sp)
+    comps = (0, 1, 2)
+
+    def solve(g, chunks):
+        s = Solve3D(sp, steps, comps=comps, geo=g)
+        for n1 in chunks:
+            s.run(n1)
+        r = s.results()
+        out = dict(res=r, ph=[s.phasor(c).cpu() for c in comps], fields={nm: s.grid.view(nm).cpu()
+                   for nm in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')})
+        del s
+        torch.cuda.empty_cache()
+        return out
+
+    a = solve(geo, (steps,))
+    b = solve(geo, (1237, 2711, steps))
+    for nm, f in a['fields'].items():
+        assert torch.equal(f, b['fields'][nm]), nm
+    for p, q in zip(a['ph'], b['ph']):
+        assert torch.equal(p, q)
+        assert float(p.abs().max()) > 0 and bool(torch.isfinite(p).all())
+    ra, rb = a['res'], b['res']
+    for k in ('P_in', 'P_out', 'S_in', 'S_out', 'transmission', 'cw_rel_change'):
+        assert ra[k] == pytest.approx(rb[k], rel=1e-9, abs=0.0), k
+    c = solve(dict(geo, src=_doubled_source(geo['src'])), (steps,))
+    # each component's deviation relative to the whole vector field (E or H), so
+    # that a weak component is not judged by its own small norm
+    for group in (('ex', 'ey', 'ez'), ('hx', 'hy', 'hz')):
+        tot = sum(float((2 * a['fields'][nm]).norm()) ** 2 for nm in group) ** 0.5
+        for nm in group:
+            e = float((c['fields'][nm] - 2 * a['fields'][nm]).norm()) / tot
+            assert e <= REL_LIN, (nm, e)
+    tot = sum(float((2 * p).abs().norm()) ** 2 for p in a['ph']) ** 0.5
+    for p, q in zip(a['ph'], c['ph']):
+        assert float((q - 2 * p).abs().norm()) / tot <= REL_LIN
+    rc = c['res']
+    for k in ('S_in', 'S_out'):
+        assert rc[k] == pytest.approx(4 * ra[k], rel=REL_LIN), k
+    for k in ('P_in', 'P_out'):
+        assert rc[k] == pytest.approx(4 * ra[k], rel=REL_LIN), k
+    assert rc['transmission'] == pytest.approx(ra['transmission'], rel=REL_LIN)
+    # a difference of two windows' sums, ~2e-3 of either: the fields' relative
+    # deviation is magnified by ~500 in it
+    assert rc['cw_rel_change'] == pytest.approx(ra['cw_rel_change'], rel=5e-2)

@@ -6,7 +6,7 @@ is no fallback: if the library is missing the import of the engine raises.
 """
 import ctypes
 import os
-from ctypes import POINTER, c_double, c_float, c_int, c_void_p
+from ctypes import POINTER, c_float, c_int, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, '_lib', 'liblens_fdtd.so')

@@ -25,7 +25,7 @@ from typing import List, Optional, Tuple
 
 import numpy as np
 
-from .physics import C0, EPS0, MU0, N_AIR
+from .physics import C0, EPS0, N_AIR
 
 F32 = np.float32
 

@@ -10,7 +10,6 @@ results.  This is the engine behind fdtd3d_core.run_3d's full-domain CPML path
   * the convergence DFT of the driven component on the z mid-plane for the
     window before (:1159-1175).
 """
-import math
 import time
 from concurrent.futures import ThreadPoolExecutor
 

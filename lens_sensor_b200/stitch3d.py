@@ -20,7 +20,6 @@ Follows planar_3d/fdtd3d_core.py:1311-1782 (run_3d_stitched):
 
 The handoff amplitudes never leave the device.
 """
-import math
 
 import numpy as np
 import torch

@@ -7,7 +7,6 @@ tests/golden/cases.json): geometry in the reference's own parameters, so the
 same dict drives the reference (tests/golden/make_golden.py), this oracle and
 the GPU engine.
 """
-import math
 
 import numpy as np
 

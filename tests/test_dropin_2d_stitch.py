@@ -26,7 +26,6 @@ import pytest
 
 import _oracle_engine
 from lens_sensor_b200 import fdtd2d_core as D2
-from test_dropin_2d import _check as _check_npz_pkl  # noqa: F401  (shared comparison rules)
 
 HERE = os.path.dirname(__file__)
 GOLD = json.load(open(os.path.join(HERE, 'golden', 'dropin_2d_stitch.json')))

@@ -125,22 +125,32 @@ class Solve3D:
         comp = self.spec.src_comp if comp is None else comp
         return (2.0 / self.n_acc) * self.epi.phasor(comp)
 
-    def _host_buffers(self, comps):
-        """Host complex64 destinations (nx, ny, pitch) of the phasor read-back,
-        written once so that their pages are resident before the copy."""
+    def _host_buffers(self, comps, pinned=False):
+        """Host complex64 destinations (nx, ny, pitch) of the phasor read-back:
+        page-locked torch tensors, or numpy arrays written once so that their
+        pages are resident before the copy."""
         out = {}
         for c in comps:
-            a = np.empty(tuple(self.epi.dft[c].shape[:3]), np.complex64)
-            a.view(np.float32).fill(0.0)
-            out[c] = a
+            shape = tuple(self.epi.dft[c].shape[:3])
+            if pinned:
+                out[c] = torch.empty(shape, dtype=torch.complex64, pin_memory=True)
+            else:
+                a = np.empty(shape, np.complex64)
+                a.view(np.float32).fill(0.0)
+                out[c] = a
         return out
 
-    def stage_host(self, comps=None):
+    def stage_host(self, comps=None, pinned=False):
         """Prepare the host destinations of phasors_host(comps) on a background
         thread, so that it overlaps the stepping (call before run(); the
-        launches run without the GIL)."""
+        launches run without the GIL).  pinned: page-locked buffers from torch's
+        host cache.  The copy back then runs at the link's rate (0.013 s for
+        the three 189 MB phasors of a 480 x 192 x 256 grid, against 0.03-0.09 s
+        pageable), but a first allocation of that size holds up the kernel
+        launches of the concurrent run (0.19 s), so it pays only once the cache
+        holds the blocks, for repeated solves in one process."""
         comps = self.comps if comps is None else tuple(comps)
-        self._staged = (comps, _HOST_POOL.submit(self._host_buffers, comps))
+        self._staged = (comps, _HOST_POOL.submit(self._host_buffers, comps, pinned))
         return self
 
     def phasors_host(self, comps=None, stream=None):
@@ -160,8 +170,12 @@ class Solve3D:
         scale = 2.0 / self.n_acc
         with torch.cuda.stream(st):
             for c in comps:
-                torch.from_numpy(host[c]).copy_(torch.view_as_complex(self.epi.dft[c]) * scale)
+                h = host[c]
+                pinned = isinstance(h, torch.Tensor)
+                (h if pinned else torch.from_numpy(h)).copy_(torch.view_as_complex(self.epi.dft[c]) * scale,
+                                                             non_blocking=pinned)
         st.synchronize()
+        host = {c: (h.numpy() if isinstance(h, torch.Tensor) else h) for c, h in host.items()}
         self.d2h_bytes = sum(host[c].nbytes for c in comps)
         nx, ny, nz = self.spec.nx, self.spec.ny, self.spec.nz
         shape = {0: (nx - 1, ny, nz), 1: (nx, ny - 1, nz), 2: (nx, ny, nz - 1)}

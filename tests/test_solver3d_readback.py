@@ -29,13 +29,14 @@ def test_host_phasors_match_device_phasors(pol):
 
 @pytest.mark.gpu
 def test_host_phasors_without_staging_and_partial():
-    """Without stage_host(), and for a subset of the staged components."""
+    """Without stage_host(), and for a subset of the components staged in
+    page-locked buffers."""
     from lens_sensor_b200.solver3d import Solve3D
     st = Stack(1.49, 1.0, [(1.0, 1.333)], 1.376)
     sp = Spec3D('p', 48, 40, 36, 100.0, st, 2.0)
     s = Solve3D(sp, 200, comps=(0, 1, 2)).run()
     a = s.phasors_host((1,))
-    s.stage_host((0, 2))
+    s.stage_host((0, 2), pinned=True)
     b = s.phasors_host((2,))
     for c, h in ((1, a[1]), (2, b[2])):
         d = s.phasor(c).cpu().numpy()

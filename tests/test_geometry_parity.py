@@ -85,3 +85,31 @@ def test_3d_setup_bitwise_two_beads_lossy():
                                          dict(x_um=3.4, d_um=0.6, n=1.59, z_um=-0.3)])
     c.pop('bead')
     _check3d(c)
+
+
+def test_3d_setup_same_on_any_thread_count(monkeypatch):
+    """The volume builders split the x range over host threads; the arrays do
+    not depend on how many (1, 3 and 7 threads, uneven slabs)."""
+    c = dict(CASES['d3'], Nx=113, beads=[dict(x_um=1.6, d_um=0.5, n=1.59, z_um=0.2),
+                                          dict(x_um=3.4, d_um=0.6, n=1.59, z_um=-0.3)])
+    c.pop('bead')
+    sp = spec3d(c)
+    out = []
+    for n in (1, 3, 7):
+        monkeypatch.setattr(G, 'HOST_THREADS', n)
+        out.append(G.build_3d(sp))
+    for p in out[1:]:
+        for a in range(3):
+            np.testing.assert_array_equal(p['ce'][a], out[0]['ce'][a])
+            np.testing.assert_array_equal(p['da'][a], out[0]['da'][a])
+
+
+def test_slabs_cover_the_range_once():
+    seen = []
+    G._slabs(101, lambda a, b: seen.append((a, b)), min_rows=4)
+    seen.sort()
+    assert seen[0][0] == 0 and seen[-1][1] == 101
+    assert all(p[1] == q[0] for p, q in zip(seen, seen[1:]))
+    one = []
+    G._slabs(10, lambda a, b: one.append((a, b)), min_rows=16)
+    assert one == [(0, 10)]

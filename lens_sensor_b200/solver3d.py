@@ -149,9 +149,16 @@ class Solve3D:
         pageable), but a first allocation of that size holds up the kernel
         launches of the concurrent run (0.19 s), so it pays only once the cache
         holds the blocks, for repeated solves in one process."""
-        comps = self.comps if comps is None else tuple(comps)
+        comps = self._accumulated(comps)
         self._staged = (comps, _HOST_POOL.submit(self._host_buffers, comps, pinned))
         return self
+
+    def _accumulated(self, comps):
+        comps = self.comps if comps is None else tuple(int(c) for c in comps)
+        bad = [c for c in comps if c not in self.comps]
+        if bad:
+            raise ValueError(f'components {bad} are not accumulated by this solve (comps={self.comps})')
+        return comps
 
     def phasors_host(self, comps=None, stream=None):
         """{comp: (2/N) sum F e^{-i w t}} as host complex64 arrays in each
@@ -162,7 +169,7 @@ class Solve3D:
         on `stream` (default: the current stream), into the buffers stage_host()
         prepared if it was called for these components, else into new ones.
         Returns once the copies have ended."""
-        comps = self.comps if comps is None else tuple(comps)
+        comps = self._accumulated(comps)
         st = stream if stream is not None else torch.cuda.current_stream()
         staged, self._staged = getattr(self, '_staged', None), None
         host = staged[1].result() if staged is not None and set(comps) <= set(staged[0]) else {}

@@ -41,3 +41,13 @@ def test_host_phasors_without_staging_and_partial():
     for c, h in ((1, a[1]), (2, b[2])):
         d = s.phasor(c).cpu().numpy()
         assert h.shape == d.shape and np.linalg.norm(h - d) <= 1e-6 * np.linalg.norm(d), c
+
+
+def test_read_back_refuses_components_not_accumulated():
+    from lens_sensor_b200.solver3d import Solve3D
+    s = Solve3D.__new__(Solve3D)       # no device needed for the argument check
+    s.comps = (1,)
+    assert s._accumulated(None) == (1,)
+    assert s._accumulated([1]) == (1,)
+    with pytest.raises(ValueError):
+        s._accumulated((0, 1))

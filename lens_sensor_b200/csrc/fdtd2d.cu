@@ -323,6 +323,17 @@ bool grid2d_ok(const G *g) {
            (g->src.ix < 0 || (g->src.amp && g->src.ph1 && g->src.ph2 && g->src.ix + 1 < g->nx));
 }
 
+// psi arrays of the strips each kernel updates (te2d_h/te2d_e, tm2d_h/tm2d_e)
+bool psi2d_ok(const LensTE2D *g) {
+    return lens_psi_ok(g->ay.h, g->psi_hxy) && lens_psi_ok(g->ax.h, g->psi_hyx) &&
+           lens_psi_ok(g->ax.e, g->psi_ezx) && lens_psi_ok(g->ay.e, g->psi_ezy);
+}
+
+bool psi2d_ok(const LensTM2D *g) {
+    return lens_psi_ok(g->ax.h, g->psi_hzx) && lens_psi_ok(g->ay.h, g->psi_hzy) &&
+           lens_psi_ok(g->ay.e, g->psi_exy) && lens_psi_ok(g->ax.e, g->psi_eyx);
+}
+
 LensEpi2D empty_epi() {
     LensEpi2D e{};
     e.dft_n0 = e.dft_n1 = 0;
@@ -339,7 +350,7 @@ bool drive2d_ok(const LensDrive2D *d, const LensStepTable *tab, int nx) {
 
 int te2d_run(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep, const LensDrive2D *dr, int n0,
              int nsteps, void *stream) {
-    if (!grid2d_ok(g) || !g->ez || !g->hx || !g->hy || !g->ce_e || !g->ce_h || nsteps < 0 ||
+    if (!grid2d_ok(g) || !psi2d_ok(g) || !g->ez || !g->hx || !g->hy || !g->ce_e || !g->ce_h || nsteps < 0 ||
         !lens_table_ok(tab, n0, nsteps) || !epi2d_ok(ep, tab, g->nx) || !drive2d_ok(dr, tab, g->nx))
         return LENS_ERR_ARG;
     const LensEpi2D e = ep ? *ep : empty_epi();
@@ -355,7 +366,7 @@ int te2d_run(const LensTE2D *g, const LensStepTable *tab, const LensEpi2D *ep, c
 
 int tm2d_run(const LensTM2D *g, const LensStepTable *tab, const LensEpi2D *ep, const LensDrive2D *dr, int n0,
              int nsteps, void *stream) {
-    if (!grid2d_ok(g) || !g->ex || !g->ey || !g->hz || !g->ca_x || !g->ca_y ||
+    if (!grid2d_ok(g) || !psi2d_ok(g) || !g->ex || !g->ey || !g->hz || !g->ca_x || !g->ca_y ||
         (!g->da_x) != (!g->da_y) || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) ||
         !epi2d_ok(ep, tab, g->nx) || !drive2d_ok(dr, tab, g->nx))
         return LENS_ERR_ARG;

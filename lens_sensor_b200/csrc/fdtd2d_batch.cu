@@ -643,6 +643,11 @@ bool inst_ok(const LensInst2D &g) {
         return false;
     if (g.src.ix >= 0 && (!g.src.amp || !g.src.ph1 || !g.src.ph2 || g.src.ix + 1 >= g.nx || g.src.nj > g.ny))
         return false;
+    // psi[q] of the strip it serves: TE hxy (y, H), hyx (x, H), ezx (x, E), ezy (y, E);
+    // TM hzx (x, H), hzy (y, H), exy (y, E), eyx (x, E)
+    const LensProfile *strip[2][4] = {{&g.ay.h, &g.ax.h, &g.ax.e, &g.ay.e}, {&g.ax.h, &g.ay.h, &g.ay.e, &g.ax.e}};
+    for (int q = 0; q < 4; ++q)
+        if (!lens_psi_ok(*strip[g.pol][q], g.psi[q])) return false;
     return true;
 }
 

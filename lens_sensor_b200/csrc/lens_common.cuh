@@ -55,6 +55,9 @@ static inline bool lens_profile_ok(const LensProfile &p, int n) {
     return p.b && p.c && p.ik && p.n == n && p.lo >= 0 && p.hi >= 0 && p.lo + p.hi <= n;
 }
 
+// A psi array must be present wherever its profile has a strip.
+static inline bool lens_psi_ok(const LensProfile &p, const void *psi) { return p.lo + p.hi == 0 || psi; }
+
 static inline bool lens_table_ok(const LensStepTable *t, int n0, int nsteps) {
     return t && t->wt && t->env && n0 >= t->t0 && (n0 + nsteps) <= (t->t0 + t->n_table);
 }

@@ -30,6 +30,8 @@ def _fake_inst(nx, ny, pol):
     for ax, n in ((s.ax, nx), (s.ay, ny)):
         for tag, m in (('e', n), ('h', n - 1)):
             setattr(ax, tag, N.Profile(16, 16, 16, m, 2, 2))
+    for q in range(4):          # every profile has strips, so every psi array is needed
+        s.psi[q] = 16
     s.src = N.Source(-1, None, None, None, 0, 0, 0)
     return s
 

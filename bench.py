@@ -108,7 +108,7 @@ def split_steps(K, steps_total, n_acc):
     return K - kb, kb
 
 
-def cpu_baseline(spec, steps=8):
+def cpu_baseline(spec, steps=16):
     """The NumPy oracle (restatement of the reference path) on a bounded sample:
     `steps` consecutive full-grid steps with the detector sums, one host thread."""
     from oracle import harness as H

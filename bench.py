@@ -194,7 +194,7 @@ def run_e2e(spec, steps_total, cells, ws, pg):
 
 
 def run_batched(plain_sample=16, count=256):
-    """Config 2: the 256-instance uneven 2D TE/TM sweep (4000 steps each).
+    """The sweep2d workload: 256 uneven 2D TE/TM solves (4000 steps each).
 
     plain   instances one at a time through the single-grid engine (the drop-in
             run_beads path, lens_te2d_step / lens_tm2d_step), on a seeded sample of
@@ -265,8 +265,8 @@ def run_batched(plain_sample=16, count=256):
 
 
 def run_stitch(windows=3):
-    """Config 3 windows: a 3D stitch of `windows` windows of 480 x 192 x 256 cells
-    (30 nm, 40-cell overlap; 19 windows = the whole 240 um config) through
+    """The stitch3d_plan workload: a 3D stitch of `windows` windows of 480 x 192 x
+    256 cells (30 nm, 40-cell overlap; 19 windows = the whole 240 um guide) through
     stitch3d.StitchSolve: per-window geometry built on a host thread while the
     previous window runs, steady-state steps, on-device handoff of the overlap
     amplitudes, assembly to host memory.  Rate = cell updates of every window
@@ -304,11 +304,11 @@ def run_stitch(windows=3):
                 unit=UNIT, value=cu / wall, wall_s=wall, cell_updates=cu, windows=pl.n_win,
                 steps_per_window=pl.steps_win, transmission=T,
                 handoff='on device (3 complex components x overlap planes)',
-                full_config_windows=19)
+                full_plan_windows=19)
 
 
 def run_serving(count=32, seed=4):
-    """Config 4: the first `count` requests of the seeded Poisson stream (mean 50
+    """The serving_stream workload: the first `count` requests of the seeded Poisson stream (mean 50
     req/s; 70 % 2D, 25 % 3D, 5 % stitch) replayed in real time through
     serve.Server (160 GB budget).  Latency = completion (result on the host)
     minus arrival."""

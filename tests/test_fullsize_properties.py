@@ -113,7 +113,7 @@ def test_waveguide3d_full_size_chunking_and_linearity():
         assert ra[k] == pytest.approx(rb[k], rel=1e-9, abs=0.0), k
     c = solve(dict(geo, src=_doubled_source(geo['src'])), (steps,))
     # each component's deviation relative to the whole vector field (E or H), so
-    # that a weak component is not judged by its own small norm
+    # that a weak component is not measured against its own small norm
     for group in (('ex', 'ey', 'ez'), ('hx', 'hy', 'hz')):
         tot = sum(float((2 * a['fields'][nm]).norm()) ** 2 for nm in group) ** 0.5
         for nm in group:

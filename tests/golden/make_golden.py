@@ -28,6 +28,7 @@ Outputs:
 `python tests/golden/make_golden.py sliding2d` writes dropin_2d_sliding.json.
 `python tests/golden/make_golden.py pulse2d` writes dropin_2d_pulse.json.
 `python tests/golden/make_golden.py pulse3d` writes dropin_3d_pulse.json.
+`python tests/golden/make_golden.py extend2d` writes dropin_2d_extend.json.
 """
 import json
 import os
@@ -312,17 +313,28 @@ def _summ(v):
     return d
 
 
-def dropin_2d():
-    """Run the reference driver end to end for DROPIN_2D and summarise its outputs."""
+# The CW convergence extension (fdtd2d_core.py:859-873): with the tolerance on the
+# phasor change between DFT windows set below what these short runs reach, the
+# driver extends the run window by window up to CW_MAX_EXTEND x its step count.
+DROPIN_2D_EXTEND = dict(
+    te_extend=dict(DROPIN_2D['te'], cw_tol=1e-4),
+    tm_extend=dict(DROPIN_2D['tm_kappa'], cw_tol=1e-3),
+)
+
+
+def dropin_2d(cases=None):
+    """Run the reference driver end to end for DROPIN_2D (or `cases`) and
+    summarise its outputs; a case's 'cw_tol' replaces the module's CW_TOL."""
     import glob
     import pickle
     out = {}
-    for name, c in DROPIN_2D.items():
+    for name, c in (DROPIN_2D if cases is None else cases).items():
         prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_dropin_')
-        old_k = d2.KAPPA
+        old_k, old_tol = d2.KAPPA, d2.CW_TOL
         try:
             os.chdir(tmp)
             d2.KAPPA = dict(c['kappa'])
+            d2.CW_TOL = c.get('cw_tol', old_tol)
             r = d2.run_beads(**c['kw'])
             d2.save_results(r)
             z = np.load(glob.glob('results/*_frames.npz')[0])
@@ -330,7 +342,7 @@ def dropin_2d():
             with open(glob.glob('results/*.pkl')[0], 'rb') as f:
                 pk = pickle.load(f)
         finally:
-            d2.KAPPA = old_k
+            d2.KAPPA, d2.CW_TOL = old_k, old_tol
             os.chdir(prev)
             shutil.rmtree(tmp, ignore_errors=True)
         scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
@@ -340,6 +352,8 @@ def dropin_2d():
         out[name] = dict(kw={k: v for k, v in c['kw'].items() if k != 'stack'}, kappa=c['kappa'],
                          stack=[dict(L, n=[L['n'].real, L['n'].imag]) for L in c['kw'].get('stack', [])],
                          npz=npz, pkl=scal)
+        if 'cw_tol' in c:
+            out[name]['cw_tol'] = c['cw_tol']
     return out
 
 
@@ -509,7 +523,7 @@ def dropin_2d_stitch():
                 pk = pickle.load(f)
             left = sorted(re.sub(r'_\d+_\d+\.npy$', '_{tag}.npy', f) for f in os.listdir('results'))
         finally:
-            d2.KAPPA = old_k
+            d2.KAPPA, d2.CW_TOL = old_k, old_tol
             os.chdir(prev)
             shutil.rmtree(tmp, ignore_errors=True)
         scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
@@ -627,7 +641,7 @@ def dropin_2d_pulse():
                 pk = pickle.load(f)
             left = sorted(re.sub(r'_\d+_\d+\.npy$', '_{tag}.npy', f) for f in os.listdir('results'))
         finally:
-            d2.KAPPA = old_k
+            d2.KAPPA, d2.CW_TOL = old_k, old_tol
             os.chdir(prev)
             shutil.rmtree(tmp, ignore_errors=True)
         scal = {k: (v if isinstance(v, (str, bool, int)) or v is None else
@@ -703,6 +717,11 @@ def dropin_3d_pulse():
 
 
 def main():
+    if 'extend2d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_2d_extend.json'), 'w') as f:
+            json.dump(dropin_2d(DROPIN_2D_EXTEND), f, indent=1)
+        print('wrote dropin_2d_extend.json')
+        return
     if 'pulse3d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_3d_pulse.json'), 'w') as f:
             json.dump(dropin_3d_pulse(), f, indent=1)

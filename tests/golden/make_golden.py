@@ -29,6 +29,7 @@ Outputs:
 `python tests/golden/make_golden.py pulse2d` writes dropin_2d_pulse.json.
 `python tests/golden/make_golden.py pulse3d` writes dropin_3d_pulse.json.
 `python tests/golden/make_golden.py extend2d` writes dropin_2d_extend.json.
+`python tests/golden/make_golden.py edges2d` writes dropin_2d_edges.json.
 """
 import json
 import os
@@ -319,6 +320,15 @@ def _summ(v):
 DROPIN_2D_EXTEND = dict(
     te_extend=dict(DROPIN_2D['te'], cw_tol=1e-4),
     tm_extend=dict(DROPIN_2D['tm_kappa'], cw_tol=1e-3),
+)
+
+
+# Geometry edge cases of run_beads: the reference run without a bead
+# (place_bead=False, fdtd2d_core.py:218-219, label suffix '_ref'), and a bead
+# whose centre lies beyond the domain end, which build_materials skips (:224).
+DROPIN_2D_EDGES = dict(
+    te_nobead=dict(DROPIN_2D['te'], kw=dict(DROPIN_2D['te']['kw'], place_bead=False)),
+    tm_bead_outside=dict(DROPIN_2D['tm_kappa'], kw=dict(DROPIN_2D['tm_kappa']['kw'], bead_x_um=9.5)),
 )
 
 
@@ -717,6 +727,11 @@ def dropin_3d_pulse():
 
 
 def main():
+    if 'edges2d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_2d_edges.json'), 'w') as f:
+            json.dump(dropin_2d(DROPIN_2D_EDGES), f, indent=1)
+        print('wrote dropin_2d_edges.json')
+        return
     if 'extend2d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_2d_extend.json'), 'w') as f:
             json.dump(dropin_2d(DROPIN_2D_EXTEND), f, indent=1)

@@ -30,6 +30,7 @@ Outputs:
 `python tests/golden/make_golden.py pulse3d` writes dropin_3d_pulse.json.
 `python tests/golden/make_golden.py extend2d` writes dropin_2d_extend.json.
 `python tests/golden/make_golden.py edges2d` writes dropin_2d_edges.json.
+`python tests/golden/make_golden.py edges3d` writes dropin_3d_edges.json.
 """
 import json
 import os
@@ -393,12 +394,23 @@ DROPIN_3D = dict(
 )
 
 
-def dropin_3d():
-    """Run the reference 3D driver end to end for DROPIN_3D and summarise its outputs."""
+# Geometry edge cases of run_3d: no bead (bead=None), and a bead whose sphere
+# crosses the z end of the domain, so its sub-pixel box is clipped there.
+DROPIN_3D_EDGES = dict(
+    te_nobead=dict(DROPIN_3D['golden3d'], kw=dict(DROPIN_3D['golden3d']['kw'], label='te_nobead', bead=None)),
+    tm_bead_clipped=dict(DROPIN_3D['tm_stack'],
+                         kw=dict(DROPIN_3D['tm_stack']['kw'], label='tm_bead_clipped',
+                                 bead=dict(x_um=2.3, d_um=0.6, n=1.59, z_um=1.05))),
+)
+
+
+def dropin_3d(cases=None):
+    """Run the reference 3D driver end to end for DROPIN_3D (or `cases`) and
+    summarise its outputs."""
     import glob
     import pickle
     out = {}
-    for name, c in DROPIN_3D.items():
+    for name, c in (DROPIN_3D if cases is None else cases).items():
         prev, tmp = os.getcwd(), tempfile.mkdtemp(prefix='lens_dropin3d_')
         old_k = d3.KAPPA
         try:
@@ -727,6 +739,11 @@ def dropin_3d_pulse():
 
 
 def main():
+    if 'edges3d' in sys.argv[1:]:
+        with open(os.path.join(OUT, 'dropin_3d_edges.json'), 'w') as f:
+            json.dump(dropin_3d(DROPIN_3D_EDGES), f, indent=1)
+        print('wrote dropin_3d_edges.json')
+        return
     if 'edges2d' in sys.argv[1:]:
         with open(os.path.join(OUT, 'dropin_2d_edges.json'), 'w') as f:
             json.dump(dropin_2d(DROPIN_2D_EDGES), f, indent=1)

@@ -20,6 +20,11 @@ Outputs:
   dropin_3d.json                       the same for run_3d + save_results_3d
   dropin_3d_stitch.json                the same for run_3d_stitched + save_results_3d
   dropin_2d_stitch.json                the same for run_beads(method='stitch') + save_results
+  dropin_2d_sliding.json, dropin_2d_pulse.json, dropin_3d_pulse.json
+                                       the co-moving window and the pulse stitches
+  dropin_2d_extend.json                run_beads with a tighter CW_TOL (window extensions)
+  dropin_2d_edges.json, dropin_3d_edges.json
+                                       no bead; a bead beyond or across the domain end
 
 `python tests/golden/make_golden.py dropin` stops after the two JSON files;
 `python tests/golden/make_golden.py stitch` writes only the 3D stitch fixtures

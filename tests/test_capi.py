@@ -164,3 +164,34 @@ def test_batch_plan_requires_the_psi_of_every_strip(lib, pol):
         p.lo = p.hi = 0
         one = (N.Inst2D * 1)(s)
         assert lib.lens_batch2d_plan(one, 1, 8, blk, None) > 0, q
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No CPU fallback: without the built library the bindings raise."""
+    from lens_sensor_b200 import _native as N
+    monkeypatch.setattr(N, '_lib', None)
+    with pytest.raises(N.LensError, match='not found'):
+        N.load(str(tmp_path / 'liblens_fdtd.so'))
+
+
+def test_abi_mismatch_fails_loudly(lib, monkeypatch):
+    """A library built from another header than the bindings is refused."""
+    from lens_sensor_b200 import _native as N
+
+    class Wrong(ctypes.Structure):
+        _fields_ = [('x', ctypes.c_char * 3)]
+    monkeypatch.setattr(N, '_lib', None)
+    monkeypatch.setattr(N, 'MIRRORS', (Wrong,) + tuple(N.MIRRORS[1:]))
+    with pytest.raises(N.LensError, match='ABI mismatch'):
+        N.load()
+
+
+def test_grids_need_a_cuda_device():
+    """Constructing a grid without a CUDA device raises instead of falling back."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('a CUDA device is present')
+    from lens_sensor_b200 import _native as N
+    from lens_sensor_b200 import engine as E
+    with pytest.raises(N.LensError, match='no CPU fallback'):
+        E.StepTable(0, 4, 1e-17, 1e15, 1e15, E.cw_envelope(3e14))

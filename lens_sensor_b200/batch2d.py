@@ -133,13 +133,18 @@ class Instance:
         sp = self.spec
         ph = self.phasor() if ph is None else ph
         I = 0.5 * (ph.real ** 2 + ph.imag ** 2)
-        dx, nx = sp.dx, sp.nx
-        c, w = 0.8 * nx, 0.1 * nx
-        lo, hi = max(0, int(round(c - w / 2))), min(nx, int(round(c + w / 2)))
-        j0 = int(round(sp.tear_m / dx))                            # y = 0: core bottom
-        j1 = int(round((sp.tear_m + sp.stack.t_wg_um * 1e-6) / dx))
-        tear = sum(t for t, _ in sp.stack.layers) * 1e-6
-        jt = max(0, int(round((sp.tear_m - tear) / dx)))
+        nx, ny = sp.nx, sp.ny
+        # the analyzer's display extents (um) and its index rounding (:2737-2747)
+        L = nx * sp.dx * 1e6
+        y0 = -sp.tear_m * 1e6
+        y1 = y0 + ny * sp.dx * 1e6
+        xi = lambda v: int(round(v / L * nx))
+        vi = lambda v: int(round((v - y0) / (y1 - y0) * ny))
+        c, w = 0.8 * L, 0.1 * L
+        lo = max(0, xi(c - w / 2))
+        hi = max(lo + 1, min(xi(c + w / 2), nx))
+        j0, j1 = max(0, vi(0.0)), min(ny, vi(sp.stack.t_wg_um))   # core band; y = 0 is its bottom
+        jt = max(0, vi(-sum(t for t, _ in sp.stack.layers)))    # the whole layer stack below
         band = lambda a, b: float(torch.mean(torch.sum(I[lo:hi, a:b], dim=1))) if b > a else 0.0
         g = band(j0, j1)
         return band(jt, j0) / g if g > 0 else 0.0

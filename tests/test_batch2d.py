@@ -132,3 +132,33 @@ def test_graph_replay_and_storage_variants():
         for q, r in enumerate(c.results()):
             err = float((r['phasor'] - ref[q]).abs().norm() / ref[q].abs().norm())
             assert err < tol, (st, q, err)
+
+
+def test_overlap_uses_the_analyzer_windows():
+    """Instance.overlap against the reference analyzer's band sums written out
+    (common/fdtd_analyzer.py:2737-2747 index rounding, :2880-2935 windows and
+    bands; custom-stack tear band), on a seeded CW amplitude.  CPU tensors."""
+    import torch
+    from types import SimpleNamespace
+    from lens_sensor_b200 import batch2d as B
+    from lens_sensor_b200.workloads import sweep2d
+    specs, _ = sweep2d(count=4)
+    rng = np.random.default_rng(5)
+    for sp in specs:
+        ph = torch.from_numpy(rng.standard_normal((sp.nx, sp.ny)) + 1j * rng.standard_normal((sp.nx, sp.ny)))
+        got = B.Instance.overlap(SimpleNamespace(spec=sp), ph)
+        # the analyzer: display extents x in [0, L], y in [-tear_buffer, -tear_buffer + H] (um)
+        I = 0.5 * np.abs(ph.numpy()) ** 2
+        L, H = sp.nx * sp.dx * 1e6, sp.ny * sp.dx * 1e6
+        y0, y1 = -sp.tear_m * 1e6, -sp.tear_m * 1e6 + H
+        xi = lambda v: int(round(v / L * sp.nx))
+        vi = lambda v: int(round((v - y0) / (y1 - y0) * sp.ny))
+        c, w = 0.8 * L, 0.1 * L
+        dl = max(0, xi(c - w / 2))
+        dh = max(dl + 1, min(xi(c + w / 2), sp.nx))
+        lo, hi = max(0, vi(0.0)), min(sp.ny, vi(sp.stack.t_wg_um))
+        tear = sum(t for t, _ in sp.stack.layers)
+        tl = max(0, vi(-tear))
+        band = lambda a, b: float(np.mean(np.sum(I[dl:dh, a:b], axis=1))) if b > a else 0.0
+        want = band(tl, lo) / band(lo, hi)
+        assert got == pytest.approx(want, rel=1e-12), (sp.nx, sp.ny, got, want)

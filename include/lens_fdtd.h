@@ -26,7 +26,9 @@
  *  - CPML psi is updated only in the strips where the profile's c != 0 (leading
  *    `lo` and trailing `hi` entries of the profile); the 2D strip arrays and the
  *    3D psi volumes are documented with each grid.  Outside the strips psi is
- *    identically zero.
+ *    identically zero.  A profile with a strip (lo + hi > 0) needs the psi
+ *    arrays that strip serves; a NULL one is refused with LENS_ERR_ARG before
+ *    anything is launched.
  */
 #ifndef LENS_FDTD_H
 #define LENS_FDTD_H

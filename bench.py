@@ -175,7 +175,7 @@ def run_e2e(spec, steps_total, cells, ws, pg):
     s2.stage_host((0, 1, 2))          # the read-back's host buffers are made while the device steps
     s2.run()
     ev[1].record()
-    s2.phasors_host((0, 1, 2))
+    ph = s2.phasors_host((0, 1, 2))
     res = s2.results()
     torch.cuda.synchronize()
     t3 = time.perf_counter()
@@ -188,8 +188,133 @@ def run_e2e(spec, steps_total, cells, ws, pg):
                d2h_bytes_per_step=d2h / steps_total, solve_seconds=t_e2e, host_setup_seconds=s2.t_setup_host,
                phase_seconds={k: round(v, 4) for k, v in phases.items()},
                transmission=res['transmission'], cw_rel_change=res['cw_rel_change'])
+    out['err_vs_fp64'] = err3d_vs_fp64(spec, ph, res, s2)
     del s2
     torch.cuda.empty_cache()
+    return out
+
+
+FP64 = os.path.join(ROOT, 'tests', 'golden', 'fp64')
+
+
+def _fp64_meta():
+    try:
+        with open(os.path.join(FP64, 'fp64.json')) as f:
+            return json.load(f)['runs']
+    except Exception:
+        return None
+
+
+def _sample_mask(n, shift):
+    """The fixtures' hashed cell sample (tests/golden/make_fp64.py sample_mask)."""
+    i = np.arange(n, dtype=np.uint64)
+    return (((i * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)) >> np.uint64(32 - shift)) == 0
+
+
+def _rel(a, b):
+    return float(np.linalg.norm((np.asarray(a) - np.asarray(b)).ravel()) / max(np.linalg.norm(np.asarray(b).ravel()), 1e-300))
+
+
+def err3d_vs_fp64(spec, ph, res, solve):
+    """Relative L2 errors of the config-1 phasors (hashed 1/256 cell sample and z
+    mid-plane; Ex, Ez against the vector norm) and scalars against the FP64 run
+    of the reference algorithm (tests/golden/fp64), with the reference
+    algorithm's own float32 errors beside them."""
+    m = _fp64_meta()
+    if m is None or 'c1' not in m:
+        return None
+    fx = np.load(os.path.join(FP64, 'c1.npz'))
+    r = m['c1']
+    vs = np.sqrt(sum(np.linalg.norm(fx[f'{k}_sample']) ** 2 for k in ('Ex', 'Ey', 'Ez')))
+    out = {}
+    for q, c in enumerate(('Ex', 'Ey', 'Ez')):
+        a = ph[q]
+        sel = a.ravel()[_sample_mask(a.size, 8)]
+        out[c] = dict(own=_rel(sel, fx[f'{c}_sample']), vector=float(np.linalg.norm(sel - fx[f'{c}_sample']) / vs),
+                      zmid=_rel(a[:, :, a.shape[2] // 2], fx[f'{c}_zmid']))
+    for k in ('P_in', 'P_out', 'transmission'):
+        out[k] = abs(res[k] - r[k]) / max(abs(r[k]), 1e-300)
+    out['bar'] = 1e-4
+    out['reference_fp32'] = {c: r['ref_fp32_err'][c] for c in ('Ex', 'Ey', 'Ez', 'transmission')}
+    return out
+
+
+def cpu_baseline_2d(spec, steps=200):
+    """The NumPy oracle (restatement of the reference 2D TE path) on `steps`
+    consecutive full-grid steps, one host thread."""
+    from oracle import fdtd_oracle as O
+    from lens_sensor_b200.geometry import build_2d
+    geo = build_2d(spec)
+    src = O.Huygens.__new__(O.Huygens)
+    src.ix, src.omega = int(geo['src']['ix']), float(geo['src']['omega'])
+    src.amp, src.ph1, src.ph2 = (np.asarray(geo['src'][k], np.float32) for k in ('amp', 'ph1', 'ph2'))
+    g = O.Grid2D('s', spec.nx, spec.ny, spec.dx, spec.dt, geo['cx'], geo['cy'], src,
+                 {k: geo[k] for k in ('ce_e', 'ce_h')}, np.float32)
+    g.step(0, 0.0)
+    t0 = time.perf_counter()
+    for n in range(1, steps + 1):
+        g.step(n, 0.5)
+    dt = time.perf_counter() - t0
+    return spec.nx * spec.ny * steps / dt, f'{steps} consecutive full-grid steps of the 1600x480 2D TE CPML step ' \
+                                            f'on the NumPy oracle (float32), {dt:.1f} s'
+
+
+def run_planar2d(cpu=True):
+    """Config 0 (planar2d_te: 2D TE 1600 x 480 @ 25 nm, 6000 steps, one-period CW
+    phasor, Ez snapshots every 200 steps) on the single-grid engine.  value: the
+    whole 6000-step solve on the device (CUDA events, inputs resident); e2e: the
+    same solve from the host spec (setup, upload, run, read-back of the phasor and
+    the 30 snapshots)."""
+    import torch
+    from lens_sensor_b200.solver2d import Solve2D
+    from lens_sensor_b200.workloads import planar2d_te
+    sp, steps = planar2d_te()
+    cells = sp.nx * sp.ny
+    warm = Solve2D(sp, steps)
+    warm.run()
+    geo = warm.geo
+    del warm
+    s = Solve2D(sp, steps, geo=geo)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    s.run()
+    ev[1].record()
+    torch.cuda.synchronize()
+    t_dev = ev[0].elapsed_time(ev[1]) * 1e-3
+    del s
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s = Solve2D(sp, steps)
+    s.run()
+    ph, snaps = s.host_results()
+    t_e2e = time.perf_counter() - t0
+    peak, peak_src = peaks()
+    achieved = 32.0 * cells / (t_dev / steps) / 1e9
+    out = dict(workload=f'planar2d_te: 2D TE planar waveguide {sp.nx}x{sp.ny} @ 25 nm, fp32, 12-cell CPML, '
+                        f'{steps} steps, CW ramped over 20 periods, one seeded PS bead, one-period phasor, '
+                        'Ez snapshots every 200 steps',
+               unit=UNIT, value=cells * steps / t_dev, ms_per_step=t_dev / steps * 1e3, steps=steps, cells=cells,
+               l2=f'working set {(5 * cells * 4) / 1e6:.0f} MB of fields and coefficients fits in the 126 MB L2: '
+                  'the steps of one solve run L2-resident, as in use; no flush between steps',
+               roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
+                             peak_source=peak_src, kernel='2D TE step (te2d_h + te2d_e)',
+                             alg_bytes_per_step=32 * cells, step_ms=t_dev / steps * 1e3),
+               e2e=dict(value=cells * steps / t_e2e, unit=UNIT, solve_seconds=t_e2e,
+                        h2d_bytes_per_step=s.h2d_bytes / steps, d2h_bytes_per_step=s.d2h_bytes / steps,
+                        host_setup_seconds=s.t_setup_host))
+    m = _fp64_meta()
+    if m and 'c0' in m:
+        fx = np.load(os.path.join(FP64, 'c0.npz'))
+        mk = _sample_mask(snaps[-1].size, 3)
+        out['err_vs_fp64'] = dict(phasor=_rel(ph, fx['phasor']),
+                                  snap_last=_rel(snaps[-1].ravel()[mk], fx['snap_last_sample']), bar=1e-4,
+                                  reference_fp32=m['c0']['ref_fp32_err'])
+    del s
+    torch.cuda.empty_cache()
+    if cpu:
+        v, sample = cpu_baseline_2d(sp)
+        out['cpu_baseline'] = dict(value=v, unit=UNIT, cores=1, kind='port', sample=sample)
     return out
 
 
@@ -247,9 +372,29 @@ def run_batched(plain_sample=16, count=256):
     e1.record()
     torch.cuda.synchronize()
     t_h = e0.elapsed_time(e1) * 1e-3
+    res16 = sh.results()
     err = [float((r['phasor'] - ref[q]).abs().norm() / max(float(ref[q].abs().norm()), 1e-300))
-           for q, r in enumerate(sh.results())]
+           for q, r in enumerate(res16)]
+    fp64 = None
+    m = _fp64_meta()
+    if m:
+        fp64 = dict(bar=1e-4)
+        for q in [int(k[2:]) for k in m if k.startswith('sw') and int(k[2:]) < len(specs)]:
+            fx = np.load(os.path.join(FP64, f'sw{q}.npz'))['phasor_sample']
+            for tag, ph in (('f32', ref[q]), ('f16', res16[q]['phasor'])):
+                a = ph.cpu().numpy()
+                fp64[f'sw{q}_{tag}'] = _rel(a.ravel()[_sample_mask(a.size, 3)], fx)
     del sh
+    torch.cuda.empty_cache()
+    # the FP16 acceptance gate over the whole sweep (probes in both storages)
+    e0.record()
+    gres, gate = B.gated_sweep(specs, steps, 'f16', tol=1e-4, by=by, budget=budget, geos=geos)
+    e1.record()
+    torch.cuda.synchronize()
+    t_g = e0.elapsed_time(e1) * 1e-3
+    gate['value'] = cells * steps / t_g
+    gate['probe_err_max'] = max(p['err'] for p in gate['probes'])
+    del gres
     torch.cuda.empty_cache()
     plain = pc * steps / t_p
     f32 = cells * steps / t_b
@@ -261,7 +406,7 @@ def run_batched(plain_sample=16, count=256):
                 batched_f32=f32, batched_f16=f16, batched_vs_plain=f32 / plain, f16_vs_plain=f16 / plain,
                 tile=f'128 x {2 * by} nodes', group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
                 f16_phasor_err_vs_f32_max=max(err), f16_phasor_err_vs_f32_median=float(np.median(err)),
-                K_median=float(np.median(K)))
+                K_median=float(np.median(K)), err_vs_fp64=fp64, f16_gate=gate)
 
 
 def run_stitch(windows=3):
@@ -402,6 +547,7 @@ def ours_arm(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(spec, steps_total, cells, ws, pg)
+    planar = run_planar2d(cpu=(rank == 0 and not args.no_cpu)) if (ws == 1 and not args.no_planar) else None
     batched = run_batched(count=args.batch_instances) if (ws == 1 and not args.no_batch) else None
     stitch = run_stitch(args.stitch_windows) if (ws == 1 and not args.no_stitch) else None
     serving = run_serving(args.serve_requests) if (ws == 1 and not args.no_serve) else None
@@ -423,7 +569,7 @@ def ours_arm(args):
                                   launch_ms=t_launch * 1e3,
                                   mix_alg_bytes_per_cell_update=alg / (cells * K),
                                   mix_achieved=alg / (ms * 1e-3) / 1e9),
-                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches, batched=batched,
+                    cpu_baseline=cpu, e2e=e2e, clocks=ck, gpu_launches=launches, planar2d=planar, batched=batched,
                     stitch=stitch, serving=serving)
         print(json.dumps(line), flush=True)
     if pg:
@@ -440,6 +586,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
     ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (sweep2d)')
+    ap.add_argument('--no-planar', action='store_true', help='skip the 2D single-grid solve (planar2d_te)')
     ap.add_argument('--no-stitch', action='store_true', help='skip the 3D stitch (stitch3d_plan windows)')
     ap.add_argument('--batch-instances', type=int, default=256,
                     help='instances of the sweep2d sweep (fewer: a small case for profiling)')

@@ -225,10 +225,17 @@ int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, c
  * about 8.6 MB that every GPU loading this library holds until the process
  * exits; at most 512 instances and 2^21 tiles (128 x 2*by nodes each) per call,
  * larger calls return LENS_ERR_SIZE.  Nothing is allocated.  The first call on
- * a device looks up that array's device address; make it before any stream
- * capture.  Every call rewrites the whole array (nothing carries over between
- * calls), so calls that overlap on the GPU (other streams, other threads) race
- * on it; the fields, psi and DFT buffers are the caller's as usual.          */
+ * a device looks up that array's device address and keeps it for the life of
+ * the process (a cudaDeviceReset of that device invalidates it: do not reset a
+ * device that has run this call).  inst is copied to the device with
+ * cudaMemcpyAsync on `stream`: from pageable memory the copy is staged before
+ * the call returns, from page-locked memory it runs later, so a page-locked inst
+ * must stay unchanged until the stream has reached the call.  The call is not
+ * capturable: on a stream that is capturing it returns LENS_ERR_ARG before
+ * anything is enqueued.  Every call rewrites the whole array (nothing carries
+ * over between calls), so calls that overlap on the GPU (other streams, other
+ * threads) race on it; the fields, psi and DFT buffers are the caller's as
+ * usual.                                                                     */
 int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int storage, int by,
                               const LensStepTable *tab, int n0, int nsteps, void *stream);
 

@@ -286,3 +286,61 @@ class Sweep:
             ph = q.phasor()
             out.append(dict(pol=q.spec.pol, nx=q.spec.nx, ny=q.spec.ny, phasor=ph, K=q.overlap(ph)))
         return out
+
+
+def gated_sweep(specs, steps, storage='f16', tol=1e-4, probe_every=16, by=8, budget=None, device=None,
+                geos=None):
+    """A sweep whose FP16 / BF16 field storage is accepted only where it meets
+    `tol` (relative L2 phasor error).
+
+    Reduced storage rounds every stored field value to 11 (FP16) or 8 (BF16)
+    significant bits, so its error depends on the instance.  The gate probes
+    every `probe_every`-th instance of each polarisation in both the reduced
+    storage and FP32; a polarisation keeps the reduced storage for its other
+    instances only if every one of its probes' phasor error against FP32 is
+    within tol / 2 (half the bar, as margin for the instances not probed), and
+    runs in FP32 otherwise.  Probes keep their FP32 results.
+
+    Returns (results in the order of specs, each with its 'storage', and a
+    report: the probes' errors, the accepted polarisations and the instance
+    counts per storage)."""
+    if storage not in ('f16', 'bf16'):
+        raise ValueError(f'gated storage {storage!r}: f16 or bf16')
+    geos = list(geos) if geos is not None else [build_2d(sp) for sp in specs]
+    n = len(specs)
+    probes = []
+    for pol in ('s', 'p'):
+        idx = [q for q in range(n) if specs[q].pol == pol]
+        probes += idx[::max(1, int(probe_every))]
+    probes.sort()
+    sub = lambda ids, st: Sweep([specs[q] for q in ids], steps, st, by=by, budget=budget, device=device,
+                                geos=[geos[q] for q in ids])
+    out = [None] * n
+    errs = {}
+    if probes:
+        ref = sub(probes, 'f32')
+        ref.run()
+        r32 = ref.results()
+        del ref
+        red = sub(probes, storage)
+        red.run()
+        for q, a, b in zip(probes, r32, red.results()):
+            errs[q] = float((b['phasor'] - a['phasor']).abs().norm() / max(float(a['phasor'].abs().norm()), 1e-300))
+            out[q] = dict(a, storage='f32')
+        del red
+    ok = {pol: all(errs[q] <= 0.5 * tol for q in probes if specs[q].pol == pol) and
+          any(specs[q].pol == pol for q in probes) for pol in ('s', 'p')}
+    rest = [q for q in range(n) if out[q] is None]
+    for st, ids in ((storage, [q for q in rest if ok[specs[q].pol]]), ('f32', [q for q in rest if not ok[specs[q].pol]])):
+        if ids:
+            sw = sub(ids, st)
+            sw.run()
+            for q, r in zip(ids, sw.results()):
+                out[q] = dict(r, storage=st)
+            del sw
+    report = dict(storage=storage, tol=tol, probe_every=int(probe_every),
+                  probes=[dict(index=q, pol=specs[q].pol, err=errs[q]) for q in probes],
+                  accepted={pol: bool(v) for pol, v in ok.items()},
+                  n_reduced=sum(1 for r in out if r['storage'] == storage),
+                  n_f32=sum(1 for r in out if r['storage'] == 'f32'))
+    return out, report

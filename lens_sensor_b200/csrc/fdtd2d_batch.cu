@@ -796,13 +796,22 @@ extern "C" int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int 
     }
     blk[ninst] = (int)tot;
     if (any_dft && !tab->pe) return LENS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the descriptors and block offsets are copied from host memory at call time;
+    // a captured copy would re-read that memory at every replay, so a capturing
+    // stream is refused before anything is enqueued
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return LENS_ERR_ARG;
+    }
+    if (cap != cudaStreamCaptureStatusNone) return LENS_ERR_ARG;
     unsigned char *base = nullptr;
     const int st = na_scratch(&base);
     if (st != LENS_OK) return st;
     LensInst2D *desc = reinterpret_cast<LensInst2D *>(base);
     int *blk_dev = reinterpret_cast<int *>(base + NA_DESC_BYTES);
     int *owner = reinterpret_cast<int *>(base + NA_DESC_BYTES + NA_BLK_BYTES);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     // every table is rewritten in full by each call (nothing carries over)
     if (cudaMemcpyAsync(desc, inst, ninst * sizeof(LensInst2D), cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(blk_dev, blk, (ninst + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess)

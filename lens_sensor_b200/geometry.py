@@ -17,6 +17,7 @@ stack) and on a small per-(x, z) column type (core column, air in front of the
 entry facet, ...); beads are local patches.  Coefficient volumes are expanded
 from per-type columns, then the bead boxes are patched.
 """
+import itertools
 import math
 import os
 from concurrent.futures import ThreadPoolExecutor
@@ -90,42 +91,43 @@ def column_average(ys, dy, eps_of_y, S=16, harmonic=False, shift=0.0):
     return np.mean(e, axis=1).astype(np.complex64 if cplx else F32)
 
 
+def ball_fraction(axes, centre, r, h, S):
+    """Share of each grid cell (side h, centred on the nodes axes[0] x axes[1]
+    [x axes[2]]) that lies inside the ball |p - centre| <= r: 1 for cells whose
+    node is at least half a cell diagonal inside the surface, 0 beyond it, and
+    for the cells the surface cuts the share of S samples per axis (at the
+    centres of S equal sub-intervals) that fall inside.  The sample squares are
+    summed in axis order, so the shares do not depend on how the loop is cut."""
+    dim = len(axes)
+    rel = [np.asarray(a, np.float64) - c for a, c in zip(axes, centre)]
+    grid = np.meshgrid(*rel, indexing='ij', sparse=True)
+    dist = np.sqrt(sum(g * g for g in grid))
+    half = h * np.sqrt(float(dim)) / 2.0
+    share = (dist <= r - half).astype(np.float64)
+    cut = np.nonzero((dist > r - half) & (dist < r + half))
+    if len(cut[0]):
+        off = _sub(S, h)
+        lead = [rel[a][cut[a]] for a in range(dim - 1)]
+        last = rel[-1][cut[-1]][:, None] + off[None, :]
+        last2 = last * last
+        inside = np.zeros(len(cut[0]))
+        for shift in itertools.product(off, repeat=dim - 1):
+            s2 = sum((v + o) * (v + o) for v, o in zip(lead, shift))
+            inside += np.count_nonzero(s2[:, None] + last2 <= r * r, axis=1)
+        share[cut] = inside / S ** dim
+    return share
+
+
 def circle_fraction(xs, ys, xc, yc, r, h, S=8):
-    """Area fraction of a disc in the cells around the nodes xs x ys."""
-    X = xs[:, None] - xc
-    Y = ys[None, :] - yc
-    d = np.sqrt(X * X + Y * Y)
-    half = h * np.sqrt(2.0) / 2.0
-    f = (d <= r - half).astype(np.float64)
-    edge = np.nonzero((d > r - half) & (d < r + half))
-    if len(edge[0]):
-        o = _sub(S, h)
-        px = X[edge[0], 0][:, None, None] + o[None, :, None]
-        py = Y[0, edge[1]][:, None, None] + o[None, None, :]
-        f[edge] = np.mean((px * px + py * py) <= r * r, axis=(1, 2))
-    return f
+    """Area share of a disc in the cells around the nodes xs x ys (S^2 samples
+    on the cells its edge cuts; the material blend of subpixel.py:25-39)."""
+    return ball_fraction((xs, ys), (xc, yc), r, h, S)
 
 
 def sphere_fraction(xs, ys, zs, xc, yc, zc, r, h, S=6):
-    """Volume fraction of a sphere in the cells around xs x ys x zs (S^3 samples
-    on surface cells)."""
-    X = xs[:, None, None] - xc
-    Y = ys[None, :, None] - yc
-    Z = zs[None, None, :] - zc
-    d = np.sqrt(X * X + Y * Y + Z * Z)
-    half = h * np.sqrt(3.0) / 2.0
-    f = (d <= r - half).astype(np.float64)
-    edge = np.nonzero((d > r - half) & (d < r + half))
-    if len(edge[0]):
-        o = _sub(S, h)
-        hit = np.zeros(len(edge[0]))
-        for a in o:
-            px = (X[edge[0], 0, 0] + a)[:, None, None]
-            py = Y[0, edge[1], 0][:, None, None] + o[None, :, None]
-            pz = Z[0, 0, edge[2]][:, None, None] + o[None, None, :]
-            hit += np.sum((px * px + py * py + pz * pz) <= r * r, axis=(1, 2))
-        f[edge] = hit / S ** 3
-    return f
+    """Volume share of a sphere in the cells around xs x ys x zs (S^3 samples on
+    the cells its surface cuts; subpixel.py:42-62)."""
+    return ball_fraction((xs, ys, zs), (xc, yc, zc), r, h, S)
 
 
 def _blend(eps, frac, n):

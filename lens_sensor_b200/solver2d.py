@@ -1,0 +1,82 @@
+"""One plain full-domain 2D solve on the GPU with a fixed schedule: the
+planar-waveguide run of fdtd2d_core.run_beads(method='full') reduced to its
+time-stepping outputs (planar_beads/fdtd2d_core.py:781-890):
+
+  * the CW phasor (2/N) sum F e^{-i w t} of the node field (TE Ez, TM Ey on
+    the nodes) over the last `periods` periods of the run (:838-847, :879),
+  * snapshots of the driven raw component (TE Ez, TM Ey) every `snap_every`
+    steps (the transient frames of the reference's frame writer, :876-890).
+
+schedule_2d() is torch-free so the oracle's FP64 replay of a workload uses the
+same windows.
+"""
+import contextlib
+import time
+
+import numpy as np
+import torch
+
+from . import engine as E
+from .geometry import Spec2D, build_2d
+
+
+def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
+    """DFT window over the last `periods` periods (steps_per_T = round(T/dt),
+    fdtd2d_core.py:757-758) and the snapshot steps (after steps n with
+    (n + 1) % snap_every == 0)."""
+    n = int(steps_total)
+    steps_per_T = max(4, int(round((1.0 / sp.f0) / sp.dt)))
+    n_acc = min(n, int(periods) * steps_per_T)
+    snaps = list(range(snap_every, n + 1, snap_every)) if snap_every else []
+    return dict(omega=2 * np.pi * sp.f0, steps_per_T=steps_per_T, n_acc=n_acc, dft=(n - n_acc, n), snaps=snaps)
+
+
+class Solve2D:
+    """Resident 2D solve of `steps_total` steps on the single-grid engine."""
+
+    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None):
+        self.spec = sp = spec
+        self.steps_total = int(steps_total)
+        t0 = time.perf_counter()
+        self.geo = g = geo if geo is not None else build_2d(sp)
+        self.t_setup_host = time.perf_counter() - t0
+        sc = schedule_2d(sp, steps_total, periods, snap_every)
+        self.omega, self.steps_per_T, self.n_acc = sc['omega'], sc['steps_per_T'], sc['n_acc']
+        self.dft, self.snap_steps = sc['dft'], sc['snaps']
+        coef = {k: g[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if g.get(k) is not None}
+        self.grid = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, g['cx'], g['cy'], g['src'], device=device)
+        self.h2d_bytes = sum(np.asarray(a).nbytes for a in coef.values()) + \
+            sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
+        self.table = E.StepTable(0, self.steps_total, sp.dt, g['src']['omega'], self.omega,
+                                 E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
+        self.epi = E.Epi2D(self.grid, dft=self.dft)
+        self.comp = 'ez' if self.grid.pol == 's' else 'ey'
+        v = self.grid.view(self.comp)
+        self.snaps = torch.zeros((len(self.snap_steps),) + tuple(v.shape), dtype=torch.float32, device=v.device)
+        self.n = 0
+
+    def run(self, stream=None):
+        """Advance to the end of the schedule, copying the snapshots on the way."""
+        n = self.n
+        with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+            for q, m in enumerate(self.snap_steps + [self.steps_total]):
+                if m > n:
+                    self.grid.step(self.table, n, m - n, self.epi, stream)
+                    n = m
+                if q < len(self.snap_steps):
+                    self.snaps[q].copy_(self.grid.view(self.comp))
+        self.n = n
+        return self
+
+    def phasor(self):
+        """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 on the device."""
+        return (2.0 / self.n_acc) * self.epi.phasor()
+
+    def host_results(self):
+        """Phasor (complex64, the reference's CW dtype) and snapshots (float32) on
+        the host; d2h_bytes counts what crossed."""
+        ph = self.phasor().to(torch.complex64).cpu().numpy()
+        snaps = self.snaps.cpu().numpy()
+        self.d2h_bytes = ph.nbytes + snaps.nbytes
+        return ph, snaps
+

@@ -31,6 +31,43 @@ def guard_in_plane(i_in, src_ix, n_max, margin=5):
     return int(i_in) if i_in >= lo else min(lo, int(n_max) - 2)
 
 
+def schedule_3d(sp: Spec3D, steps_total, x_facet_um):
+    """The run_3d schedule of a solve of `steps_total` steps (torch-free, so the
+    oracle's FP64 replay of a workload uses the same windows and boxes):
+    steady-state DFT over the last 8 periods and the convergence window before
+    it (fdtd3d_core.py:757-758, 1150-1175), |E|^2 every steps_per_T // 8 steps
+    of the second half (:1144-1148), the input / output detector boxes
+    (:1038-1062, the input box kept downstream of the source and facet) and the
+    flux planes.  x_facet_um: the entry facet (geometry.build_3d)."""
+    Nx = sp.nx
+    dx_um = sp.dx_nm / 1000.0
+    f0 = sp.f0
+    n = int(steps_total)
+    steps_per_T = max(4, int(round((1.0 / f0) / sp.dt)))
+    n_acc = min(n, 8 * steps_per_T)
+    y0_um = -sp.tear_um
+    j_wg0 = int(round((0.0 - y0_um) / dx_um))
+    j_wg1 = int(round((sp.stack.t_wg_um - y0_um) / dx_um))
+    hw = max(2, int(round(1.0 / dx_um)))
+    lx = Nx * dx_um
+
+    def xr(xu):
+        c = int(round(xu / dx_um))
+        return max(0, c - hw), min(Nx, c + hw)
+    iin0, iin1 = xr(0.2 * lx)
+    iout0, iout1 = xr(0.8 * lx)
+    ci = (iin0 + iin1) // 2
+    sh = guard_in_plane(ci, max(sp.src_ix, int(round(x_facet_um / dx_um))), Nx) - ci
+    iin0, iin1 = iin0 + sh, min(Nx, iin1 + sh)
+    nsp = sp.n_sp
+    return dict(omega=2 * np.pi * f0, steps_per_T=steps_per_T, n_acc=n_acc, dft=(n - n_acc, n),
+                prev=(max(0, n - 2 * n_acc), n - n_acc), n_avg0=n // 2, m_I=max(1, steps_per_T // 8),
+                # z range slice(n_sp, -n_sp) of each component (fdtd3d_core.py:1139-1142)
+                boxes=[(iin0, iin1, j_wg0, j_wg1, nsp, -nsp), (iout0, iout1, j_wg0, j_wg1, nsp, -nsp)],
+                planes={'in': max(1, (iin0 + iin1) // 2), 'out': max(1, (iout0 + iout1) // 2),
+                        'src_up': sp.src_ix - 1, 'src_dn': sp.src_ix + 3})
+
+
 class Solve3D:
     """Resident 3D solve.  comps: components whose phasor is accumulated
     (0 Ex, 1 Ey, 2 Ez; default the driven one)."""
@@ -48,35 +85,12 @@ class Solve3D:
                              src_comp=sp.src_comp, fused=fused, device=device)
         self.h2d_bytes = sum(a.nbytes for a in g['ce']) + (0 if g['da'] is None else sum(a.nbytes for a in g['da'])) \
             + sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
+        sc = schedule_3d(sp, self.steps_total, g['x_facet_um'])
+        self.omega, self.steps_per_T, self.n_acc = sc['omega'], sc['steps_per_T'], sc['n_acc']
+        self.dft, self.prev, self.n_avg0, self.m_I = sc['dft'], sc['prev'], sc['n_avg0'], sc['m_I']
+        self.boxes, self.planes = sc['boxes'], sc['planes']
         f0 = sp.f0
-        self.omega = 2 * np.pi * f0
-        self.steps_per_T = max(4, int(round((1.0 / f0) / sp.dt)))
         n = self.steps_total
-        self.n_acc = min(n, 8 * self.steps_per_T)
-        self.dft = (n - self.n_acc, n)
-        self.prev = (max(0, n - 2 * self.n_acc), n - self.n_acc)
-        self.n_avg0 = n // 2
-        self.m_I = max(1, self.steps_per_T // 8)
-        # detector boxes (fdtd3d_core.py:1038-1062)
-        y0_um = -sp.tear_um
-        j_wg0 = int(round((0.0 - y0_um) / dx_um))
-        j_wg1 = int(round((sp.stack.t_wg_um - y0_um) / dx_um))
-        hw = max(2, int(round(1.0 / dx_um)))
-        lx = Nx * dx_um
-
-        def xr(xu):
-            c = int(round(xu / dx_um))
-            return max(0, c - hw), min(Nx, c + hw)
-        iin0, iin1 = xr(0.2 * lx)
-        iout0, iout1 = xr(0.8 * lx)
-        ci = (iin0 + iin1) // 2
-        sh = guard_in_plane(ci, max(sp.src_ix, int(round(g['x_facet_um'] / dx_um))), Nx) - ci
-        iin0, iin1 = iin0 + sh, min(Nx, iin1 + sh)
-        nsp = sp.n_sp
-        # z range slice(n_sp, -n_sp) of each component (fdtd3d_core.py:1139-1142)
-        self.boxes = [(iin0, iin1, j_wg0, j_wg1, nsp, -nsp), (iout0, iout1, j_wg0, j_wg1, nsp, -nsp)]
-        self.planes = {'in': max(1, (iin0 + iin1) // 2), 'out': max(1, (iout0 + iout1) // 2),
-                       'src_up': sp.src_ix - 1, 'src_dn': sp.src_ix + 3}
         self.comps = tuple(comps) if comps is not None else (sp.src_comp,)
         src_shape = (Ny - 1, Nz) if sp.src_comp == 1 else (Ny, Nz - 1)
         self.kc = src_shape[1] // 2

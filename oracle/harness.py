@@ -43,7 +43,8 @@ def setup_2d(c):
     stack = [(t, _cplx(n)) for t, n in c['stack']]
     T_WG = c['wg_um'] * 1e-6
     r = c['bead']['d_um'] * 1e-6 / 2.0
-    bead = dict(xc=c['bead']['x_um'] * 1e-6, yc=-r, r=r, n=c.get('bead_n', 1.59))
+    yc = c['bead']['y_um'] * 1e-6 if c['bead'].get('y_um') is not None else -r
+    bead = dict(xc=c['bead']['x_um'] * 1e-6, yc=yc, r=r, n=c.get('bead_n', 1.59))
     tm = c['pol'] == 'p'
     eps, sig, patch = O.materials_2d(Nx, Ny, dx, -c['tear_m'], c['wg_n'], T_WG, stack, c['n_sub'],
                                      bead, x_wg=(x_facet_um * 1e-6, Nx * dx * 1e6 * 1e-6),

@@ -3,7 +3,7 @@
 Run from the repository root, in a container where the reference checkout is
 available (it is read only, nothing is written there):
 
-    LENS_REF=/root/reference python tests/golden/make_golden.py
+    LENS_REF=<path of the reference checkout> python tests/golden/make_golden.py
 
 The reference (s1alknau/lens_sensor) is pure NumPy here (CuPy absent), so its
 primitives are imported and driven for a fixed number of steps in the loop order
@@ -45,7 +45,9 @@ import tempfile
 
 import numpy as np
 
-REF = os.environ.get('LENS_REF', '/root/reference')
+REF = os.environ.get('LENS_REF')
+if not REF or not os.path.isdir(REF):
+    raise SystemExit('set LENS_REF to the path of the reference (s1alknau/lens_sensor) checkout')
 OUT = os.path.dirname(os.path.abspath(__file__))
 os.environ['PYTHONDONTWRITEBYTECODE'] = '1'
 sys.dont_write_bytecode = True

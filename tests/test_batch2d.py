@@ -162,3 +162,45 @@ def test_overlap_uses_the_analyzer_windows():
         band = lambda a, b: float(np.mean(np.sum(I[dl:dh, a:b], axis=1))) if b > a else 0.0
         want = band(tl, lo) / band(lo, hi)
         assert got == pytest.approx(want, rel=1e-12), (sp.nx, sp.ny, got, want)
+
+
+class _FakeSweep:
+    """Stand-in for batch2d.Sweep: instance q's phasor is q + 1, and reduced
+    storage adds a relative error of 1e-6 (TE) or 1e-3 (TM)."""
+    runs = []
+
+    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None):
+        self.specs, self.storage = specs, storage
+        _FakeSweep.runs.append((storage, [sp.tag for sp in specs]))
+
+    def run(self):
+        return 0
+
+    def results(self):
+        import torch
+        out = []
+        for sp in self.specs:
+            e = 0.0 if self.storage == 'f32' else (1e-6 if sp.pol == 's' else 1e-3)
+            out.append(dict(phasor=torch.full((4,), complex(sp.tag + 1, 0) * (1 + e), dtype=torch.complex128)))
+        return out
+
+
+def test_fp16_gate_accepts_per_polarisation(monkeypatch):
+    """The gate probes every 4th instance of each polarisation in both storages,
+    keeps FP16 for the TE instances (probe error 1e-6 <= tol/2) and runs the TM
+    instances in FP32 (1e-3 > tol/2); probes keep their FP32 results."""
+    from types import SimpleNamespace
+    from lens_sensor_b200 import batch2d as B
+    monkeypatch.setattr(B, 'Sweep', _FakeSweep)
+    _FakeSweep.runs = []
+    specs = [SimpleNamespace(pol='s' if q % 2 == 0 else 'p', tag=q) for q in range(16)]
+    res, rep = B.gated_sweep(specs, 10, 'f16', tol=1e-4, probe_every=4, geos=[None] * 16)
+    assert rep['accepted'] == {'s': True, 'p': False}
+    probes = [p['index'] for p in rep['probes']]
+    assert probes == [0, 1, 8, 9]
+    assert all(res[q]['storage'] == 'f32' for q in probes)
+    assert all(res[q]['storage'] == ('f16' if q % 2 == 0 else 'f32') for q in range(16) if q not in probes)
+    assert rep['n_reduced'] == 6 and rep['n_f32'] == 10
+    assert all(float(r['phasor'][0].real) == pytest.approx(q + 1, rel=2e-6) for q, r in enumerate(res))
+    # both storages of the probes, then the accepted and the refused rest
+    assert [r[0] for r in _FakeSweep.runs] == ['f32', 'f16', 'f16', 'f32']

@@ -239,6 +239,47 @@ int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, c
 int lens_batch2d_step_noalloc(const LensInst2D *inst, int ninst, int storage, int by,
                               const LensStepTable *tab, int n0, int nsteps, void *stream);
 
+/* ------------------------------------------- temporally blocked 2D solves
+ * The batched 2D step with LENS_TB_K time steps per launch: each field value
+ * crosses HBM once per K steps instead of once per step.  A warp streams a tile
+ * of 128 columns (y) down a chunk of rows (x) and advances K time levels held
+ * in registers, one row behind the other; the K columns on each side of the
+ * tile and the K rows before and after the chunk are recomputed halo.  Fields
+ * and psi are double-buffered: a launch reads buffer `b` and writes buffer
+ * 1 - b, starting from buffer 0, so nsteps must be a multiple of 2*K and the
+ * state ends in buffer 0 again.  The CPML psi of the K-1 intermediate levels
+ * live in a scratch array.  Epilogue: the node-field DFT of LensInst2D (Ez for
+ * TE, Ey on the nodes for TM) over its window, accumulated as (re, im) or, with
+ * dft_kahan, compensated (re, im, c_re, c_im) as the single-grid epilogue
+ * does.  Every instance must have started (n_start <= n0).                  */
+#define LENS_TB_K 4
+
+typedef struct {
+    LensInst2D g;                /* the instance; g.f and g.psi are buffer 0    */
+    void *f1[3];                 /* buffer 1 of the fields (same layout as g.f) */
+    float *psi1[4];              /* buffer 1 of the psi arrays (shapes of g.psi) */
+    float *psi_lv;               /* scratch of the intermediate psi levels:
+                                    (LENS_TB_K - 1) x the sum of the four psi
+                                    array sizes (x strips w x pitch, y strips
+                                    nx x w; an empty strip takes no space), or
+                                    NULL when the instance has no strip        */
+    int dft_kahan;               /* g.dft layout: 1 (re, im, c_re, c_im), 0 (re, im) */
+} LensTB2D;
+
+/* Units (warps) of a temporally blocked batch with row chunks of `chunk` rows:
+ * writes first[0..ninst] (first unit of each instance) and returns the unit
+ * count, or < 0. */
+int lens_tb2d_plan(const LensTB2D *inst, int ninst, int chunk, int *first);
+
+/* Advance every instance by nsteps (a multiple of 2 * LENS_TB_K) from batch
+ * step n0, LENS_TB_K steps per launch.  inst_host / inst_dev: the same
+ * descriptors in host and device memory; first_dev: the plan's first[] in
+ * device memory; storage: LENS_F32 / LENS_F16 / LENS_BF16 (all arithmetic
+ * FP32).  Replaces the per-step loop of fdtd2d_core.py:781-847 (no counterpart
+ * entry in the reference, which advances one step per call).                */
+int lens_tb2d_step(const LensTB2D *inst_host, const LensTB2D *inst_dev, const int *first_dev, int ninst,
+                   int chunk, int storage, const LensStepTable *tab, int n0, int nsteps, void *stream);
+
 /* ---------------------------------------------------------------- 3D grid */
 /* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
  * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same
@@ -268,8 +309,9 @@ typedef struct {
     int pec[6];                  /* PEC on x-lo, x-hi, y-lo, y-hi, z-lo, z-hi  */
     LensSource src;              /* plane (nj, nk) of the driven component     */
     int src_comp;                /* 0 Ex, 1 Ey, 2 Ez                           */
-    int *flag;                   /* optional device int, set nonzero when a
-                                    pipeline wait gave up (results invalid)    */
+    int *flag;                   /* optional device int: bit 1 set when a
+                                    pipeline wait gave up, bit 2 when a detector
+                                    box sum was not finite (results invalid)   */
     /* Optional column form of the six coefficient volumes (NULL ctype: the
        fused step reads every coefficient from the volumes).  A layered slab
        repeats a few coefficient columns (over y) at almost every (x, z): the
@@ -321,6 +363,17 @@ int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *e
 int lens_fdtd3d_step_driven(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
                             const LensDrive3D *drive, int n0, int nsteps, void *stream);
 
+/* Self-test of the fused step's failure detection (no counterpart in the
+ * reference, whose NumPy loop has no device waits): one fused step in which the
+ * first CTA of the launch withholds the E copy of one x-plane of its chunk (the
+ * plane `offset` = 0 or 1 after the first plane it stages) and every pipeline
+ * wait is bounded at 256 tries instead of about a second, so that CTA's waits
+ * run out: it stops, drains its copies in flight, sets bit 1 of *g->flag and
+ * returns, and the launch ends normally.  The step's results are invalid; the
+ * grid and the context stay usable (reset the flag, restore the fields).
+ * Needs the fused path (buffer 1) and g->flag.                              */
+int lens_fdtd3d_watchdog_test(LensGrid3D *g, const LensStepTable *tab, int n0, int offset, void *stream);
+
 /* Iavg += |E|^2 of all three components mapped onto the grid of component
  * `target` (1 Ey, 2 Ez) exactly as fdtd3d_core.py:438-474 (_sq_on_grid/_accum_E2),
  * over the x-planes [0, nx_target) of the slices Ex[:nx_target-1], Ey[:nx_target],
@@ -334,8 +387,8 @@ const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
  * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D,
- * LensDrive3D, LensDrive2D.  Writes min(n, 12) entries and returns 12 (bindings
- * check their mirrors). */
+ * LensDrive3D, LensDrive2D, LensTB2D.  Writes min(n, 13) entries and returns 13
+ * (bindings check their mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

@@ -97,6 +97,14 @@ class Inst2D(ctypes.Structure):
                 ('rtype', c_void_p), ('ctab', c_void_p)]
 
 
+class TB2D(ctypes.Structure):
+    _fields_ = [('g', Inst2D), ('f1', c_void_p * 3), ('psi1', c_void_p * 4), ('psi_lv', c_void_p),
+                ('dft_kahan', c_int)]
+
+
+TB_K = 4
+
+
 class Drive3D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p * 3)]
 
@@ -105,7 +113,7 @@ class Drive2D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p), ('tab', c_void_p)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D)
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D, TB2D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
@@ -120,11 +128,15 @@ SIGNATURES = {
     'lens_fdtd3d_step_driven': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), POINTER(Drive3D),
                                         c_int, c_int, c_void_p]),
     'lens_fdtd3d_accum_e2': (c_int, [POINTER(Grid3D), c_int, c_int, c_void_p, c_void_p]),
+    'lens_fdtd3d_watchdog_test': (c_int, [POINTER(Grid3D), POINTER(StepTable), c_int, c_int, c_void_p]),
     'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
     'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                   POINTER(StepTable), c_int, c_int, c_void_p]),
     'lens_batch2d_step_noalloc': (c_int, [POINTER(Inst2D), c_int, c_int, c_int, POINTER(StepTable), c_int,
                                           c_int, c_void_p]),
+    'lens_tb2d_plan': (c_int, [POINTER(TB2D), c_int, c_int, POINTER(c_int)]),
+    'lens_tb2d_step': (c_int, [POINTER(TB2D), c_void_p, c_void_p, c_int, c_int, c_int, POINTER(StepTable), c_int,
+                               c_int, c_void_p]),
     'lens_version': (c_int, []),
     'lens_status_string': (ctypes.c_char_p, [c_int]),
     'lens_abi_sizes': (c_int, [POINTER(c_int), c_int]),

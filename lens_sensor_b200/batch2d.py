@@ -62,9 +62,14 @@ def row_types(arrays, shape, dev, min_rows=8):
 
 
 class Instance:
-    """Device state of one 2D solve in a batch."""
+    """Device state of one 2D solve in a batch.
 
-    def __init__(self, sp, steps, dtype, dev, geo=None):
+    tb: also the second field / psi buffers and the psi level scratch of the
+    temporally blocked step (lens_tb2d_step); kahan: a compensated DFT
+    accumulator (re, im, c_re, c_im) instead of (re, im); window: the DFT steps
+    (default the last 8 periods)."""
+
+    def __init__(self, sp, steps, dtype, dev, geo=None, tb=False, kahan=False, window=None):
         self.spec, self.steps = sp, int(steps)
         geo = build_2d(sp) if geo is None else geo
         self.geo = geo
@@ -92,9 +97,14 @@ class Instance:
         self.omega = src['omega']
         f0 = sp.f0
         self.steps_per_T = max(4, int(round((1.0 / f0) / sp.dt)))
-        self.n_acc = min(self.steps, 8 * self.steps_per_T)
-        self.window = (self.steps - self.n_acc, self.steps)
-        self.dft = torch.zeros((nx, P, 2), dtype=torch.float32, device=dev)
+        if window is None:
+            self.n_acc = min(self.steps, 8 * self.steps_per_T)
+            self.window = (self.steps - self.n_acc, self.steps)
+        else:
+            self.window = (int(window[0]), int(window[1]))
+            self.n_acc = self.window[1] - self.window[0]
+        self.kahan = bool(kahan)
+        self.dft = torch.zeros((nx, P, 4 if self.kahan else 2), dtype=torch.float32, device=dev)
         s = N.Inst2D()
         s.pol, s.nx, s.ny, s.pitch = self.pol, nx, ny, P
         for q in range(3):
@@ -113,18 +123,48 @@ class Instance:
         if self.rtype is not None:
             s.rtype, s.ctab = self.rtype.data_ptr(), self.ctab.data_ptr()
         self.s = s
+        self.tb = None
+        if tb:
+            self._tb_buffers(dtype, dev)
+
+    def _tb_buffers(self, dtype, dev):
+        """Second buffers of the fields and psi, and the scratch of the K - 1
+        intermediate psi levels (x strips (w, pitch), y strips (nx, w))."""
+        nx, P = self.spec.nx, self.pitch
+        self.f1 = [torch.zeros_like(t) for t in self.f]
+        self.psi1 = [torch.zeros_like(t) for t in self.psi]
+        w = [self.axy.w('h'), self.axx.w('h'), self.axx.w('e'), self.axy.w('e')] if self.pol == 0 else \
+            [self.axx.w('h'), self.axy.w('h'), self.axy.w('e'), self.axx.w('e')]
+        xs = [False, True, True, False] if self.pol == 0 else [True, False, False, True]
+        tot = sum((wq * P if x else nx * wq) for wq, x in zip(w, xs))
+        self.psi_lv = torch.zeros(max(1, (N.TB_K - 1) * tot), dtype=torch.float32, device=dev)
+        t = N.TB2D()
+        t.g = self.s
+        for q in range(3):
+            t.f1[q] = self.f1[q].data_ptr()
+        for q in range(4):
+            t.psi1[q] = self.psi1[q].data_ptr()
+        t.psi_lv = self.psi_lv.data_ptr()
+        t.dft_kahan = 1 if self.kahan else 0
+        self.tb = t
+
+    def _state(self):
+        extra = (self.f1 + self.psi1 + [self.psi_lv]) if self.tb is not None else []
+        return self.f + self.psi + [self.dft] + extra
 
     def nbytes(self):
-        t = self.f + self.c + self.psi + [self.dft] + ([self.ctab] if self.ctab is not None else [])
+        t = self._state() + self.c + ([self.ctab] if self.ctab is not None else [])
         return sum(x.numel() * x.element_size() for x in t)
 
     def reset(self):
-        for t in self.f + self.psi + [self.dft]:
+        for t in self._state():
             t.zero_()
 
     def phasor(self):
         """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 (fdtd2d_core.py:879)."""
         a = self.dft[:, :self.spec.ny].double()
+        if self.kahan:
+            return (2.0 / self.n_acc) * torch.complex(a[..., 0] - a[..., 2], a[..., 1] - a[..., 3])
         return (2.0 / self.n_acc) * torch.complex(a[..., 0], a[..., 1])
 
     def overlap(self, ph=None):
@@ -151,13 +191,29 @@ class Instance:
 
 
 class Group:
-    """Instances advanced by the same batched launches."""
+    """Instances advanced by the same batched launches (tb: the temporally
+    blocked step, LENS_TB_K steps per launch, warps over `chunk` rows)."""
 
-    def __init__(self, insts, storage, by, dev):
+    def __init__(self, insts, storage, by, dev, tb=False, chunk=64):
         self.insts, self.storage, self.by, self.dev = insts, storage, by, dev
         n = len(insts)
-        self.host = (N.Inst2D * n)(*[q.s for q in insts])
         self.lib = N.load()
+        self.tb, self.chunk = bool(tb), int(chunk)
+        self.steps = max(q.steps for q in insts)
+        self.graph = None
+        if self.tb:
+            self.host = (N.TB2D * n)(*[q.tb for q in insts])
+            first = (ctypes.c_int * (n + 1))()
+            nu = self.lib.lens_tb2d_plan(self.host, n, self.chunk, first)
+            N.check(min(0, nu))
+            self.nunits = nu
+            raw = ctypes.string_at(ctypes.addressof(self.host), ctypes.sizeof(self.host))
+            self.dev_desc = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
+            self.dev_first = torch.tensor(list(first), dtype=torch.int32, device=dev)
+            return
+        if any(q.kahan for q in insts):
+            raise ValueError('the single-step batched kernels accumulate (re, im) DFTs: no compensated instances')
+        self.host = (N.Inst2D * n)(*[q.s for q in insts])
         blk = (ctypes.c_int * (n + 1))()
         nblk = self.lib.lens_batch2d_plan(self.host, n, int(by), blk, None)
         N.check(min(0, nblk))
@@ -168,10 +224,14 @@ class Group:
         self.dev_desc = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
         self.dev_blk = torch.tensor(list(blk), dtype=torch.int32, device=dev)
         self.dev_owner = torch.frombuffer(bytearray(owner), dtype=torch.int32).to(dev)
-        self.steps = max(q.steps for q in insts)
-        self.graph = None
 
     def step(self, tab, n0, nsteps, stream=None):
+        if self.tb:
+            N.check(self.lib.lens_tb2d_step(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()),
+                                            ctypes.c_void_p(self.dev_first.data_ptr()), len(self.insts), self.chunk,
+                                            self.storage, ctypes.byref(tab.s), int(n0), int(nsteps),
+                                            E._stream_ptr(stream)))
+            return
         N.check(self.lib.lens_batch2d_step(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()),
                                            ctypes.c_void_p(self.dev_blk.data_ptr()),
                                            ctypes.c_void_p(self.dev_owner.data_ptr()), len(self.insts),
@@ -179,7 +239,10 @@ class Group:
                                            E._stream_ptr(stream)))
 
     def launches(self, n0, n1):
-        """Kernel launches of steps [n0, n1): H and E, plus the TM node DFT on window steps."""
+        """Kernel launches of steps [n0, n1): H and E, plus the TM node DFT on window
+        steps; one per LENS_TB_K steps for the temporally blocked step."""
+        if self.tb:
+            return (n1 - n0) // N.TB_K
         tm = [q.window for q in self.insts if q.pol == 1]
         extra = sum(1 for n in range(n0, n1) if any(a <= n < b for a, b in tm))
         return 2 * (n1 - n0) + extra
@@ -203,8 +266,12 @@ class Sweep:
     storage: 'f32' | 'f16' | 'bf16'.  by: rows per 32-lane tile; budget: bytes of
     resident state per group (None: one group).  autotune() chooses both."""
 
-    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None):
+    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None, tb=False,
+                 chunk=64):
         dev = self.dev = E._device(device)
+        self.tb, self.chunk = bool(tb), int(chunk)
+        if self.tb and int(steps) % (2 * N.TB_K):
+            raise ValueError(f'the temporally blocked sweep runs in spans of {2 * N.TB_K} steps')
         if storage not in DTYPES:
             raise ValueError(f'storage {storage!r}: one of {sorted(DTYPES)}')
         self.storage_name = storage
@@ -215,7 +282,7 @@ class Sweep:
             raise ValueError('a batched sweep shares one time step and one wavelength')
         self.steps = int(steps)
         geos = geos if geos is not None else [None] * len(specs)
-        self.insts = [Instance(sp, steps, dtype, dev, geo) for sp, geo in zip(specs, geos)]
+        self.insts = [Instance(sp, steps, dtype, dev, geo, tb=self.tb) for sp, geo in zip(specs, geos)]
         sp0 = specs[0]
         self.table = E.StepTable(0, self.steps, sp0.dt, self.insts[0].omega, 2 * np.pi * sp0.f0,
                                  E.cw_envelope(sp0.f0, sp0.ramp_periods), device=dev)
@@ -235,7 +302,7 @@ class Sweep:
             size += b
         if cur:
             groups.append(cur)
-        return [Group(g, self.storage, by, self.dev) for g in groups]
+        return [Group(g, self.storage, by, self.dev, tb=self.tb, chunk=self.chunk) for g in groups]
 
     def cells(self):
         return sum(q.spec.nx * q.spec.ny for q in self.insts)
@@ -247,7 +314,10 @@ class Sweep:
     def autotune(self, candidates=((8, None), (4, None), (8, 96 << 20), (4, 96 << 20), (8, 48 << 20), (2, 96 << 20)),
                  probe_steps=24):
         """Time `probe_steps` batched steps of every (rows per tile, group budget)
-        candidate on this sweep, keep the fastest, reset the fields."""
+        candidate on this sweep, keep the fastest, reset the fields.  The
+        temporally blocked sweep tunes (rows per chunk, group budget) instead."""
+        if self.tb:
+            return self._autotune_tb()
         res = []
         for by, budget in candidates:
             groups = self._groups(by, budget)
@@ -264,6 +334,29 @@ class Sweep:
         self.by, self.budget = best[1], best[2]
         self.groups = self._groups(self.by, self.budget)
         self.tuned = [dict(by=b, budget=u, s_per_step=t) for t, b, u in res]
+        return self.tuned
+
+    def _autotune_tb(self, candidates=((64, None), (32, None), (128, None), (64, 96 << 20), (32, 96 << 20),
+                                       (16, None)), probe_steps=24):
+        span = 2 * N.TB_K
+        probe_steps = max(span, probe_steps // span * span)
+        res = []
+        for chunk, budget in candidates:
+            self.chunk = chunk
+            groups = self._groups(self.by, budget)
+            for g in groups:              # warm-up
+                g.step(self.table, 0, span)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for g in groups:
+                g.step(self.table, span, probe_steps)
+            torch.cuda.synchronize()
+            res.append(((time.perf_counter() - t0) / probe_steps, chunk, budget))
+        self.reset()
+        best = min(res, key=lambda r: r[0])
+        self.chunk, self.budget = best[1], best[2]
+        self.groups = self._groups(self.by, self.budget)
+        self.tuned = [dict(chunk=c, budget=u, s_per_step=t) for t, c, u in res]
         return self.tuned
 
     def run(self, graphs=True):

@@ -48,6 +48,7 @@ struct K3 {
     const unsigned char *ctype, *cexpl;  // coefficient column form (LensGrid3D)
     const float *ctab;
     int ntype;
+    int wd_plane;  // watchdog self-test: offset of the plane whose E copy CTA 0 withholds (-1: normal step)
 };
 
 struct Hv {
@@ -435,9 +436,9 @@ __device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
 // Bounded wait for phase `parity` of an mbarrier; false if it gave up.  Each
 // try_wait may suspend the thread for up to 1 us (suspend-time hint), so the
 // bound (2^20 tries) is about a second.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int tries = 1 << 20) {
     uint32_t ok = 0;
-    for (int t = 0; t < (1 << 20) && !ok; ++t) {
+    for (int t = 0; t < tries && !ok; ++t) {
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
             " selp.u32 %0, 1, 0, p;\n}\n"
@@ -827,9 +828,17 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     // (bounded) before the CTA exits.
     bool ok = true;
     int ie = xs - 1, we = xs - 1, ih = xs - 1, wh = xs - 1;
+    // watchdog self-test (lens_fdtd3d_watchdog_test): CTA 0 withholds one plane's
+    // E copy and every wait of the launch is bounded at a few hundred tries
+    const bool wd = g.wd_plane >= 0;
+    const int tries = wd ? 256 : (1 << 20);
     auto issue_e = [&](int p) {
         const int s = (p - xs) % NSE;
         const uint32_t bar = bar0 + 8u * s;
+        if (wd && blockIdx.x == 0 && p == xs + g.wd_plane) {
+            ie = p;  // never armed: the waits on this plane run out
+            return;
+        }
         mbar_expect(bar, 3 * E_BYTES);
 #pragma unroll
         for (int q = 0; q < 3; ++q) tma3(sbase + (s * 3 + q) * E_SLOT, &tm.e[q], k0 - 4, j0 - 1, p, bar);
@@ -951,7 +960,7 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
     float cya = 0.f, cza = 0.f, cyb = 0.f, czb = 0.f;
     float hyma = 0.f, hzma = 0.f, hymb = 0.f, hzmb = 0.f;  // new H(i-1)
     __syncthreads();  // the mbarriers are initialised
-    if (ok) ok = mbar_wait(bar0, 0u);  // E(xs)
+    if (ok) ok = mbar_wait(bar0, 0u, tries);  // E(xs)
     if (prod && ok) we = xs;
     if (owner) {  // plane xs sits in slot 0
         cya = sE[EF + ea];
@@ -965,8 +974,8 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         const unsigned u = i - xs;
         const unsigned tc = tcn;  // column type of (i, k)
         if (owner && ccol && i + 1 < x1) tcn = ldg_u8_early(g.ctype + (IX)(i + 1) * P + k);
-        if (ok) ok = mbar_wait(bar0 + 8u * sn, pn);   // E(i+1)
-        if (ok) ok = mbar_wait(barh + 8u * sh, ph);   // HC(i)
+        if (ok) ok = mbar_wait(bar0 + 8u * sn, pn, tries);   // E(i+1)
+        if (ok) ok = mbar_wait(barh + 8u * sh, ph, tries);   // HC(i)
         if (prod && ok) { we = i + 1; wh = i; }
         const float *eC = sE + se * 3 * EF, *eN = sE + sn * 3 * EF;
         const float *hc = sHC + sh * (HC_SLOT / 4);
@@ -1077,11 +1086,11 @@ __device__ __forceinline__ void tile3d(const EMaps &tm, const K3 &g, const LensS
         if (++sn == NSE) { sn = 0; pn ^= 1u; }
         if (++sh == NHC) { sh = 0; ph ^= 1u; }
     }
-    if (!ok && g.flag) atomicExch(g.flag, 1);
+    if (!ok && g.flag) atomicOr(g.flag, 1);
     if (prod && !ok) {
-        for (int p = we + 1; p <= ie; ++p) mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1);
-        for (int p = wh + 1; p <= ih; ++p) mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1);
-        if (g.flag) atomicExch(g.flag, 1);
+        for (int p = we + 1; p <= ie; ++p) mbar_wait(bar0 + 8u * ((p - xs) % NSE), ((p - xs) / NSE) & 1, tries);
+        for (int p = wh + 1; p <= ih; ++p) mbar_wait(barh + 8u * ((p - xs) % NHC), ((p - xs) / NHC) & 1, tries);
+        if (g.flag) atomicOr(g.flag, 1);
     }
 }
 
@@ -1214,6 +1223,8 @@ __global__ void __launch_bounds__(NT) box3d(const K3 g, const LensEpi3D ep, cons
         v = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
         v = warp_sum(v);
         if (threadIdx.x == 0 && v != 0.0) atomicAdd(ep.box_acc + b, v);
+        // a NaN or infinity in a detector box marks the solve invalid (flag bit 2)
+        if (threadIdx.x == 0 && g.flag && !isfinite(v)) atomicOr(g.flag, 2);
     }
 }
 
@@ -1379,6 +1390,7 @@ K3 view(const LensGrid3D *g, int rb, int wb) {
     for (int q = 0; q < 6; ++q) k.pec[q] = g->pec[q];
     k.src = g->src; k.src_comp = g->src_comp; k.flag = g->flag;
     k.ctype = g->ctype; k.cexpl = g->cexpl; k.ctab = g->ctab; k.ntype = g->ntype;
+    k.wd_plane = -1;
     return k;
 }
 
@@ -1553,7 +1565,7 @@ bool drive3d_ok(const LensDrive3D *d, const LensStepTable *t, const LensGrid3D *
 // Steps [n0, n0+nsteps): the Yee update (source included), then the optional
 // stitch drive on the new E, then the epilogue that reads the new E.
 int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const LensDrive3D *dr, int n0,
-           int nsteps, void *stream) {
+           int nsteps, void *stream, int wd_plane = -1) {
     if (!grid3d_ok(g) || nsteps < 0 || !lens_table_ok(tab, n0, nsteps) || !epi3d_ok(ep, tab, g) ||
         !drive3d_ok(dr, tab, g, ep))
         return LENS_ERR_ARG;
@@ -1628,7 +1640,8 @@ int step3d(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep, const L
     const dim3 grd_w((g->pitch + BK * WK - 1) / (BK * WK), (g->ny + BJ - 1) / BJ, g->nx);
     for (int n = n0; n < n0 + nsteps; ++n) {
         const int rb = g->cur;
-        const K3 k = view(g, rb, 1 - rb);
+        K3 k = view(g, rb, 1 - rb);
+        k.wd_plane = wd_plane;
         const int ea = epi3d_active(&e, n);
         if (ix32)
             yee3d<uint32_t><<<nblk, dim3(TK, NW3), SMEM3, s>>>(tm[rb], k, *tab, e, n, ea, wk);
@@ -1657,6 +1670,11 @@ extern "C" int lens_fdtd3d_step_driven(LensGrid3D *g, const LensStepTable *tab, 
     return step3d(g, tab, ep, drive, n0, nsteps, stream);
 }
 
+extern "C" int lens_fdtd3d_watchdog_test(LensGrid3D *g, const LensStepTable *tab, int n0, int offset, void *stream) {
+    if (!g || !g->flag || !has_buffer1(g) || offset < 0 || offset > 1) return LENS_ERR_ARG;
+    return step3d(g, tab, nullptr, nullptr, n0, 1, stream, offset);
+}
+
 extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, int nx_target, float *iavg, void *stream) {
     if (!grid3d_ok(g) || !iavg || (target != 1 && target != 2) || nx_target < 2 || nx_target > g->nx)
         return LENS_ERR_ARG;
@@ -1669,12 +1687,13 @@ extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, int nx_targ
 extern "C" int lens_version(void) { return 100; }
 
 extern "C" int lens_abi_sizes(int *sizes, int n) {
-    const int v[12] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
+    const int v[13] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
                        (int)sizeof(LensSource),  (int)sizeof(LensTE2D), (int)sizeof(LensTM2D),
                        (int)sizeof(LensEpi2D),   (int)sizeof(LensGrid3D), (int)sizeof(LensEpi3D),
-                       (int)sizeof(LensInst2D),  (int)sizeof(LensDrive3D), (int)sizeof(LensDrive2D)};
-    for (int q = 0; q < n && q < 12; ++q) sizes[q] = v[q];
-    return 12;
+                       (int)sizeof(LensInst2D),  (int)sizeof(LensDrive3D), (int)sizeof(LensDrive2D),
+                       (int)sizeof(LensTB2D)};
+    for (int q = 0; q < n && q < 13; ++q) sizes[q] = v[q];
+    return 13;
 }
 
 extern "C" const char *lens_status_string(int status) {

@@ -479,9 +479,13 @@ class Grid3D:
                                                      _stream_ptr(stream)))
 
     def check_flag(self):
-        """Raise if a pipeline wait in the fused kernel gave up (results invalid)."""
-        if int(self.flag.item()) != 0:
+        """Raise if a pipeline wait in the fused kernel gave up or a detector box
+        saw a NaN / infinity (results invalid)."""
+        f = int(self.flag.item())
+        if f & 1:
             raise N.LensError('fused 3D kernel: a pipeline wait timed out')
+        if f & 2:
+            raise N.LensError('3D solve: a detector box sum is not finite (the fields hold NaN or infinity)')
 
     def accum_e2(self, iavg, target=None, stream=None, nx=None):
         """iavg += |E|^2 on the driven component's grid over x-planes [0, nx)."""

@@ -45,7 +45,13 @@ from .stitch3d import StitchSolve
 @dataclass
 class Request:
     """kind '2d': spec = geometry.Spec2D; '3d': geometry.Spec3D; 'stitch':
-    stitch3d.StitchPlan (steps is then the per-window count of the plan)."""
+    stitch3d.StitchPlan (steps is then the per-window count of the plan).
+
+    status: 'waiting', 'running', 'done', or the request's end without a result:
+    'rejected' (its footprint exceeds the whole budget), 'cancelled'
+    (Server.cancel, or cancel_at seconds after the stream's start), 'failed'
+    (its host-side setup raised; error holds the message).  A request that ends
+    without a result frees its memory and slot; the others carry on."""
     rid: int
     kind: str
     spec: Any
@@ -56,6 +62,9 @@ class Request:
     t_done: Optional[float] = None
     footprint: int = 0
     result: Any = None
+    status: str = 'waiting'
+    error: Optional[str] = None
+    cancel_at: Optional[float] = None
 
     @property
     def latency(self):
@@ -87,6 +96,35 @@ def footprint(req, storage='f32'):
         lossy = s.stack.lossy or any(np.iscomplexobj(b.n) for b in s.beads)
         return cells * 4 * (2 * (6 + 12) + 3 + (3 if lossy else 0) + 2 + 1) + (1 << 20)
     return s.window_bytes()
+
+
+def admission(queue, used, budget, n2d, n3d, slots2d, slots3d):
+    """Which waiting requests to admit, in arrival order (`queue`): first fit
+    under the memory budget and the slot limits of their kind, except that the
+    oldest request that does not fit keeps its claim on the memory (later ones
+    are admitted only in what is left beside it), so a large job is not starved
+    by a run of small ones.  A request larger than the whole budget can never
+    run and is rejected.  Returns (admitted, rejected); changes nothing."""
+    admitted, rejected = [], []
+    held = 0
+    for r in queue:
+        if r.footprint > budget:
+            rejected.append(r)
+            continue
+        is2d = r.kind == '2d'
+        if not (n2d < slots2d if is2d else n3d < slots3d):
+            continue
+        if used + held + r.footprint > budget:
+            if held == 0:
+                held = r.footprint
+            continue
+        admitted.append(r)
+        used += r.footprint
+        if is2d:
+            n2d += 1
+        else:
+            n3d += 1
+    return admitted, rejected
 
 
 class _Batch2D:
@@ -132,12 +170,25 @@ class _Batch2D:
                 ph = q.phasor()
                 r.result = dict(phasor=ph.cpu(), K=q.overlap(ph))
                 r.t_done = time.perf_counter() - self.srv.t0
+                r.status = 'done'
                 self.srv.release(r)
             self.members = [m for m in self.members if m not in done]
         changed = bool(done)
+        gone = [(r, q) for r, q in self.members if r.status == 'cancelled']
+        for r, q in gone:
+            self.srv.release(r)
+        if gone:
+            self.members = [m for m in self.members if m not in gone]
+            changed = True
         ready = [(r, f) for r, f in self.building if f.done()]
         for r, f in ready:
             self.building.remove((r, f))
+            if r.status == 'cancelled':
+                self.srv.release(r)
+                continue
+            if f.exception() is not None:
+                self.srv.fail(r, f.exception())
+                continue
             self.joining.append((r, B.Instance(r.spec, r.steps, self.srv.dtype, self.srv.dev, f.result())))
         if self.joining:
             for r, q in self.joining:
@@ -158,6 +209,7 @@ class _Batch2D:
         for r, _ in self.members:
             if r.t_start is None:
                 r.t_start = now
+                r.status = 'running'
         self.n += k
         self.event = torch.cuda.Event()
         self.event.record(self.stream)
@@ -199,9 +251,16 @@ class _Job:
             return False
         self.event = None
         r = self.req
+        if r.status == 'cancelled':
+            self.solve = None
+            self.srv.release(r)
+            return True
         if self.solve is None:
             if not self.geo.done():
                 return False
+            if self.geo.exception() is not None:
+                self.srv.fail(r, self.geo.exception())
+                return True
             self._start()
         if r.kind == '3d':
             s = self.solve
@@ -221,12 +280,17 @@ class _Job:
             self.srv.launched += s.advance(self.srv.quantum3d)
         if r.t_start is None:
             r.t_start = now
+            r.status = 'running'
         self.event = torch.cuda.Event()
         self.event.record(self.stream)
         return True
 
+    def ended(self):
+        return self.req.status in ('done', 'cancelled', 'failed')
+
     def _finish(self):
         self.req.t_done = time.perf_counter() - self.srv.t0
+        self.req.status = 'done'
         self.solve = None
         self.srv.release(self.req)
 
@@ -259,23 +323,46 @@ class Server:
         self.used = 0
         self.t0 = 0.0
         self.launched = 0
+        self._cancel = set()
+        # host-side geometry builders (run on the pool; an exception fails only its request)
+        self.build2d, self.build3d = build_2d, build_3d
 
     def release(self, req):
-        self.used -= req.footprint
+        """Give back the memory of an admitted request that ended."""
+        if req.t_admit is not None and not getattr(req, '_released', False):
+            req._released = True
+            self.used -= req.footprint
+
+    def fail(self, req, exc):
+        """A request whose host-side setup raised: record it, free its memory."""
+        req.status, req.error = 'failed', f'{type(exc).__name__}: {exc}'
+        req.t_done = time.perf_counter() - self.t0
+        self.release(req)
+
+    def cancel(self, rid):
+        """Cancel request `rid`: a waiting request leaves the queue, a running
+        one stops at the end of its current quantum (its memory is freed then).
+        Safe to call from another thread while run() serves."""
+        self._cancel.add(int(rid))
+
+    def _cancels(self, reqs, queue, now):
+        for r in reqs:
+            if r.status in ('done', 'cancelled', 'failed', 'rejected'):
+                continue
+            if r.rid in self._cancel or (r.cancel_at is not None and now >= r.cancel_at):
+                r.status = 'cancelled'
+                r.t_done = now
+                if r in queue:
+                    queue.remove(r)
 
     def _admit(self, queue, now, batches, jobs):
-        held = 0
         n2d = sum(b.size() for b in batches.values())
-        for r in list(queue):
-            if r.footprint > self.budget:
-                raise ValueError(f'request {r.rid}: footprint {r.footprint / 1e9:.1f} GB exceeds the budget')
-            slot = n2d < self.slots2d if r.kind == '2d' else len(jobs) < self.slots3d
-            if not slot:
-                continue
-            if self.used + held + r.footprint > self.budget:
-                if held == 0:            # the oldest waiting request keeps its claim
-                    held = r.footprint
-                continue
+        admitted, rejected = admission(queue, self.used, self.budget, n2d, len(jobs), self.slots2d, self.slots3d)
+        for r in rejected:
+            queue.remove(r)
+            r.status, r.t_done = 'rejected', now
+            r.error = f'footprint {r.footprint / 1e9:.3f} GB exceeds the budget of {self.budget / 1e9:.3f} GB'
+        for r in admitted:
             queue.remove(r)
             self.used += r.footprint
             r.t_admit = now
@@ -285,11 +372,10 @@ class Server:
                 b = batches.get(key)
                 if b is None:
                     b = batches[key] = _Batch2D(self, key)
-                b.building.append((r, self.pool.submit(build_2d, sp)))
-                n2d += 1
+                b.building.append((r, self.pool.submit(self.build2d, sp)))
             else:
                 spec = r.spec if r.kind == '3d' else r.spec.spec(0)
-                jobs.append(_Job(self, r, self.pool.submit(build_3d, spec)))
+                jobs.append(_Job(self, r, self.pool.submit(self.build3d, spec)))
 
     def run(self, requests, realtime=True):
         """Serve `requests` (arrival times in seconds from the start); returns them
@@ -306,6 +392,7 @@ class Server:
             now = time.perf_counter() - self.t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
+            self._cancels(reqs, queue, now)
             if queue:
                 self._admit(queue, now, batches, jobs)
             did = False
@@ -313,7 +400,7 @@ class Server:
                 did |= b.pump(now)
             for j in list(jobs):
                 did |= j.pump(now)
-                if j.req.t_done is not None:
+                if j.ended() and (j.req.status != 'cancelled' or not j.busy()):
                     jobs.remove(j)
             if not did:
                 if not jobs and all(b.idle() for b in batches.values()) and pending and not queue:
@@ -325,15 +412,21 @@ class Server:
 
 
 def summary(reqs):
-    """p50 / p99 latency, makespan and aggregate cell-update rate of a served stream."""
-    lat = np.array([r.latency for r in reqs if r.latency is not None])
-    t_end = max(r.t_done for r in reqs)
-    t_begin = min(r.arrival for r in reqs)
-    cu = sum(r.cell_updates() for r in reqs)
+    """p50 / p99 latency, makespan and aggregate cell-update rate of the
+    completed requests of a served stream (with the count of each status)."""
+    done = [r for r in reqs if r.status == 'done']
+    lat = np.array([r.latency for r in done])
+    t_end = max(r.t_done for r in done)
+    t_begin = min(r.arrival for r in done)
+    cu = sum(r.cell_updates() for r in done)
     by = {}
-    for r in reqs:
+    for r in done:
         by.setdefault(r.kind, []).append(r.latency)
-    return dict(requests=len(reqs), p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
+    statuses = {}
+    for r in reqs:
+        statuses[r.status] = statuses.get(r.status, 0) + 1
+    return dict(requests=len(reqs), statuses=statuses, p50_s=float(np.percentile(lat, 50)),
+                p99_s=float(np.percentile(lat, 99)),
                 makespan_s=t_end - t_begin, cell_updates=cu, cell_updates_per_s=cu / max(t_end - t_begin, 1e-9),
                 by_kind={k: dict(n=len(v), p50_s=float(np.percentile(v, 50)), p99_s=float(np.percentile(v, 99)))
                          for k, v in by.items()})

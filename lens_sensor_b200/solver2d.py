@@ -17,6 +17,8 @@ import numpy as np
 import torch
 
 from . import engine as E
+from ._native import F32 as N_F32
+from . import _native as N
 from .geometry import Spec2D, build_2d
 
 
@@ -32,9 +34,16 @@ def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
 
 
 class Solve2D:
-    """Resident 2D solve of `steps_total` steps on the single-grid engine."""
+    """Resident 2D solve of `steps_total` steps.
 
-    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None):
+    engine='tb': the temporally blocked step (lens_tb2d_step, LENS_TB_K steps per
+    launch, one instance; the schedule and the snapshot period must be whole
+    numbers of launch pairs); engine='step': the single-grid engine
+    (lens_te2d_step / lens_tm2d_step), one step per launch pair.  chunk: rows
+    per warp of the temporally blocked step."""
+
+    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None, engine='tb',
+                 chunk=16):
         self.spec = sp = spec
         self.steps_total = int(steps_total)
         t0 = time.perf_counter()
@@ -44,16 +53,41 @@ class Solve2D:
         self.omega, self.steps_per_T, self.n_acc = sc['omega'], sc['steps_per_T'], sc['n_acc']
         self.dft, self.snap_steps = sc['dft'], sc['snaps']
         coef = {k: g[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if g.get(k) is not None}
-        self.grid = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, g['cx'], g['cy'], g['src'], device=device)
         self.h2d_bytes = sum(np.asarray(a).nbytes for a in coef.values()) + \
             sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
         self.table = E.StepTable(0, self.steps_total, sp.dt, g['src']['omega'], self.omega,
                                  E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
-        self.epi = E.Epi2D(self.grid, dft=self.dft)
-        self.comp = 'ez' if self.grid.pol == 's' else 'ey'
-        v = self.grid.view(self.comp)
+        self.engine = engine
+        if engine == 'tb':
+            from . import batch2d as B
+            span = 2 * N.TB_K
+            if self.steps_total % span or any(m % span for m in self.snap_steps):
+                raise ValueError(f"engine='tb' runs spans of {span} steps: use engine='step' for this schedule")
+            dev = E._device(device)
+            self.inst = B.Instance(sp, self.steps_total, torch.float32, dev, g, tb=True, kahan=True, window=self.dft)
+            self.group_tb = B.Group([self.inst], N_F32, 8, dev, tb=True, chunk=chunk)
+            self.grid = self.epi = None
+            fld = self.inst.f[0] if sp.pol == 's' else self.inst.f[1]
+            shape = (sp.nx, sp.ny) if sp.pol == 's' else (sp.nx, sp.ny - 1)
+            self._view = lambda: fld[:shape[0], :shape[1]]
+        else:
+            self.grid = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, g['cx'], g['cy'], g['src'], device=device)
+            self.epi = E.Epi2D(self.grid, dft=self.dft)
+            comp = 'ez' if self.grid.pol == 's' else 'ey'
+            self._view = lambda: self.grid.view(comp)
+        v = self._view()
         self.snaps = torch.zeros((len(self.snap_steps),) + tuple(v.shape), dtype=torch.float32, device=v.device)
         self.n = 0
+        self.launches = 0
+
+    def _advance(self, n, m, stream):
+        """Steps [n, m)."""
+        if self.engine != 'tb':
+            self.grid.step(self.table, n, m - n, self.epi, stream)
+            self.launches += 2 * (m - n)
+            return
+        self.group_tb.step(self.table, n, m - n, stream)
+        self.launches += (m - n) // N.TB_K
 
     def run(self, stream=None):
         """Advance to the end of the schedule, copying the snapshots on the way."""
@@ -61,15 +95,17 @@ class Solve2D:
         with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
             for q, m in enumerate(self.snap_steps + [self.steps_total]):
                 if m > n:
-                    self.grid.step(self.table, n, m - n, self.epi, stream)
+                    self._advance(n, m, stream)
                     n = m
                 if q < len(self.snap_steps):
-                    self.snaps[q].copy_(self.grid.view(self.comp))
+                    self.snaps[q].copy_(self._view())
         self.n = n
         return self
 
     def phasor(self):
         """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 on the device."""
+        if self.engine == 'tb':
+            return self.inst.phasor()
         return (2.0 / self.n_acc) * self.epi.phasor()
 
     def host_results(self):

@@ -44,12 +44,13 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
-def c0_errors():
-    """Config 0 (planar2d_te, 1600 x 480, 6000 steps) on the single-grid engine."""
+def c0_errors(engine='tb'):
+    """Config 0 (planar2d_te, 1600 x 480, 6000 steps) on the temporally blocked
+    step ('tb') or the single-grid engine ('step')."""
     from lens_sensor_b200.solver2d import Solve2D
     from lens_sensor_b200.workloads import planar2d_te
     sp, steps = planar2d_te()
-    s = Solve2D(sp, steps).run()
+    s = Solve2D(sp, steps, engine=engine).run()
     ph, snaps = s.host_results()
     fx = np.load(os.path.join(FP, 'c0.npz'))
     m = sample_mask(snaps[-1].size, 3)
@@ -111,14 +112,15 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
     out = {}
     geos = None
     for st in storages:
-        sw = B.Sweep(sel, steps, st, geos=geos)
-        geos = [q.geo for q in sw.insts]
-        sw.run()
-        for q, r in zip(SWEEP_Q, sw.results()):
-            ph = r['phasor'].cpu().numpy()
-            out[f'sw{q}_batched_{st}'] = rel(ph.ravel()[sample_mask(ph.size, 3)], ref[q])
-        del sw
-        torch.cuda.empty_cache()
+        for tb in (False, True):
+            sw = B.Sweep(sel, steps, st, geos=geos, tb=tb)
+            geos = [q.geo for q in sw.insts]
+            sw.run()
+            for q, r in zip(SWEEP_Q, sw.results()):
+                ph = r['phasor'].cpu().numpy()
+                out[f'sw{q}_{"tb" if tb else "batched"}_{st}'] = rel(ph.ravel()[sample_mask(ph.size, 3)], ref[q])
+            del sw
+            torch.cuda.empty_cache()
     for q, sp, geo in zip(SWEEP_Q, sel, geos):
         coef = {k: geo[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if geo.get(k) is not None}
         g = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, geo['cx'], geo['cy'], geo['src'])
@@ -133,9 +135,10 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
 
 
 @pytest.mark.gpu
-def test_config0_planar2d_te_against_fp64():
-    e = c0_errors()
-    print('c0 errors vs FP64:', e, 'reference fp32:', meta()['c0']['ref_fp32_err'])
+@pytest.mark.parametrize('engine', ['tb', 'step'])
+def test_config0_planar2d_te_against_fp64(engine):
+    e = c0_errors(engine)
+    print(f'c0 ({engine}) errors vs FP64:', e, 'reference fp32:', meta()['c0']['ref_fp32_err'])
     assert e['phasor'] <= TOL, e
     assert e['snap_last_sample'] <= TOL, e
     assert e['snap_norms'] <= TOL_SCALAR, e
@@ -164,5 +167,6 @@ def test_sweep_instances_against_fp64():
     from make_fp64 import SWEEP_Q
     for q in SWEEP_Q:
         assert e[f'sw{q}_batched_f32'] <= TOL, (q, e)
+        assert e[f'sw{q}_tb_f32'] <= TOL, (q, e)
         assert e[f'sw{q}_single'] <= TOL, (q, e)
         assert e[f'sw{q}_batched_f16'] < 1e-2 and e[f'sw{q}_batched_bf16'] < 5e-2, (q, e)

@@ -116,3 +116,63 @@ def test_batch_members_match_the_plain_batch():
         torch.cuda.synchronize()
         ph = sw.insts[0].phasor().cpu()
         assert torch.equal(ph, r.result['phasor'])
+
+
+def _req(rid, kind, fp, arrival=0.0):
+    from types import SimpleNamespace
+    return SimpleNamespace(rid=rid, kind=kind, footprint=fp, arrival=arrival)
+
+
+def test_admission_first_fit_with_held_claim_and_slots():
+    """CPU: first fit in arrival order; the oldest request that does not fit keeps
+    its claim (a later small one only fits beside it); slot limits per kind;
+    a request larger than the whole budget is rejected, not queued forever."""
+    from lens_sensor_b200.serve import admission
+    q = [_req(0, '2d', 40), _req(1, '3d', 70), _req(2, '2d', 30), _req(3, '2d', 10), _req(4, '3d', 500)]
+    adm, rej = admission(q, used=0, budget=100, n2d=0, n3d=0, slots2d=8, slots3d=4)
+    # 0 fits (40); 1 does not (40 + 70 > 100) and holds its 70; beside that claim
+    # neither 2 (40 + 70 + 30) nor 3 (40 + 70 + 10) fits; 4 can never fit
+    assert [r.rid for r in adm] == [0] and [r.rid for r in rej] == [4]
+    adm, rej = admission(q[1:4], used=0, budget=100, n2d=0, n3d=0, slots2d=8, slots3d=4)
+    assert [r.rid for r in adm] == [1, 2]          # 70 + 30 = 100 fits exactly
+    adm, _ = admission(q[:4], used=0, budget=1000, n2d=0, n3d=0, slots2d=1, slots3d=4)
+    assert [r.rid for r in adm] == [0, 1]          # one 2D slot: 2 and 3 wait for it
+    adm, _ = admission(q[:4], used=0, budget=1000, n2d=0, n3d=4, slots2d=8, slots3d=4)
+    assert [r.rid for r in adm] == [0, 2, 3]       # no 3D slot free
+
+
+@pytest.mark.gpu
+def test_rejected_cancelled_and_failed_requests_leave_the_rest_intact():
+    """A request too large for the budget is rejected, one is cancelled while it
+    runs, one fails in its host-side setup; every other request completes with
+    the result it has when served alone, and the memory account returns to 0."""
+    from lens_sensor_b200 import geometry as G
+    from lens_sensor_b200.serve import Request, Server, footprint, summary
+    items = [x for x in _mix() if x[0] != 'stitch']
+    reqs = [Request(i, k, sp, n, t) for i, (k, sp, n, t) in enumerate(items)]
+    budget = 2.2 * max(footprint(r) for r in reqs)
+    st = Stack(1.49, 1.0, [(1.0, 1.333)], 1.376)
+    huge = Request(100, '3d', Spec3D('p', 2048, 512, 1024, 30.0, st, 2.0), 100, 0.001)
+    reqs.append(huge)
+    reqs[1].cancel_at = 0.05                       # a 2D member, cancelled mid-run
+    bad = reqs[2]
+    srv = Server(budget=budget, slots2d=3, slots3d=2, quantum2d=32, quantum3d=32)
+
+    def build2d(sp):
+        if sp is bad.spec:
+            raise RuntimeError('host setup failed')
+        return G.build_2d(sp)
+    srv.build2d = build2d
+    out = srv.run(reqs)
+    byid = {r.rid: r for r in out}
+    assert byid[100].status == 'rejected' and 'exceeds the budget' in byid[100].error
+    assert byid[2].status == 'failed' and 'host setup failed' in byid[2].error
+    assert byid[1].status in ('cancelled', 'done')   # it may finish before the cancel lands
+    assert srv.used == 0
+    s = summary(out)
+    assert s['statuses']['rejected'] == 1 and s['statuses']['failed'] == 1
+    for r in out:
+        if r.rid in (1, 2, 100) or r.status != 'done':
+            continue
+        alone = _serve([items[r.rid][:3] + (0.0,)])[0]
+        assert torch.equal(r.result['phasor'], alone.result['phasor']), r.rid

@@ -363,6 +363,27 @@ int lens_fdtd3d_step(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *e
 int lens_fdtd3d_step_driven(LensGrid3D *g, const LensStepTable *tab, const LensEpi3D *ep,
                             const LensDrive3D *drive, int n0, int nsteps, void *stream);
 
+/* Temporally blocked 3D step: LENS_TB3_K = 2 time steps per launch, each field
+ * value crossing HBM once per two steps, with the step's epilogues fused
+ * (detector boxes, volume DFTs, convergence and flux planes of LensEpi3D).  A
+ * CTA streams a tile of 12 rows (y) x 28 lanes (z) down an x-chunk of `chunk`
+ * planes, advancing two time levels one plane apart; the two cells around the
+ * tile and the two planes around the chunk are recomputed halo.  Needs both
+ * field and psi buffers (each launch reads buffer cur, writes 1 - cur and flips
+ * cur) and psi_lv: a scratch set of the twelve psi volumes ((nx, ny, pitch)
+ * each, touched only in the strips) holding the intermediate level.  nsteps
+ * must be even; no stitch drive.  Replaces the per-step loop of
+ * fdtd3d_core.py:1106-1158 (the reference advances one step per call).      */
+#define LENS_TB3_K 2
+
+typedef struct {
+    float *psi_lv[LENS_NPSI];    /* intermediate-level psi volumes             */
+    int chunk;                   /* x-planes per CTA (>= 1)                    */
+} LensTB3D;
+
+int lens_fdtd3d_step_tb(LensGrid3D *g, const LensTB3D *tb, const LensStepTable *tab, const LensEpi3D *ep,
+                        int n0, int nsteps, void *stream);
+
 /* Self-test of the fused step's failure detection (no counterpart in the
  * reference, whose NumPy loop has no device waits): one fused step in which the
  * first CTA of the launch withholds the E copy of one x-plane of its chunk (the
@@ -387,8 +408,8 @@ const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
  * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D,
- * LensDrive3D, LensDrive2D, LensTB2D.  Writes min(n, 13) entries and returns 13
- * (bindings check their mirrors). */
+ * LensDrive3D, LensDrive2D, LensTB2D, LensTB3D.  Writes min(n, 14) entries and
+ * returns 14 (bindings check their mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

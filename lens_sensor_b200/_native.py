@@ -105,6 +105,13 @@ class TB2D(ctypes.Structure):
 TB_K = 4
 
 
+class TB3D(ctypes.Structure):
+    _fields_ = [('psi_lv', c_void_p * 12), ('chunk', c_int)]
+
+
+TB3_K = 2
+
+
 class Drive3D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p * 3)]
 
@@ -113,7 +120,7 @@ class Drive2D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p), ('tab', c_void_p)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D, TB2D)
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D, TB2D, TB3D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
@@ -128,6 +135,8 @@ SIGNATURES = {
     'lens_fdtd3d_step_driven': (c_int, [POINTER(Grid3D), POINTER(StepTable), POINTER(Epi3D), POINTER(Drive3D),
                                         c_int, c_int, c_void_p]),
     'lens_fdtd3d_accum_e2': (c_int, [POINTER(Grid3D), c_int, c_int, c_void_p, c_void_p]),
+    'lens_fdtd3d_step_tb': (c_int, [POINTER(Grid3D), POINTER(TB3D), POINTER(StepTable), POINTER(Epi3D), c_int, c_int,
+                                    c_void_p]),
     'lens_fdtd3d_watchdog_test': (c_int, [POINTER(Grid3D), POINTER(StepTable), c_int, c_int, c_void_p]),
     'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
     'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,

@@ -403,7 +403,7 @@ class Grid3D:
     FIELDS = ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')
 
     def __init__(self, nx, ny, nz, dx, dt, ce, da, cpml, src, src_comp=1, pec=(1,) * 6,
-                 device=None, fused=True):
+                 device=None, fused=True, tb=False, tb_chunk=40):
         self.lib = N.load()
         dev = self.dev = _device(device)
         self.nx, self.ny, self.nz, self.dx, self.dt = int(nx), int(ny), int(nz), dx, dt
@@ -455,6 +455,17 @@ class Grid3D:
             ct, tab, ex, nt = self.cols
             g.ctype, g.ctab, g.cexpl, g.ntype = ct.data_ptr(), tab.data_ptr(), ex.data_ptr(), nt
         self.s = g
+        # temporally blocked step: a scratch set of the psi volumes for its intermediate level
+        self.tb = None
+        if tb:
+            if not fused:
+                raise ValueError('the temporally blocked 3D step needs both field buffers (fused=True)')
+            self.psi_lv = {q: z() for q in N.PSI_NAMES}
+            t = N.TB3D()
+            for q, name in enumerate(N.PSI_NAMES):
+                t.psi_lv[q] = self.psi_lv[name].data_ptr()
+            t.chunk = int(tb_chunk)
+            self.tb = t
 
     def __getattr__(self, name):
         if name in Grid3D.FIELDS:
@@ -477,6 +488,25 @@ class Grid3D:
             N.check(self.lib.lens_fdtd3d_step_driven(ctypes.byref(self.s), ctypes.byref(table.s), e,
                                                      ctypes.byref(drive.s), int(n0), int(nsteps),
                                                      _stream_ptr(stream)))
+
+    def step_tb(self, table, n0, nsteps, epi=None, stream=None):
+        """Steps [n0, n0 + nsteps) on the temporally blocked kernel (LENS_TB3_K steps
+        per launch, epilogues fused); an odd leftover step runs on the fused
+        single-step kernel.  Returns the number of kernel launches."""
+        if self.tb is None:
+            raise ValueError('grid built without tb=True')
+        e = ctypes.byref(epi.s) if epi is not None else None
+        k = N.TB3_K
+        m = nsteps // k * k
+        launches = 0
+        if m:
+            N.check(self.lib.lens_fdtd3d_step_tb(ctypes.byref(self.s), ctypes.byref(self.tb), ctypes.byref(table.s), e,
+                                                 int(n0), int(m), _stream_ptr(stream)))
+            launches += m // k
+        if nsteps - m:
+            self.step(table, n0 + m, nsteps - m, epi, stream)
+            launches += (nsteps - m) * (2 if epi is not None else 1)
+        return launches
 
     def check_flag(self):
         """Raise if a pipeline wait in the fused kernel gave up or a detector box

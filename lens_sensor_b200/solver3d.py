@@ -70,9 +70,15 @@ def schedule_3d(sp: Spec3D, steps_total, x_facet_um):
 
 class Solve3D:
     """Resident 3D solve.  comps: components whose phasor is accumulated
-    (0 Ex, 1 Ey, 2 Ez; default the driven one)."""
+    (0 Ex, 1 Ey, 2 Ez; default the driven one).  engine: 'fused' (one step per
+    launch, lens_fdtd3d_step), 'tb' (two steps per launch with the epilogues
+    fused, lens_fdtd3d_step_tb) or 'twopass' (in place, two passes per step)."""
 
-    def __init__(self, spec: Spec3D, steps_total, comps=None, fused=True, device=None, geo=None):
+    def __init__(self, spec: Spec3D, steps_total, comps=None, fused=True, device=None, geo=None, engine=None,
+                 tb_chunk=40):
+        engine = engine or ('fused' if fused else 'twopass')
+        fused = engine != 'twopass'
+        self.engine = engine
         self.spec = sp = spec
         self.steps_total = int(steps_total)
         t0 = time.perf_counter()
@@ -82,7 +88,8 @@ class Solve3D:
         Nx, Ny, Nz = sp.nx, sp.ny, sp.nz
         dx_um = sp.dx_nm / 1000.0
         self.grid = E.Grid3D(Nx, Ny, Nz, sp.dx, sp.dt, g['ce'], g['da'], g['cpml'], g['src'],
-                             src_comp=sp.src_comp, fused=fused, device=device)
+                             src_comp=sp.src_comp, fused=fused, device=device, tb=engine == 'tb',
+                             tb_chunk=tb_chunk)
         self.h2d_bytes = sum(a.nbytes for a in g['ce']) + (0 if g['da'] is None else sum(a.nbytes for a in g['da'])) \
             + sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
         sc = schedule_3d(sp, self.steps_total, g['x_facet_um'])
@@ -115,8 +122,11 @@ class Solve3D:
         for m in self.iavg_steps(n, n1) + [None]:
             stop = n1 if m is None else m + 1
             if stop > n:
-                self.grid.step(self.table, n, stop - n, self.epi, stream)
-                self.launches += self._launches(n, stop, fused)
+                if self.engine == 'tb':
+                    self.launches += self.grid.step_tb(self.table, n, stop - n, self.epi, stream)
+                else:
+                    self.grid.step(self.table, n, stop - n, self.epi, stream)
+                    self.launches += self._launches(n, stop, fused)
                 n = stop
             if m is not None:
                 self.grid.accum_e2(self.epi.iavg, stream=stream)

@@ -158,7 +158,7 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(spec, steps_total, cells, ws, pg):
+def run_e2e(spec, steps_total, cells, ws, pg, engine='fused'):
     """The whole solve through the public API from host inputs: host setup,
     upload, the 4000-step schedule, read-back of the three phasors."""
     import torch
@@ -167,7 +167,7 @@ def run_e2e(spec, steps_total, cells, ws, pg):
         pg.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s2 = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    s2 = Solve3D(spec, steps_total, comps=(0, 1, 2), engine=engine)
     torch.cuda.synchronize()          # the uploads are synchronous already; marks the phase end
     t1 = time.perf_counter()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -261,45 +261,60 @@ def cpu_baseline_2d(spec, steps=200):
 
 def run_planar2d(cpu=True):
     """Config 0 (planar2d_te: 2D TE 1600 x 480 @ 25 nm, 6000 steps, one-period CW
-    phasor, Ez snapshots every 200 steps) on the single-grid engine.  value: the
-    whole 6000-step solve on the device (CUDA events, inputs resident); e2e: the
-    same solve from the host spec (setup, upload, run, read-back of the phasor and
-    the 30 snapshots)."""
+    phasor, Ez snapshots every 200 steps).  Each 2D engine runs the whole
+    6000-step solve on the device (CUDA events, inputs resident; the batched and
+    temporally blocked engines replay the schedule as one CUDA graph); value is
+    the fastest engine's.  e2e: that engine's solve from the host spec (setup,
+    upload, graph capture, run, read-back of the phasor and the 30 snapshots)."""
     import torch
     from lens_sensor_b200.solver2d import Solve2D
     from lens_sensor_b200.workloads import planar2d_te
     sp, steps = planar2d_te()
     cells = sp.nx * sp.ny
-    warm = Solve2D(sp, steps)
-    warm.run()
-    geo = warm.geo
-    del warm
-    s = Solve2D(sp, steps, geo=geo)
-    torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    ev[0].record()
-    s.run()
-    ev[1].record()
-    torch.cuda.synchronize()
-    t_dev = ev[0].elapsed_time(ev[1]) * 1e-3
-    del s
+    geo = None
+    rates = {}
+    for eng in ('batch', 'tb', 'step'):
+        warm = Solve2D(sp, steps, engine=eng, geo=geo)
+        geo = warm.geo
+        if eng != 'step':
+            warm.capture()
+        warm.run()
+        del warm
+        s = Solve2D(sp, steps, engine=eng, geo=geo)
+        if eng != 'step':
+            s.capture()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        s.run()
+        ev[1].record()
+        torch.cuda.synchronize()
+        rates[eng] = (ev[0].elapsed_time(ev[1]) * 1e-3, s.launches)
+        del s
+    best = min(rates, key=lambda e: rates[e][0])
+    t_dev, launches = rates[best]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s = Solve2D(sp, steps)
+    s = Solve2D(sp, steps, engine=best)
+    if best != 'step':
+        s.capture()
     s.run()
     ph, snaps = s.host_results()
     t_e2e = time.perf_counter() - t0
     peak, peak_src = peaks()
     achieved = 32.0 * cells / (t_dev / steps) / 1e9
+    kern = {'batch': 'b2d_h + b2d_e (batched passes on one instance)',
+            'tb': 'tb2d (four steps per launch)', 'step': 'te2d_h + te2d_e (single-grid passes)'}[best]
     out = dict(workload=f'planar2d_te: 2D TE planar waveguide {sp.nx}x{sp.ny} @ 25 nm, fp32, 12-cell CPML, '
                         f'{steps} steps, CW ramped over 20 periods, one seeded PS bead, one-period phasor, '
                         'Ez snapshots every 200 steps',
                unit=UNIT, value=cells * steps / t_dev, ms_per_step=t_dev / steps * 1e3, steps=steps, cells=cells,
+               engine=best, engines={e: cells * steps / t for e, (t, _) in rates.items()}, gpu_launches=launches,
                l2=f'working set {(5 * cells * 4) / 1e6:.0f} MB of fields and coefficients fits in the 126 MB L2: '
                   'the steps of one solve run L2-resident, as in use; no flush between steps',
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
-                             peak_source=peak_src, kernel='2D TE step (te2d_h + te2d_e)',
-                             alg_bytes_per_step=32 * cells, step_ms=t_dev / steps * 1e3),
+                             peak_source=peak_src, kernel=kern, alg_bytes_per_step=32 * cells,
+                             step_ms=t_dev / steps * 1e3),
                e2e=dict(value=cells * steps / t_e2e, unit=UNIT, solve_seconds=t_e2e,
                         h2d_bytes_per_step=s.h2d_bytes / steps, d2h_bytes_per_step=s.d2h_bytes / steps,
                         host_setup_seconds=s.t_setup_host))
@@ -488,11 +503,15 @@ def ours_arm(args):
     from lens_sensor_b200.workloads import waveguide3d_tm
     spec, steps_total = waveguide3d_tm()
     cells = spec.nx * spec.ny * spec.nz
-    solve = Solve3D(spec, steps_total, comps=(0, 1, 2))
+    eng = args.engine3d
+    solve = Solve3D(spec, steps_total, comps=(0, 1, 2), engine=eng)
     W = max(3, args.warmup)
+    W += W % 2                        # spans of whole launch pairs for the two-step kernel
     ka, kb = split_steps(args.steps, steps_total, solve.n_acc)
     ka = min(ka, solve.dft[0] - W)
     kb = min(kb, solve.n_acc)
+    ka -= ka % 2
+    kb -= kb % 2
     K = ka + kb
     uuid = None
     try:
@@ -533,11 +552,13 @@ def ours_arm(args):
     assert not solve.iavg_steps(W, W + ka) and W + ka <= solve.prev[0]
     peak, peak_src = peaks()
     # roofline of the dominant kernel (the fused step, one launch per segment-A step)
-    t_launch = ms_a * 1e-3 / max(ka, 1)
-    achieved = 72.0 * cells / t_launch / 1e9
+    steps_per_launch = 2 if eng == 'tb' else 1
+    t_launch = ms_a * 1e-3 / max(ka // steps_per_launch, 1)
+    achieved = 72.0 * cells * steps_per_launch / t_launch / 1e9
     traffic = None
     try:
-        with open(os.path.join(ROOT, 'profiles', 'yee3d_waveguide3d_tm_traffic.json')) as f:
+        name = 'tb3d' if eng == 'tb' else 'yee3d'
+        with open(os.path.join(ROOT, 'profiles', f'{name}_waveguide3d_tm_traffic.json')) as f:
             traffic = json.load(f).get('bytes_per_launch')
     except Exception:
         pass
@@ -546,7 +567,7 @@ def ours_arm(args):
     torch.cuda.empty_cache()
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(spec, steps_total, cells, ws, pg)
+        e2e = run_e2e(spec, steps_total, cells, ws, pg, engine=eng)
     planar = run_planar2d(cpu=(rank == 0 and not args.no_cpu)) if (ws == 1 and not args.no_planar) else None
     batched = run_batched(count=args.batch_instances) if (ws == 1 and not args.no_batch) else None
     stitch = run_stitch(args.stitch_windows) if (ws == 1 and not args.no_stitch) else None
@@ -565,7 +586,10 @@ def ours_arm(args):
                                 parallelism=f'replicas{ws}' if ws > 1 else 'single'),
                     roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s',
                                   frac=achieved / peak, traffic=traffic, peak_source=peak_src,
-                                  kernel='yee3d (fused step)', alg_bytes_per_launch=72 * cells,
+                                  kernel=('tb3d (two steps per launch, epilogues fused)' if eng == 'tb'
+                                          else 'yee3d (fused step)'),
+                                  steps_per_launch=steps_per_launch,
+                                  alg_bytes_per_launch=72 * cells * steps_per_launch,
                                   launch_ms=t_launch * 1e3,
                                   mix_alg_bytes_per_cell_update=alg / (cells * K),
                                   mix_achieved=alg / (ms * 1e-3) / 1e9),
@@ -584,6 +608,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=20)
     ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--engine3d', default='fused', choices=('fused', 'tb'),
+                    help='3D step: fused single step per launch, or two steps per launch (tb)')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end solve (profiling runs)')
     ap.add_argument('--no-batch', action='store_true', help='skip the batched 2D sweep (sweep2d)')
     ap.add_argument('--no-planar', action='store_true', help='skip the 2D single-grid solve (planar2d_te)')

@@ -36,14 +36,17 @@ def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
 class Solve2D:
     """Resident 2D solve of `steps_total` steps.
 
-    engine='tb': the temporally blocked step (lens_tb2d_step, LENS_TB_K steps per
-    launch, one instance; the schedule and the snapshot period must be whole
-    numbers of launch pairs); engine='step': the single-grid engine
-    (lens_te2d_step / lens_tm2d_step), one step per launch pair.  chunk: rows
-    per warp of the temporally blocked step."""
+    engine='batch' (default): the batched kernels on this one instance
+    (lens_batch2d_step, vector passes over 128 x 2*by tiles; capture() records
+    the whole schedule, snapshots included, as one CUDA graph that run()
+    replays); engine='tb': the temporally blocked step (lens_tb2d_step,
+    LENS_TB_K steps per launch; the schedule and the snapshot period must be
+    whole numbers of launch pairs; chunk: rows per warp); engine='step': the
+    single-grid engine (lens_te2d_step / lens_tm2d_step), one step per launch
+    pair, with the full single-grid epilogue set."""
 
-    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None, engine='tb',
-                 chunk=16):
+    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None, engine='batch',
+                 chunk=16, by=4):
         self.spec = sp = spec
         self.steps_total = int(steps_total)
         t0 = time.perf_counter()
@@ -58,14 +61,16 @@ class Solve2D:
         self.table = E.StepTable(0, self.steps_total, sp.dt, g['src']['omega'], self.omega,
                                  E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
         self.engine = engine
-        if engine == 'tb':
+        self.graph = None
+        if engine in ('tb', 'batch'):
             from . import batch2d as B
+            tb = engine == 'tb'
             span = 2 * N.TB_K
-            if self.steps_total % span or any(m % span for m in self.snap_steps):
-                raise ValueError(f"engine='tb' runs spans of {span} steps: use engine='step' for this schedule")
+            if tb and (self.steps_total % span or any(m % span for m in self.snap_steps)):
+                raise ValueError(f"engine='tb' runs spans of {span} steps: use engine='batch' for this schedule")
             dev = E._device(device)
-            self.inst = B.Instance(sp, self.steps_total, torch.float32, dev, g, tb=True, kahan=True, window=self.dft)
-            self.group_tb = B.Group([self.inst], N_F32, 8, dev, tb=True, chunk=chunk)
+            self.inst = B.Instance(sp, self.steps_total, torch.float32, dev, g, tb=tb, kahan=tb, window=self.dft)
+            self.group = B.Group([self.inst], N_F32, by, dev, tb=tb, chunk=chunk)
             self.grid = self.epi = None
             fld = self.inst.f[0] if sp.pol == 's' else self.inst.f[1]
             shape = (sp.nx, sp.ny) if sp.pol == 's' else (sp.nx, sp.ny - 1)
@@ -82,15 +87,43 @@ class Solve2D:
 
     def _advance(self, n, m, stream):
         """Steps [n, m)."""
-        if self.engine != 'tb':
+        if self.engine == 'step':
             self.grid.step(self.table, n, m - n, self.epi, stream)
             self.launches += 2 * (m - n)
             return
-        self.group_tb.step(self.table, n, m - n, stream)
-        self.launches += (m - n) // N.TB_K
+        self.group.step(self.table, n, m - n, stream)
+        self.launches += self.group.launches(n, m)
+
+    def capture(self):
+        """Record the rest of the schedule (steps and snapshot copies) as one CUDA
+        graph; the next run() replays it (batched and temporally blocked engines)."""
+        if self.engine == 'step':
+            raise ValueError("engine='step' launches step by step")
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.snaps.device)
+        s.wait_stream(torch.cuda.current_stream())
+        n0, l0 = self.n, self.launches
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self._schedule(None)
+        torch.cuda.current_stream().wait_stream(s)
+        self.n, self._graph_launches, self.launches = n0, self.launches - l0, l0
+        self.graph = g
+        return self
 
     def run(self, stream=None):
-        """Advance to the end of the schedule, copying the snapshots on the way."""
+        """Advance to the end of the schedule, copying the snapshots on the way
+        (replaying the captured graph when there is one)."""
+        if self.graph is not None:
+            with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+                self.graph.replay()
+            self.graph = None
+            self.n = self.steps_total
+            self.launches += self._graph_launches
+            return self
+        return self._schedule(stream)
+
+    def _schedule(self, stream):
         n = self.n
         with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
             for q, m in enumerate(self.snap_steps + [self.steps_total]):
@@ -104,7 +137,7 @@ class Solve2D:
 
     def phasor(self):
         """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 on the device."""
-        if self.engine == 'tb':
+        if self.engine != 'step':
             return self.inst.phasor()
         return (2.0 / self.n_acc) * self.epi.phasor()
 

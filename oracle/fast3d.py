@@ -24,7 +24,7 @@ def build(force=False):
     """Compile oracle/o3.cpp (oracle/Makefile) if the library is missing or older."""
     src = os.path.join(HERE, 'o3.cpp')
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
-        subprocess.run(['make', '-s', '-C', HERE], check=True)
+        subprocess.run(['make', '-s'] + (['-B'] if force else []) + ['-C', HERE], check=True)
     return LIB
 
 

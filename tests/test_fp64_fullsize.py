@@ -44,13 +44,17 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
-def c0_errors(engine='tb'):
-    """Config 0 (planar2d_te, 1600 x 480, 6000 steps) on the temporally blocked
-    step ('tb') or the single-grid engine ('step')."""
+def c0_errors(engine='batch'):
+    """Config 0 (planar2d_te, 1600 x 480, 6000 steps) on the batched kernels
+    ('batch', graph-replayed), the temporally blocked step ('tb') or the
+    single-grid engine ('step')."""
     from lens_sensor_b200.solver2d import Solve2D
     from lens_sensor_b200.workloads import planar2d_te
     sp, steps = planar2d_te()
-    s = Solve2D(sp, steps, engine=engine).run()
+    s = Solve2D(sp, steps, engine=engine)
+    if engine != 'step':
+        s.capture()
+    s.run()
     ph, snaps = s.host_results()
     fx = np.load(os.path.join(FP, 'c0.npz'))
     m = sample_mask(snaps[-1].size, 3)
@@ -135,7 +139,7 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('engine', ['tb', 'step'])
+@pytest.mark.parametrize('engine', ['batch', 'tb', 'step'])
 def test_config0_planar2d_te_against_fp64(engine):
     e = c0_errors(engine)
     print(f'c0 ({engine}) errors vs FP64:', e, 'reference fp32:', meta()['c0']['ref_fp32_err'])

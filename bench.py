@@ -424,47 +424,102 @@ def run_batched(plain_sample=16, count=256):
                 K_median=float(np.median(K)), err_vs_fp64=fp64, f16_gate=gate)
 
 
-def run_stitch(windows=3):
-    """The stitch3d_plan workload: a 3D stitch of `windows` windows of 480 x 192 x
-    256 cells (30 nm, 40-cell overlap; 19 windows = the whole 240 um guide) through
-    stitch3d.StitchSolve: per-window geometry built on a host thread while the
-    previous window runs, steady-state steps, on-device handoff of the overlap
-    amplitudes, assembly to host memory.  Rate = cell updates of every window
-    (absorber extension included) over the wall time from the first window's
-    setup to the last window's assembled slab."""
-    import concurrent.futures as cf
-    import torch
+def _stitch_member(pl, stream, pool):
+    """One stitch job (a member of a sweep) on its own stream; the assembled
+    slabs are written to host arrays."""
     from lens_sensor_b200 import engine as E
     from lens_sensor_b200.stitch3d import StitchSolve
-    from lens_sensor_b200.workloads import stitch3d_plan
-    windows = 19 if windows <= 0 else windows
-    pl = stitch3d_plan(nx_full=480 + (windows - 1) * 440)
     Ef = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.complex64)
     Ia = np.zeros((pl.Nx_full, pl.Nj, pl.Nk), np.float32)
 
     def sink(w, g_lo, g_hi, Ew, I):
         Ef[g_lo:g_hi] = Ew
         Ia[g_lo:g_hi] = I
-    pool = cf.ThreadPoolExecutor(1)
+    return StitchSolve(pl, E, sink, stream=stream, pool=pool)
+
+
+def stitch_vs_reference():
+    """The reference's own characterization stitch (3 windows, the last flush;
+    tests/golden/dropin_3d_stitch.json 'goldenstitch', from the reference's
+    run_3d_stitched) through this drop-in on the GPU: relative errors of its
+    result scalars and the |<E^2>| sum against the reference's values."""
+    import tempfile
+    from lens_sensor_b200 import fdtd3d_core as D3
+    case = json.load(open(os.path.join(ROOT, 'tests', 'golden', 'dropin_3d_stitch.json')))['goldenstitch']
+    cwd, kappa = os.getcwd(), D3.KAPPA
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            D3.KAPPA = dict(case['kappa'])
+            r = D3.run_3d_stitched(**dict(case['kw']))
+        finally:
+            os.chdir(cwd)
+            D3.KAPPA = kappa
+    out = {k: abs(r[k] - case['result'][k]) / max(abs(case['result'][k]), 1e-300)
+           for k in ('transmission', 'P_in', 'P_out')}
+    out['case'] = 'reference characterization stitch: 3 windows, the last flush with the domain end'
+    return out
+
+
+def run_stitch(windows=3, members=2):
+    """The stitch3d_plan workload: a 3D stitch of `windows` windows of 480 x 192 x
+    256 cells (30 nm, 40-cell overlap; 19 windows = the whole 240 um guide) through
+    stitch3d.StitchSolve: per-window geometry built on a host thread while the
+    previous window runs, steady-state steps, on-device handoff of the overlap
+    amplitudes, assembly to host memory.  Rate = cell updates of every window
+    (absorber extension included) over the wall time from the first window's
+    setup to the last window's assembled slab.  Then `members` independent
+    members of a sweep (other seeds) run at once, each on its own CUDA stream,
+    advanced in turn in quanta of steps, so one member's window setup, handoff
+    and assembly overlap the others' steps."""
+    import concurrent.futures as cf
+    import torch
+    from lens_sensor_b200.workloads import stitch3d_plan
+    windows = 19 if windows <= 0 else windows
+    nx_full = 480 + (windows - 1) * 440
+    pl = stitch3d_plan(nx_full=nx_full)
+    pool = cf.ThreadPoolExecutor(2)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    job = StitchSolve(pl, E, sink, pool=pool)
+    job = _stitch_member(pl, None, pool)
     while not job.done:
         job.advance(pl.steps_win)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    pool.shutdown()
     cu = pl.cell_updates()
     T = job.transmission()
     del job
     torch.cuda.empty_cache()
+    conc = None
+    if members > 1:
+        plans = [stitch3d_plan(seed=3 + 2 * q, nx_full=nx_full) for q in range(members)]
+        streams = [torch.cuda.Stream() for _ in plans]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        jobs = [_stitch_member(p, s, pool) for p, s in zip(plans, streams)]
+        while not all(j.done for j in jobs):
+            for j in jobs:
+                j.advance(256)
+        torch.cuda.synchronize()
+        wc = time.perf_counter() - t0
+        cuc = sum(p.cell_updates() for p in plans)
+        conc = dict(members=members, value=cuc / wc, wall_s=wc, cell_updates=cuc,
+                    vs_one_member=(cuc / wc) / (cu / wall))
+        del jobs
+        torch.cuda.empty_cache()
+    pool.shutdown()
     return dict(workload=f'stitch3d_plan: 3D stitch, {pl.n_win} windows of {pl.Nx_win} x {pl.Ny} x {pl.Nz} @ 30 nm '
                          f'(+{pl.EXT}-cell absorber on interior windows), {pl.O}-cell overlap, '
                          f'{pl.steps_win} steps per window; {pl.Nx_full} cells = {pl.lx_um:.1f} um',
                 unit=UNIT, value=cu / wall, wall_s=wall, cell_updates=cu, windows=pl.n_win,
                 steps_per_window=pl.steps_win, transmission=T,
                 handoff='on device (3 complex components x overlap planes)',
-                full_plan_windows=19)
+                full_plan_windows=19,
+                full_plan_seconds_extrapolated=wall / pl.n_win * 19,
+                extrapolation='every window of the 19-window plan has the same size and step count as the '
+                              'measured ones (the last is flush with the domain end), so the whole plan takes '
+                              '19 / windows of the measured wall time at the measured rate',
+                concurrent_members=conc, err_vs_reference=stitch_vs_reference())
 
 
 def run_serving(count=32, seed=4):

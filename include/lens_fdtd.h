@@ -217,6 +217,21 @@ int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *inst_dev, c
                       const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab,
                       int n0, int nsteps, void *stream);
 
+/* The same steps as lens_batch2d_step in ONE persistent cooperative launch:
+ * every resident block strides over the batch's tiles, phase by phase (H, E,
+ * and the TM node DFT on its window steps), and the blocks meet at a grid
+ * barrier between phases, so a batch whose state fits in L2 keeps it there
+ * across steps and no launch gap separates the steps.  sync: 2 device words of
+ * barrier state and err: a device int, both the caller's (zeroed by the call
+ * on `stream` before the launch).  Every barrier wait is bounded (about a
+ * second); if one runs out *err becomes nonzero, the launch ends and the
+ * results are invalid.  The device must support cooperative launches.  No
+ * counterpart entry in the reference (its loop advances one step per call,
+ * fdtd2d_core.py:781-847).                                                   */
+int lens_batch2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
+                     const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab, int n0,
+                     int nsteps, unsigned *sync, int *err, void *stream);
+
 /* Same step as lens_batch2d_step for callers that cannot allocate device
  * memory (an application that owns the GPU allocator, a fixed memory budget, a
  * loop where cudaMalloc's implicit synchronisation is not allowed).  No

@@ -141,6 +141,8 @@ SIGNATURES = {
     'lens_batch2d_plan': (c_int, [POINTER(Inst2D), c_int, c_int, POINTER(c_int), POINTER(c_int)]),
     'lens_batch2d_step': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                   POINTER(StepTable), c_int, c_int, c_void_p]),
+    'lens_batch2d_run': (c_int, [POINTER(Inst2D), c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                 POINTER(StepTable), c_int, c_int, c_void_p, c_void_p, c_void_p]),
     'lens_batch2d_step_noalloc': (c_int, [POINTER(Inst2D), c_int, c_int, c_int, POINTER(StepTable), c_int,
                                           c_int, c_void_p]),
     'lens_tb2d_plan': (c_int, [POINTER(TB2D), c_int, c_int, POINTER(c_int)]),

@@ -238,6 +238,26 @@ class Group:
                                            self.storage, int(self.by), ctypes.byref(tab.s), int(n0), int(nsteps),
                                            E._stream_ptr(stream)))
 
+    def step_persistent(self, tab, n0, nsteps, stream=None):
+        """Steps [n0, n0 + nsteps) in one persistent cooperative launch
+        (lens_batch2d_run); raises if a grid-barrier wait ran out."""
+        if self.tb:
+            raise ValueError('the persistent launch runs the single-step kernels')
+        if not hasattr(self, 'sync'):
+            self.sync = torch.zeros(2, dtype=torch.int32, device=self.dev)
+            self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        N.check(self.lib.lens_batch2d_run(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()),
+                                          ctypes.c_void_p(self.dev_blk.data_ptr()),
+                                          ctypes.c_void_p(self.dev_owner.data_ptr()), len(self.insts),
+                                          self.storage, int(self.by), ctypes.byref(tab.s), int(n0), int(nsteps),
+                                          ctypes.c_void_p(self.sync.data_ptr()), ctypes.c_void_p(self.err.data_ptr()),
+                                          E._stream_ptr(stream)))
+
+    def check(self):
+        """Raise if the last persistent launch's barrier wait ran out."""
+        if hasattr(self, 'err') and int(self.err.item()) != 0:
+            raise N.LensError('persistent batched launch: a grid-barrier wait timed out (results invalid)')
+
     def launches(self, n0, n1):
         """Kernel launches of steps [n0, n1): H and E, plus the TM node DFT on window
         steps; one per LENS_TB_K steps for the temporally blocked step."""
@@ -359,10 +379,18 @@ class Sweep:
         self.tuned = [dict(chunk=c, budget=u, s_per_step=t) for t, c, u in res]
         return self.tuned
 
-    def run(self, graphs=True):
-        """Run every group's whole schedule (one CUDA graph per group); returns
-        the number of kernel launches the graphs hold."""
+    def run(self, graphs=True, persistent=False):
+        """Run every group's whole schedule (one CUDA graph per group, or with
+        persistent=True one persistent cooperative launch per group); returns
+        the number of kernel launches."""
         launches = 0
+        if persistent:
+            for g in self.groups:
+                g.step_persistent(self.table, 0, g.steps)
+            torch.cuda.synchronize()
+            for g in self.groups:
+                g.check()
+            return len(self.groups)
         for g in self.groups:
             if graphs:
                 if g.graph is None:

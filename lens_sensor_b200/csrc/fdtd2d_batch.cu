@@ -15,6 +15,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "lens_common.cuh"
@@ -44,8 +45,7 @@ struct Tile {
     int i, j;  // first row and first column of this thread
 };
 
-__device__ __forceinline__ Tile tile_of(const LensInst2D *inst, const int *blk, const int *owner) {
-    const int b = blockIdx.x;
+__device__ __forceinline__ Tile tile_of(const LensInst2D *inst, const int *blk, const int *owner, int b) {
     const int q = __ldg(owner + b);
     const LensInst2D *g = inst + q;
     const int t = b - __ldg(blk + q);
@@ -127,9 +127,10 @@ __device__ __forceinline__ float psi_step(const LensProfile &pf, int m, float *q
     return p;
 }
 
+// H of tile b (boundaries.py:186-194 / 240-247).
 template <typename T>
-__global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
-    const Tile tl = tile_of(inst, blk, owner);
+__device__ __forceinline__ void h_tile(const LensInst2D *inst, const int *blk, const int *owner, int b) {
+    const Tile tl = tile_of(inst, blk, owner, b);
     const V g{tl.g};
     const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
     if (i0 >= nx || j0 >= ny) return;   // j0 < ny <= P: the four columns lie inside the row pitch
@@ -266,10 +267,11 @@ __global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const in
     }
 }
 
+// E of tile b at batch step n (boundaries.py:196-215 / 249-268), source, PEC, node DFT.
 template <typename T>
-__global__ void __launch_bounds__(256, 4)
-    b2d_e(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
-    const Tile tl = tile_of(inst, blk, owner);
+__device__ __forceinline__ void e_tile(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable &tab,
+                                       int n, int b) {
+    const Tile tl = tile_of(inst, blk, owner, b);
     const V g{tl.g};
     const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
     if (i0 >= nx || j0 >= ny) return;
@@ -549,11 +551,11 @@ __global__ void __launch_bounds__(256, 4)
     }
 }
 
-// TM node DFT: Ey averaged onto the nodes (fdtd2d_core.py:458-465).
+// TM node DFT of tile b: Ey averaged onto the nodes (fdtd2d_core.py:458-465).
 template <typename T>
-__global__ void __launch_bounds__(256)
-    b2d_tm_node(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
-    const Tile tl = tile_of(inst, blk, owner);
+__device__ __forceinline__ void node_tile(const LensInst2D *inst, const int *blk, const int *owner,
+                                          const LensStepTable &tab, int n, int b) {
+    const Tile tl = tile_of(inst, blk, owner, b);
     const V g{tl.g};
     if (g.pol() != 1) return;
     const int i0 = tl.i, j0 = tl.j, nx = g.nx(), ny = g.ny(), P = g.pitch();
@@ -574,6 +576,80 @@ __global__ void __launch_bounds__(256)
                                                                     : 0.5f * (S::ld(p1, row + j - 1) + S::ld(p1, row + j));
             dft_node(tl.g, tab, n, row + j, v);
         }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 4) b2d_h(const LensInst2D *inst, const int *blk, const int *owner) {
+    h_tile<T>(inst, blk, owner, blockIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 4)
+    b2d_e(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
+    e_tile<T>(inst, blk, owner, tab, n, blockIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    b2d_tm_node(const LensInst2D *inst, const int *blk, const int *owner, const LensStepTable tab, int n) {
+    node_tile<T>(inst, blk, owner, tab, n, blockIdx.x);
+}
+
+// ------------------------------------------------------ persistent batched run
+// One cooperative launch advances the whole batch by nsteps: the blocks (all
+// resident at once) stride over the batch's tiles in each phase and meet at a
+// grid barrier between the H and E phases of every step (and after the TM node
+// DFT on its window steps), so a batch whose state fits in L2 keeps it there
+// across steps and no launch gap separates them.  Tile b is always handled by
+// block b mod gridDim.x, so a thread's DFT sums stay its own.
+//
+// Barrier: sync[0] counts the arrivals of the current generation sync[1]; the
+// last block to arrive resets the count and opens the next generation.  Every
+// wait is bounded (PB_TRIES polls of at least 64 ns, about a second); a wait that
+// runs out, or sees another block's error, sets *err and the kernel returns.
+constexpr long long PB_TRIES = 1LL << 24;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *sync, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        volatile unsigned *gen = sync + 1;
+        volatile int *verr = err;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+            atomicExch(sync, 0u);
+            __threadfence();
+            atomicAdd(sync + 1, 1u);
+        } else {
+            long long t = 0;
+            while (*gen == g) {
+                if (*verr || ++t > PB_TRIES) {
+                    atomicOr(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *reinterpret_cast<volatile int *>(err) == 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 3)
+    pb2d(const LensInst2D *inst, const int *blk, const int *owner, int nblk, const LensStepTable tab, int n0,
+         int nsteps, int tm_lo, int tm_hi, unsigned *sync, int *err) {
+    for (int n = n0; n < n0 + nsteps; ++n) {
+        for (int b = blockIdx.x; b < nblk; b += gridDim.x) h_tile<T>(inst, blk, owner, b);
+        if (!grid_barrier(sync, err)) return;
+        for (int b = blockIdx.x; b < nblk; b += gridDim.x) e_tile<T>(inst, blk, owner, tab, n, b);
+        if (!grid_barrier(sync, err)) return;
+        // the node DFT reads Ey of the neighbouring tile's first column: after the E
+        // barrier; the next E phase that rewrites Ey comes after the next H barrier
+        if (n >= tm_lo && n < tm_hi)
+            for (int b = blockIdx.x; b < nblk; b += gridDim.x) node_tile<T>(inst, blk, owner, tab, n, b);
     }
 }
 
@@ -663,6 +739,79 @@ extern "C" int lens_batch2d_step(const LensInst2D *inst_host, const LensInst2D *
                                   inst_host, s);
             break;
         default: return LENS_ERR_ARG;
+    }
+    return lens_cuda_status();
+}
+
+namespace {
+
+// Batch steps on which a TM instance accumulates its node DFT: [lo, hi) (empty: lo = hi).
+void tm_window(const LensInst2D *inst, int ninst, int &lo, int &hi) {
+    lo = 1 << 30;
+    hi = -(1 << 30);
+    for (int q = 0; q < ninst; ++q) {
+        const LensInst2D &g = inst[q];
+        if (g.pol != 1 || !g.dft) continue;
+        lo = std::min(lo, g.dft_n0 + g.n_start);
+        hi = std::max(hi, g.dft_n1 + g.n_start);
+    }
+    if (hi < lo) lo = hi = 0;
+}
+
+template <typename T>
+int run_persistent(const LensInst2D *dev, const int *blk, const int *owner, int nblk, int by, const LensStepTable &tab,
+                   int n0, int nsteps, int tm_lo, int tm_hi, unsigned *sync, int *err, cudaStream_t s) {
+    int dv = 0, nsm = 0, per = 0, coop = 0;
+    if (cudaGetDevice(&dv) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dv) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dv) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pb2d<T>, BXB * by, 0) != cudaSuccess)
+        return LENS_ERR_CUDA;
+    if (!coop || per < 1) return LENS_ERR_CUDA;
+    const int grid = std::min(nblk, per * nsm);
+    if (cudaMemsetAsync(sync, 0, 2 * sizeof(unsigned), s) != cudaSuccess ||
+        cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess)
+        return LENS_ERR_CUDA;
+    LensStepTable t = tab;
+    void *args[] = {(void *)&dev, (void *)&blk, (void *)&owner, (void *)&nblk, (void *)&t, (void *)&n0,
+                    (void *)&nsteps, (void *)&tm_lo, (void *)&tm_hi, (void *)&sync, (void *)&err};
+    if (cudaLaunchCooperativeKernel((const void *)pb2d<T>, dim3(grid), dim3(BXB, by), args, 0, s) != cudaSuccess)
+        return LENS_ERR_CUDA;
+    return LENS_OK;
+}
+
+}  // namespace
+
+extern "C" int lens_batch2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const int *blk_dev,
+                                const int *owner_dev, int ninst, int storage, int by, const LensStepTable *tab, int n0,
+                                int nsteps, unsigned *sync, int *err, void *stream) {
+    if (!inst_host || !inst_dev || !blk_dev || !owner_dev || !sync || !err || ninst < 1 || by < 1 ||
+        BXB * by > 256 || nsteps < 0)
+        return LENS_ERR_ARG;
+    long tot = 0;
+    bool any_dft = false;
+    for (int q = 0; q < ninst; ++q) {
+        if (!inst_ok(inst_host[q]) || !lens_table_ok(tab, n0 - inst_host[q].n_start, nsteps)) return LENS_ERR_ARG;
+        tot += inst_blocks(inst_host[q], by);
+        any_dft = any_dft || inst_host[q].dft;
+    }
+    if (tot > 0x7fffffffL) return LENS_ERR_SIZE;
+    if (any_dft && !tab->pe) return LENS_ERR_ARG;
+    if (nsteps == 0) return LENS_OK;
+    int lo, hi;
+    tm_window(inst_host, ninst, lo, hi);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int st;
+    switch (storage) {
+        case LENS_F32: st = run_persistent<float>(inst_dev, blk_dev, owner_dev, (int)tot, by, *tab, n0, nsteps, lo, hi, sync, err, s); break;
+        case LENS_F16: st = run_persistent<__half>(inst_dev, blk_dev, owner_dev, (int)tot, by, *tab, n0, nsteps, lo, hi, sync, err, s); break;
+        case LENS_BF16:
+            st = run_persistent<__nv_bfloat16>(inst_dev, blk_dev, owner_dev, (int)tot, by, *tab, n0, nsteps, lo, hi, sync, err, s);
+            break;
+        default: return LENS_ERR_ARG;
+    }
+    if (st != LENS_OK) {
+        cudaGetLastError();
+        return st;
     }
     return lens_cuda_status();
 }

@@ -36,6 +36,9 @@ def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
 class Solve2D:
     """Resident 2D solve of `steps_total` steps.
 
+    engine='persistent': the batched kernels on this one instance in one
+    persistent cooperative launch per snapshot period (lens_batch2d_run, the
+    grid kept on chip across steps, no launch gaps);
     engine='batch' (default): the batched kernels on this one instance
     (lens_batch2d_step, vector passes over 128 x 2*by tiles; capture() records
     the whole schedule, snapshots included, as one CUDA graph that run()
@@ -62,7 +65,7 @@ class Solve2D:
                                  E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
         self.engine = engine
         self.graph = None
-        if engine in ('tb', 'batch'):
+        if engine in ('tb', 'batch', 'persistent'):
             from . import batch2d as B
             tb = engine == 'tb'
             span = 2 * N.TB_K
@@ -91,14 +94,18 @@ class Solve2D:
             self.grid.step(self.table, n, m - n, self.epi, stream)
             self.launches += 2 * (m - n)
             return
+        if self.engine == 'persistent':
+            self.group.step_persistent(self.table, n, m - n, stream)
+            self.launches += 1
+            return
         self.group.step(self.table, n, m - n, stream)
         self.launches += self.group.launches(n, m)
 
     def capture(self):
         """Record the rest of the schedule (steps and snapshot copies) as one CUDA
         graph; the next run() replays it (batched and temporally blocked engines)."""
-        if self.engine == 'step':
-            raise ValueError("engine='step' launches step by step")
+        if self.engine in ('step', 'persistent'):
+            raise ValueError(f"engine={self.engine!r} is not captured")
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(device=self.snaps.device)
         s.wait_stream(torch.cuda.current_stream())

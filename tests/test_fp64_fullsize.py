@@ -52,7 +52,7 @@ def c0_errors(engine='batch'):
     from lens_sensor_b200.workloads import planar2d_te
     sp, steps = planar2d_te()
     s = Solve2D(sp, steps, engine=engine)
-    if engine != 'step':
+    if engine in ('batch', 'tb'):
         s.capture()
     s.run()
     ph, snaps = s.host_results()
@@ -139,7 +139,7 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('engine', ['batch', 'tb', 'step'])
+@pytest.mark.parametrize('engine', ['batch', 'persistent', 'tb', 'step'])
 def test_config0_planar2d_te_against_fp64(engine):
     e = c0_errors(engine)
     print(f'c0 ({engine}) errors vs FP64:', e, 'reference fp32:', meta()['c0']['ref_fp32_err'])

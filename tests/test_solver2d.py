@@ -1,6 +1,7 @@
-"""The plain 2D solve (solver2d.Solve2D) on its three engines: the batched
-kernels on one instance replayed as one CUDA graph ('batch'), the temporally
-blocked step ('tb') and the single-grid engine ('step').  The snapshots and
+"""The plain 2D solve (solver2d.Solve2D) on its engines: the batched
+kernels on one instance replayed as one CUDA graph ('batch') or run in one
+persistent cooperative launch per snapshot period ('persistent'), the
+temporally blocked step ('tb') and the single-grid engine ('step').  The snapshots and
 the one-period CW phasor must agree (the single-grid engine is pinned to the
 oracle by test_gpu_parity.py; all three to FP64 at full size by
 test_fp64_fullsize.py).  The schedule itself is CPU-checked."""
@@ -36,14 +37,14 @@ def test_engines_agree(pol):
     sp = _spec(pol)
     out = {}
     geo = None
-    for eng in ('step', 'batch', 'tb'):
+    for eng in ('step', 'batch', 'tb', 'persistent'):
         s = Solve2D(sp, 400, snap_every=80, engine=eng, geo=geo)
         geo = s.geo
-        if eng != 'step':
+        if eng in ('batch', 'tb'):
             s.capture()
         s.run()
         out[eng] = s.host_results()
-    for eng in ('batch', 'tb'):
+    for eng in ('batch', 'tb', 'persistent'):
         assert _rel(out[eng][0], out['step'][0]) <= TOL, (eng, 'phasor')
         assert _rel(out[eng][1], out['step'][1]) <= TOL, (eng, 'snapshots')
     assert np.abs(out['step'][0]).max() > 0

@@ -273,15 +273,16 @@ def run_planar2d(cpu=True):
     cells = sp.nx * sp.ny
     geo = None
     rates = {}
-    for eng in ('batch', 'tb', 'step'):
-        warm = Solve2D(sp, steps, engine=eng, geo=geo)
+    cands = [('batch', 2), ('batch', 4), ('batch', 8), ('persistent', 8), ('tb', 4), ('step', 4)]
+    for eng, by in cands:
+        warm = Solve2D(sp, steps, engine=eng, geo=geo, by=by)
         geo = warm.geo
-        if eng != 'step':
+        if eng in ('batch', 'tb'):
             warm.capture()
         warm.run()
         del warm
-        s = Solve2D(sp, steps, engine=eng, geo=geo)
-        if eng != 'step':
+        s = Solve2D(sp, steps, engine=eng, geo=geo, by=by)
+        if eng in ('batch', 'tb'):
             s.capture()
         torch.cuda.synchronize()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -289,27 +290,30 @@ def run_planar2d(cpu=True):
         s.run()
         ev[1].record()
         torch.cuda.synchronize()
-        rates[eng] = (ev[0].elapsed_time(ev[1]) * 1e-3, s.launches)
+        rates[(eng, by)] = (ev[0].elapsed_time(ev[1]) * 1e-3, s.launches)
         del s
-    best = min(rates, key=lambda e: rates[e][0])
-    t_dev, launches = rates[best]
+    best_key = min(rates, key=lambda e: rates[e][0])
+    best, best_by = best_key
+    t_dev, launches = rates[best_key]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s = Solve2D(sp, steps, engine=best)
-    if best != 'step':
+    s = Solve2D(sp, steps, engine=best, by=best_by)
+    if best in ('batch', 'tb'):
         s.capture()
     s.run()
     ph, snaps = s.host_results()
     t_e2e = time.perf_counter() - t0
     peak, peak_src = peaks()
     achieved = 32.0 * cells / (t_dev / steps) / 1e9
-    kern = {'batch': 'b2d_h + b2d_e (batched passes on one instance)',
+    kern = {'batch': f'b2d_h + b2d_e (batched passes on one instance, tiles of 128 x {2 * best_by})',
+            'persistent': 'pb2d (persistent cooperative launch)',
             'tb': 'tb2d (four steps per launch)', 'step': 'te2d_h + te2d_e (single-grid passes)'}[best]
     out = dict(workload=f'planar2d_te: 2D TE planar waveguide {sp.nx}x{sp.ny} @ 25 nm, fp32, 12-cell CPML, '
                         f'{steps} steps, CW ramped over 20 periods, one seeded PS bead, one-period phasor, '
                         'Ez snapshots every 200 steps',
                unit=UNIT, value=cells * steps / t_dev, ms_per_step=t_dev / steps * 1e3, steps=steps, cells=cells,
-               engine=best, engines={e: cells * steps / t for e, (t, _) in rates.items()}, gpu_launches=launches,
+               engine=best, by=best_by,
+               engines={f'{e}_by{b}': cells * steps / t for (e, b), (t, _) in rates.items()}, gpu_launches=launches,
                l2=f'working set {(5 * cells * 4) / 1e6:.0f} MB of fields and coefficients fits in the 126 MB L2: '
                   'the steps of one solve run L2-resident, as in use; no flush between steps',
                roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
@@ -375,6 +379,20 @@ def run_batched(plain_sample=16, count=256):
     e1.record()
     torch.cuda.synchronize()
     t_p = e0.elapsed_time(e1) * 1e-3
+    # the fastest one-at-a-time path: each sampled instance alone on the batched
+    # kernels, its whole schedule replayed as one CUDA graph (Solve2D's 'batch' engine)
+    alone = []
+    for q in idx:
+        one = B.Sweep([specs[q]], steps, 'f32', by=sw.by, geos=[sw.insts[q].geo])
+        one.groups[0].capture(one.table)
+        alone.append(one)
+    e0.record()
+    for one in alone:
+        one.run()
+    e1.record()
+    torch.cuda.synchronize()
+    t_g = e0.elapsed_time(e1) * 1e-3
+    del alone
     geos = [q.geo for q in sw.insts]
     by, budget = sw.by, sw.budget
     del sw
@@ -388,6 +406,15 @@ def run_batched(plain_sample=16, count=256):
     torch.cuda.synchronize()
     t_h = e0.elapsed_time(e1) * 1e-3
     res16 = sh.results()
+    # the same FP32 sweep as one persistent cooperative launch per group (lens_batch2d_run)
+    sp_ = B.Sweep(specs, steps, 'f32', by=by, budget=budget, geos=geos)
+    e0.record()
+    sp_.run(persistent=True)
+    e1.record()
+    torch.cuda.synchronize()
+    t_pers = e0.elapsed_time(e1) * 1e-3
+    pers_same = all(torch.equal(a['phasor'], b) for a, b in zip(sp_.results(), ref))
+    del sp_
     err = [float((r['phasor'] - ref[q]).abs().norm() / max(float(ref[q].abs().norm()), 1e-300))
            for q, r in enumerate(res16)]
     fp64 = None
@@ -412,13 +439,20 @@ def run_batched(plain_sample=16, count=256):
     del gres
     torch.cuda.empty_cache()
     plain = pc * steps / t_p
+    plain_graph = pc * steps / t_g
     f32 = cells * steps / t_b
     f16 = cells * steps / t_h
     return dict(workload=f'sweep2d: {len(specs)} uneven 2D TE/TM solves, widths 600-2400 x heights 300-560 @ 25 nm, '
                          '12-cell CPML, 4000 steps, seeded tear-film / lipid / bead sweep',
                 unit=UNIT, cells_total=cells, steps=steps, plain=plain,
-                plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time',
+                plain_sample=f'{len(idx)} instances (every {len(specs) // len(idx)}th) one at a time, through '
+                             'the drop-in single-grid engine (run_beads path)',
+                plain_graph=plain_graph,
+                plain_graph_sample='the same instances one at a time on the batched kernels, each schedule '
+                                   'replayed as one CUDA graph (the fastest one-at-a-time path)',
                 batched_f32=f32, batched_f16=f16, batched_vs_plain=f32 / plain, f16_vs_plain=f16 / plain,
+                batched_vs_plain_graph=f32 / plain_graph,
+                batched_persistent_f32=cells * steps / t_pers, persistent_identical_to_graphs=pers_same,
                 tile=f'128 x {2 * by} nodes', group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
                 f16_phasor_err_vs_f32_max=max(err), f16_phasor_err_vs_f32_median=float(np.median(err)),
                 K_median=float(np.median(K)), err_vs_fp64=fp64, f16_gate=gate)

@@ -381,18 +381,19 @@ def run_batched(plain_sample=16, count=256):
     t_p = e0.elapsed_time(e1) * 1e-3
     # the fastest one-at-a-time path: each sampled instance alone on the batched
     # kernels, its whole schedule replayed as one CUDA graph (Solve2D's 'batch' engine)
-    alone = []
+    t_g = 0.0
     for q in idx:
         one = B.Sweep([specs[q]], steps, 'f32', by=sw.by, geos=[sw.insts[q].geo])
         one.groups[0].capture(one.table)
-        alone.append(one)
-    e0.record()
-    for one in alone:
+        one.run()                      # the graph's first launch uploads it
+        torch.cuda.synchronize()
+        one.reset()
+        e0.record()
         one.run()
-    e1.record()
-    torch.cuda.synchronize()
-    t_g = e0.elapsed_time(e1) * 1e-3
-    del alone
+        e1.record()
+        torch.cuda.synchronize()
+        t_g += e0.elapsed_time(e1) * 1e-3
+        del one
     geos = [q.geo for q in sw.insts]
     by, budget = sw.by, sw.budget
     del sw

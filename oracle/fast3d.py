@@ -1,7 +1,7 @@
 """Multi-threaded C++ stepper for the oracle's 3D grid (TEST INFRASTRUCTURE ONLY).
 
 Grid3DC is oracle.fdtd_oracle.Grid3D with its step() done by oracle/o3.cpp
-(same operation order, OpenMP over x-planes); the fields stay NumPy arrays of the
+(same operation order, std::thread workers over x-planes); the fields stay NumPy arrays of the
 reference's shapes, so the oracle's source injection, detector sums, flux
 pairs and |E|^2 averaging run on them unchanged.  tests/test_oracle_c.py checks
 Grid3DC against Grid3D bit for bit in float32 and float64.  Used only to make

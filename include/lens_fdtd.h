@@ -33,6 +33,8 @@
 #ifndef LENS_FDTD_H
 #define LENS_FDTD_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -295,6 +297,46 @@ int lens_tb2d_plan(const LensTB2D *inst, int ninst, int chunk, int *first);
 int lens_tb2d_step(const LensTB2D *inst_host, const LensTB2D *inst_dev, const int *first_dev, int ninst,
                    int chunk, int storage, const LensStepTable *tab, int n0, int nsteps, void *stream);
 
+/* ------------------------------------------------- resident 2D solves
+ * A group of FP32 instances whose state fits on the chip, advanced by nsteps
+ * in ONE cooperative launch that keeps every field value in registers from the
+ * first step to the last: a CTA owns a band of x rows of one instance (every y
+ * column, ny <= 576), and neighbouring bands exchange one row per half step
+ * through L2 as {value, step tag} words.  No counterpart entry in the
+ * reference (its loop advances one step per call, fdtd2d_core.py:781-847);
+ * the per-cell update is lens_batch2d_step's.  Outputs per instance: the node
+ * DFT into g.dft over [dft_n0, dft_n1) as (re, im), or compensated (re, im,
+ * c_re, c_im) with kahan = 1, and optional snapshot frames of the driven raw
+ * component (TE Ez (nx, ny), TM Ey (nx, ny - 1)): frame f holds the field after
+ * the instance's own step (f + 1) * every - 1.  Every instance must have started
+ * (n_start <= n0).  Waits between bands are bounded (a few seconds at most); if
+ * one runs out *err becomes nonzero, the launch ends and the results are
+ * invalid.                                                                   */
+#define LENS_RS_MAX_INST 32
+
+typedef struct {
+    float *frames;      /* NULL: none                                          */
+    int every, nframes; /* frame cadence (own steps) and the frames' count     */
+    int kahan;          /* g.dft layout: 1 (re, im, c_re, c_im), 0 (re, im)    */
+} LensRsOut2D;
+
+/* Band plan on the current device: rows per band, CTAs and threads per CTA;
+ * LENS_ERR_SIZE when the group does not fit on the chip (more bands than
+ * resident CTAs at 20 rows per band, ny > 576, a y strip wider than 64, or
+ * more than LENS_RS_MAX_INST instances).                                     */
+int lens_rs2d_plan(const LensInst2D *inst, int ninst, int *rows, int *ctas, int *threads);
+
+/* Bytes of the halo scratch of a plan (device memory, the caller's).        */
+size_t lens_rs2d_scratch_bytes(int ctas, int threads);
+
+/* Advance every instance by nsteps from batch step n0.  inst_host / inst_dev:
+ * the same descriptors in host and device memory; out: NULL or ninst entries
+ * (host memory); scratch: scratch_bytes of device memory; err: a device int.
+ * The call zeroes scratch and *err on `stream` before the launch.            */
+int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const LensRsOut2D *out, int ninst,
+                  const LensStepTable *tab, int n0, int nsteps, void *scratch, size_t scratch_bytes, int *err,
+                  void *stream);
+
 /* ---------------------------------------------------------------- 3D grid */
 /* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
  * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same
@@ -423,8 +465,8 @@ const char *lens_status_string(int status);
 
 /* sizeof of the ABI structs, in this order: LensProfile, LensAxis, LensStepTable,
  * LensSource, LensTE2D, LensTM2D, LensEpi2D, LensGrid3D, LensEpi3D, LensInst2D,
- * LensDrive3D, LensDrive2D, LensTB2D, LensTB3D.  Writes min(n, 14) entries and
- * returns 14 (bindings check their mirrors). */
+ * LensDrive3D, LensDrive2D, LensTB2D, LensTB3D, LensRsOut2D.  Writes min(n, 15)
+ * entries and returns 15 (bindings check their mirrors). */
 int lens_abi_sizes(int *sizes, int n);
 
 #ifdef __cplusplus

@@ -109,6 +109,13 @@ class TB3D(ctypes.Structure):
     _fields_ = [('psi_lv', c_void_p * 12), ('chunk', c_int)]
 
 
+class RsOut2D(ctypes.Structure):
+    _fields_ = [('frames', c_void_p), ('every', c_int), ('nframes', c_int), ('kahan', c_int)]
+
+
+RS_MAX_INST = 32
+
+
 TB3_K = 2
 
 
@@ -120,7 +127,8 @@ class Drive2D(ctypes.Structure):
     _fields_ = [('nplanes', c_int), ('taper', c_void_p), ('hand', c_void_p), ('tab', c_void_p)]
 
 
-MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D, TB2D, TB3D)
+MIRRORS = (Profile, Axis, StepTable, Source, TE2D, TM2D, Epi2D, Grid3D, Epi3D, Inst2D, Drive3D, Drive2D, TB2D, TB3D,
+           RsOut2D)
 
 # Every exported entry point with its ctypes signature (checked by the tests
 # against include/lens_fdtd.h).
@@ -148,6 +156,10 @@ SIGNATURES = {
     'lens_tb2d_plan': (c_int, [POINTER(TB2D), c_int, c_int, POINTER(c_int)]),
     'lens_tb2d_step': (c_int, [POINTER(TB2D), c_void_p, c_void_p, c_int, c_int, c_int, POINTER(StepTable), c_int,
                                c_int, c_void_p]),
+    'lens_rs2d_plan': (c_int, [POINTER(Inst2D), c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    'lens_rs2d_scratch_bytes': (ctypes.c_size_t, [c_int, c_int]),
+    'lens_rs2d_run': (c_int, [POINTER(Inst2D), c_void_p, POINTER(RsOut2D), c_int, POINTER(StepTable), c_int, c_int,
+                              c_void_p, ctypes.c_size_t, c_void_p, c_void_p]),
     'lens_version': (c_int, []),
     'lens_status_string': (ctypes.c_char_p, [c_int]),
     'lens_abi_sizes': (c_int, [POINTER(c_int), c_int]),

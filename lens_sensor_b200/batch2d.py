@@ -280,6 +280,66 @@ class Group:
         return g
 
 
+class ResidentGroup:
+    """FP32 instances advanced by ONE resident cooperative launch per call
+    (lens_rs2d_run): every field value stays in registers from the first step
+    to the last, bands of x rows exchanging one row per half step through L2.
+
+    frames: per instance None or (every, tensor (nframes, nx, ny) TE / (nframes,
+    nx, ny-1) TM) of snapshot frames written by the kernel; an instance with
+    kahan=True accumulates its DFT compensated."""
+
+    def __init__(self, insts, dev, frames=None):
+        if any(q.f[0].dtype != torch.float32 for q in insts):
+            raise ValueError('the resident launch keeps FP32 state: FP32 instances only')
+        n = len(insts)
+        self.insts, self.dev = insts, dev
+        self.lib = N.load()
+        self.steps = max(q.steps for q in insts)
+        self.host = (N.Inst2D * n)(*[q.s for q in insts])
+        rows, ctas, threads = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.check(self.lib.lens_rs2d_plan(self.host, n, ctypes.byref(rows), ctypes.byref(ctas), ctypes.byref(threads)))
+        self.rows, self.ctas, self.threads = rows.value, ctas.value, threads.value
+        raw = ctypes.string_at(ctypes.addressof(self.host), ctypes.sizeof(self.host))
+        self.dev_desc = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev)
+        nb = self.lib.lens_rs2d_scratch_bytes(self.ctas, self.threads)
+        self.scratch = torch.empty(max(8, nb), dtype=torch.uint8, device=dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.out = (N.RsOut2D * n)()
+        self._frames = []
+        for k, q in enumerate(insts):
+            self.out[k].kahan = 1 if q.kahan else 0
+            fr = frames[k] if frames is not None else None
+            if fr is not None:
+                every, t = fr
+                self.out[k].frames, self.out[k].every, self.out[k].nframes = t.data_ptr(), int(every), int(t.shape[0])
+                self._frames.append(t)
+
+    @staticmethod
+    def fits(insts):
+        """True when lens_rs2d_plan places these instances on this device."""
+        n = len(insts)
+        if n < 1 or n > N.RS_MAX_INST:
+            return False
+        host = (N.Inst2D * n)(*[q.s for q in insts])
+        r, c, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        return N.load().lens_rs2d_plan(host, n, ctypes.byref(r), ctypes.byref(c), ctypes.byref(t)) == 0
+
+    def step(self, tab, n0, nsteps, stream=None):
+        N.check(self.lib.lens_rs2d_run(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()), self.out,
+                                       len(self.insts), ctypes.byref(tab.s), int(n0), int(nsteps),
+                                       ctypes.c_void_p(self.scratch.data_ptr()), self.scratch.numel(),
+                                       ctypes.c_void_p(self.err.data_ptr()), E._stream_ptr(stream)))
+
+    def check(self):
+        """Raise if the last launch's wait between bands ran out."""
+        if int(self.err.item()) != 0:
+            raise N.LensError('resident 2D launch: a wait between bands timed out (results invalid)')
+
+    def launches(self, n0, n1):
+        return 1 if n1 > n0 else 0
+
+
 class Sweep:
     """A batched sweep of 2D solves (one shared time step and wavelength).
 
@@ -287,9 +347,12 @@ class Sweep:
     resident state per group (None: one group).  autotune() chooses both."""
 
     def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None, tb=False,
-                 chunk=64):
+                 chunk=64, resident=False):
         dev = self.dev = E._device(device)
         self.tb, self.chunk = bool(tb), int(chunk)
+        self.resident = bool(resident)
+        if self.resident and (self.tb or storage != 'f32'):
+            raise ValueError('the resident sweep keeps FP32 state on chip: storage f32, tb False')
         if self.tb and int(steps) % (2 * N.TB_K):
             raise ValueError(f'the temporally blocked sweep runs in spans of {2 * N.TB_K} steps')
         if storage not in DTYPES:
@@ -311,6 +374,8 @@ class Sweep:
         self.tuned = None
 
     def _groups(self, by, budget):
+        if self.resident:
+            return self._resident_groups()
         order = sorted(range(len(self.insts)), key=lambda q: -self.insts[q].nbytes())
         groups, cur, size = [], [], 0
         for q in order:
@@ -323,6 +388,24 @@ class Sweep:
         if cur:
             groups.append(cur)
         return [Group(g, self.storage, by, self.dev, tb=self.tb, chunk=self.chunk) for g in groups]
+
+    def _resident_groups(self):
+        """Instances packed into resident launches in order of height (similar
+        column counts share a launch's threads), each launch as full as the
+        chip holds."""
+        order = sorted(self.insts, key=lambda q: (q.spec.ny, q.spec.nx))
+        groups, cur = [], []
+        for q in order:
+            if cur and not ResidentGroup.fits(cur + [q]):
+                groups.append(cur)
+                cur = []
+            cur.append(q)
+        if cur:
+            groups.append(cur)
+        for g in groups:
+            if not ResidentGroup.fits(g):
+                raise ValueError('an instance does not fit the resident launch: use the batched sweep')
+        return [ResidentGroup(g, self.dev) for g in groups]
 
     def cells(self):
         return sum(q.spec.nx * q.spec.ny for q in self.insts)
@@ -338,6 +421,10 @@ class Sweep:
         temporally blocked sweep tunes (rows per chunk, group budget) instead."""
         if self.tb:
             return self._autotune_tb()
+        if self.resident:   # one launch per group, its band plan fixed by the device
+            self.tuned = [dict(rows=g.rows, ctas=g.ctas, threads=g.threads, instances=len(g.insts))
+                          for g in self.groups]
+            return self.tuned
         res = []
         for by, budget in candidates:
             groups = self._groups(by, budget)
@@ -384,6 +471,13 @@ class Sweep:
         persistent=True one persistent cooperative launch per group); returns
         the number of kernel launches."""
         launches = 0
+        if self.resident:
+            for g in self.groups:
+                g.step(self.table, 0, g.steps)
+            torch.cuda.synchronize()
+            for g in self.groups:
+                g.check()
+            return len(self.groups)
         if persistent:
             for g in self.groups:
                 g.step_persistent(self.table, 0, g.steps)

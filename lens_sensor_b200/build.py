@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, 'csrc')
 LIBDIR = os.path.join(HERE, '_lib')
 LIB = os.path.join(LIBDIR, 'liblens_fdtd.so')
-SOURCES = ['fdtd2d.cu', 'fdtd2d_batch.cu', 'fdtd2d_tb.cu', 'fdtd3d.cu', 'fdtd3d_tb.cu']
+SOURCES = ['fdtd2d.cu', 'fdtd2d_batch.cu', 'fdtd2d_resident.cu', 'fdtd2d_tb.cu', 'fdtd3d.cu', 'fdtd3d_tb.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -1687,13 +1687,13 @@ extern "C" int lens_fdtd3d_accum_e2(const LensGrid3D *g, int target, int nx_targ
 extern "C" int lens_version(void) { return 100; }
 
 extern "C" int lens_abi_sizes(int *sizes, int n) {
-    const int v[14] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
+    const int v[15] = {(int)sizeof(LensProfile), (int)sizeof(LensAxis), (int)sizeof(LensStepTable),
                        (int)sizeof(LensSource),  (int)sizeof(LensTE2D), (int)sizeof(LensTM2D),
                        (int)sizeof(LensEpi2D),   (int)sizeof(LensGrid3D), (int)sizeof(LensEpi3D),
                        (int)sizeof(LensInst2D),  (int)sizeof(LensDrive3D), (int)sizeof(LensDrive2D),
-                       (int)sizeof(LensTB2D), (int)sizeof(LensTB3D)};
-    for (int q = 0; q < n && q < 14; ++q) sizes[q] = v[q];
-    return 14;
+                       (int)sizeof(LensTB2D), (int)sizeof(LensTB3D), (int)sizeof(LensRsOut2D)};
+    for (int q = 0; q < n && q < 15; ++q) sizes[q] = v[q];
+    return 15;
 }
 
 extern "C" const char *lens_status_string(int status) {

@@ -36,6 +36,11 @@ def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
 class Solve2D:
     """Resident 2D solve of `steps_total` steps.
 
+    engine='resident': the whole schedule in ONE cooperative launch that keeps
+    the fields in registers (lens_rs2d_run, bands of x rows exchanging one row
+    per half step through L2), the snapshots written by the kernel and the DFT
+    accumulated compensated; the grid must fit on the chip (ny <= 576, at most
+    20 rows per band);
     engine='persistent': the batched kernels on this one instance in one
     persistent cooperative launch per snapshot period (lens_batch2d_run, the
     grid kept on chip across steps, no launch gaps);
@@ -65,6 +70,20 @@ class Solve2D:
                                  E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
         self.engine = engine
         self.graph = None
+        if engine == 'resident':
+            from . import batch2d as B
+            dev = E._device(device)
+            self.inst = B.Instance(sp, self.steps_total, torch.float32, dev, g, kahan=True, window=self.dft)
+            self.grid = self.epi = None
+            shape = (sp.nx, sp.ny) if sp.pol == 's' else (sp.nx, sp.ny - 1)
+            self.snaps = torch.zeros((len(self.snap_steps),) + shape, dtype=torch.float32, device=dev)
+            frames = [(snap_every, self.snaps)] if self.snap_steps else None
+            self.group = B.ResidentGroup([self.inst], dev, frames=frames)
+            fld = self.inst.f[0] if sp.pol == 's' else self.inst.f[1]
+            self._view = lambda: fld[:shape[0], :shape[1]]
+            self.n = 0
+            self.launches = 0
+            return
         if engine in ('tb', 'batch', 'persistent'):
             from . import batch2d as B
             tb = engine == 'tb'
@@ -90,6 +109,10 @@ class Solve2D:
 
     def _advance(self, n, m, stream):
         """Steps [n, m)."""
+        if self.engine == 'resident':
+            self.group.step(self.table, n, m - n, stream)
+            self.launches += 1
+            return
         if self.engine == 'step':
             self.grid.step(self.table, n, m - n, self.epi, stream)
             self.launches += 2 * (m - n)
@@ -104,7 +127,7 @@ class Solve2D:
     def capture(self):
         """Record the rest of the schedule (steps and snapshot copies) as one CUDA
         graph; the next run() replays it (batched and temporally blocked engines)."""
-        if self.engine in ('step', 'persistent'):
+        if self.engine in ('step', 'persistent', 'resident'):
             raise ValueError(f"engine={self.engine!r} is not captured")
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(device=self.snaps.device)
@@ -132,6 +155,11 @@ class Solve2D:
 
     def _schedule(self, stream):
         n = self.n
+        if self.engine == 'resident':   # one launch; the kernel writes the snapshot frames
+            if self.steps_total > n:
+                self._advance(n, self.steps_total, stream)
+            self.n = self.steps_total
+            return self
         with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
             for q, m in enumerate(self.snap_steps + [self.steps_total]):
                 if m > n:
@@ -141,6 +169,11 @@ class Solve2D:
                     self.snaps[q].copy_(self._view())
         self.n = n
         return self
+
+    def check(self):
+        """Raise if a resident launch's wait between bands ran out."""
+        if self.engine == 'resident':
+            self.group.check()
 
     def phasor(self):
         """(2/N) sum F e^{-i w t} on the nodes (nx, ny), complex128 on the device."""

@@ -46,8 +46,9 @@ def rel(a, b):
 
 def c0_errors(engine='batch'):
     """Config 0 (planar2d_te, 1600 x 480, 6000 steps) on the batched kernels
-    ('batch', graph-replayed), the temporally blocked step ('tb') or the
-    single-grid engine ('step')."""
+    ('batch', graph-replayed), the resident launch ('resident'), the persistent
+    batched launch, the temporally blocked step ('tb') or the single-grid
+    engine ('step')."""
     from lens_sensor_b200.solver2d import Solve2D
     from lens_sensor_b200.workloads import planar2d_te
     sp, steps = planar2d_te()
@@ -125,6 +126,13 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
                 out[f'sw{q}_{"tb" if tb else "batched"}_{st}'] = rel(ph.ravel()[sample_mask(ph.size, 3)], ref[q])
             del sw
             torch.cuda.empty_cache()
+    sw = B.Sweep(sel, steps, 'f32', geos=geos, resident=True)
+    sw.run()
+    for q, r in zip(SWEEP_Q, sw.results()):
+        ph = r['phasor'].cpu().numpy()
+        out[f'sw{q}_resident'] = rel(ph.ravel()[sample_mask(ph.size, 3)], ref[q])
+    del sw
+    torch.cuda.empty_cache()
     for q, sp, geo in zip(SWEEP_Q, sel, geos):
         coef = {k: geo[k] for k in ('ce_e', 'ce_h', 'ca_x', 'ca_y', 'da_x', 'da_y') if geo.get(k) is not None}
         g = E.Grid2D(sp.pol, sp.nx, sp.ny, sp.dx, sp.dt, coef, geo['cx'], geo['cy'], geo['src'])
@@ -139,7 +147,7 @@ def sweep_errors(storages=('f32', 'f16', 'bf16')):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('engine', ['batch', 'persistent', 'tb', 'step'])
+@pytest.mark.parametrize('engine', ['batch', 'resident', 'persistent', 'tb', 'step'])
 def test_config0_planar2d_te_against_fp64(engine):
     e = c0_errors(engine)
     print(f'c0 ({engine}) errors vs FP64:', e, 'reference fp32:', meta()['c0']['ref_fp32_err'])
@@ -172,5 +180,6 @@ def test_sweep_instances_against_fp64():
     for q in SWEEP_Q:
         assert e[f'sw{q}_batched_f32'] <= TOL, (q, e)
         assert e[f'sw{q}_tb_f32'] <= TOL, (q, e)
+        assert e[f'sw{q}_resident'] <= TOL, (q, e)
         assert e[f'sw{q}_single'] <= TOL, (q, e)
         assert e[f'sw{q}_batched_f16'] < 1e-2 and e[f'sw{q}_batched_bf16'] < 5e-2, (q, e)

@@ -66,11 +66,12 @@ constexpr unsigned T_LEAN_MASK = T_HX | T_JLT | T_JIN | T_YH | T_YE | T_JPEC, T_
 enum : unsigned { B_PREV = 1u, B_NEXT = 2u, B_LOSSY = 4u, B_KAHAN = 8u };
 
 // Row constants of a band (shared memory): x profile values and strip indices.
-struct RowC {
+struct __align__(16) RowC {
     float kxh, kxe, bxh, cxh, bxe, cxe;
     int sxh_sxe;         // x-strip index of the H psi (low 16 bits) and E psi (high 16 bits)
     unsigned flags;
 };
+static_assert(sizeof(RowC) % 16 == 0 && alignof(RowC) == 16, "row constants: whole 16-byte vectors");
 
 // Band constants (shared memory, read into registers before the step loop).
 struct Band {
@@ -256,7 +257,11 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
     float *zb = ypc + 4 * RS_MAXWY;      // lane 0 of each warp: E field read at j+1 (TE Ez, TM Ex)
     float *xb = zb + RM * RS_MAXW;       // lane 31: H field read at j-1 (TE Hx, TM Hz)
     float *eb = xb + RM * RS_MAXW;       // lane 31: TM Ey (node average)
-    RowC *rowc = reinterpret_cast<RowC *>(eb + RM * RS_MAXW);
+    float *junk = eb + RM * RS_MAXW;     // [NT]: the y-psi slot of a column outside the y strips (stays 0)
+    // the row constants are read as 16-byte vectors: their array starts on a 16-byte boundary
+    RowC *rowc = reinterpret_cast<RowC *>((reinterpret_cast<uintptr_t>(junk + NT) + 15) & ~uintptr_t(15));
+    for (int t = threadIdx.y * 32 + threadIdx.x; t < 2 * RM * NT + 2 * RM * RS_MAXWY; t += NT) xps_h[t] = 0.f;
+    junk[w * 32 + lane] = 0.f;
     Band &B = *reinterpret_cast<Band *>(rowc + RM);
     band_setup<RM, POL>(gp, pl, q, cta, NT, B, rowc, ypc, cs);
     __syncthreads();
@@ -268,6 +273,12 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
     const int sjh = (j < ny - 1) ? strip_of(j, gp->ay.h.lo, gp->ay.h.hi, ny - 1) : -1;
     const int sje = (j > 0 && j < ny - 1) ? strip_of(j, gp->ay.e.lo, gp->ay.e.hi, ny) : -1;
     const float kyh = j < ny - 1 ? __ldg(gp->ay.h.ik + j) : 0.f, kye = j < ny ? __ldg(gp->ay.e.ik + j) : 0.f;
+    const float byh = sjh >= 0 ? ypc[sjh] : 0.f, cyh = sjh >= 0 ? ypc[RS_MAXWY + sjh] : 0.f;
+    const float bye = sje >= 0 ? ypc[2 * RS_MAXWY + sje] : 0.f, cye = sje >= 0 ? ypc[3 * RS_MAXWY + sje] : 0.f;
+    // y-psi slot of row r: yqh + r * ysh (H), yqe + r * yse (E); outside the strips a
+    // zero slot of this thread's own, with b = c = 0, so the psi terms need no branch
+    float *yqh = sjh >= 0 ? yps_h + sjh : junk + j, *yqe = sje >= 0 ? yps_e + sje : junk + j;
+    const int ysh = sjh >= 0 ? RS_MAXWY : 0, yse = sje >= 0 ? RS_MAXWY : 0;
     unsigned tf = 0;
     if (j < ny - 1) tf |= T_HX;
     if (j < ny) tf |= T_JLT;
@@ -329,35 +340,72 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         if (lane == 0) u = w > 0 ? edge[r * RS_MAXW + w - 1] : 0.f;
         return u;
     };
-    // H of row r (any band), en: the E field of row i+1 (TE Ez, TM Ey)
-    auto h_row = [&](int r, float en) {
-        const RowC &rc = rowc[r];
+    // thread tests, as booleans
+    const bool t_hx = tf & T_HX, t_jlt = tf & T_JLT, t_jin = tf & T_JIN, t_yh = tf & T_YH, t_ye = tf & T_YE,
+               t_zero = (tf & T_JPEC) || !(tf & T_JLT), t_jpec = tf & T_JPEC, t_src = tf & T_SRCJ;
+    // The general rows evaluate every update and keep it where it applies
+    // (selects): psi slots exist for every row and column (zero outside the
+    // strips, with b = c = 0 there), so no psi term is a branch and the
+    // compiler interleaves the rows.  A psi value is stored back only where the
+    // batched kernels update it.
+    // H of row r below the band's last (TE: also Hx of every row, the last included)
+    auto h_gen = [&](int r) {
+        const RowC rc = rowc[r];
         const unsigned rf = rc.flags;
+        const bool below = r + 1 < R;
         if (POL == 0) {
             const float ez = fa[r];
-            const float ezj = nb_up(ez, r);
-            if (tf & T_HX) {  // Hx (boundaries.py:186-190)
-                const float d = ezj - ez;
-                float p = 0.f;
-                if (tf & T_YH) p = psi_upd(ypc[sjh], ypc[RS_MAXWY + sjh], yps_h + r * RS_MAXWY + sjh, d);
-                fb[r] = fb[r] - ch * (d * kyh + p);
+            const float d = nb_up(ez, r) - ez;
+            float *qy = yqh + r * ysh;
+            const float py = byh * (*qy) + cyh * d;  // psi_hxy (the zero slot outside the strip)
+            *qy = py;
+            const float hx = fb[r] - ch * (d * kyh + py);  // Hx (boundaries.py:186-190)
+            fb[r] = t_hx ? hx : fb[r];
+            if (r + 1 < RM) {  // Hy (:191-194)
+                const float d2 = fa[r + 1] - ez;
+                float *qx = xps_h + r * NT + j;
+                const float ox = *qx, px = rc.bxh * ox + rc.cxh * d2;
+                const bool on = below && (rf & R_HOK) && t_jlt;
+                *qx = on ? px : ox;
+                const float hy = fc[r] + ch * (d2 * rc.kxh + px);
+                fc[r] = on ? hy : fc[r];
             }
-            if ((rf & R_HOK) && (tf & T_JLT)) {  // Hy (:191-194)
-                const float d = en - ez;
-                float p = 0.f;
-                if (rf & R_XH) p = psi_upd(rc.bxh, rc.cxh, xps_h + r * NT + j, d);
-                fc[r] = fc[r] + ch * (d * rc.kxh + p);
-            }
-        } else {  // Hz (boundaries.py:240-247)
+        } else if (r + 1 < RM) {  // Hz (boundaries.py:240-247)
             const float ex = fa[r];
-            const float exj = nb_up(ex, r);
-            if ((rf & R_HOK) && (tf & T_HX)) {
-                const float dyx = en - fb[r], dxy = exj - ex;
-                float px = 0.f, py = 0.f;
-                if (rf & R_XH) px = psi_upd(rc.bxh, rc.cxh, xps_h + r * NT + j, dyx);
-                if (tf & T_YH) py = psi_upd(ypc[sjh], ypc[RS_MAXWY + sjh], yps_h + r * RS_MAXWY + sjh, dxy);
-                fc[r] = fc[r] - ch * ((dyx * rc.kxh + px) - (dxy * kyh + py));
-            }
+            const float dyx = fb[r + 1] - fb[r], dxy = nb_up(ex, r) - ex;
+            const bool on = below && (rf & R_HOK) && t_hx;
+            float *qx = xps_h + r * NT + j, *qy = yqh + r * ysh;
+            const float ox = *qx, oy = *qy;
+            const float px = rc.bxh * ox + rc.cxh * dyx, py = byh * oy + cyh * dxy;
+            *qx = on ? px : ox;
+            *qy = on ? py : oy;
+            const float hz = fc[r] - ch * ((dyx * rc.kxh + px) - (dxy * kyh + py));
+            fc[r] = on ? hz : fc[r];
+        }
+    };
+    // the band's last row (TE Hy, TM Hz) from en: the E field of row i+1 (TE Ez, TM Ey)
+    auto h_last = [&](int r, float en) {
+        const RowC rc = rowc[r];
+        const unsigned rf = rc.flags;
+        if (POL == 0) {
+            const float d2 = en - fa[r];
+            float *qx = xps_h + r * NT + j;
+            const float ox = *qx, px = rc.bxh * ox + rc.cxh * d2;
+            const bool on = (rf & R_HOK) && t_jlt;
+            *qx = on ? px : ox;
+            const float hy = fc[r] + ch * (d2 * rc.kxh + px);
+            fc[r] = on ? hy : fc[r];
+        } else {
+            const float ex = fa[r];
+            const float dyx = en - fb[r], dxy = nb_up(ex, r) - ex;
+            const bool on = (rf & R_HOK) && t_hx;
+            float *qx = xps_h + r * NT + j, *qy = yqh + r * ysh;
+            const float ox = *qx, oy = *qy;
+            const float px = rc.bxh * ox + rc.cxh * dyx, py = byh * oy + cyh * dxy;
+            *qx = on ? px : ox;
+            *qy = on ? py : oy;
+            const float hz = fc[r] - ch * ((dyx * rc.kxh + px) - (dxy * kyh + py));
+            fc[r] = on ? hz : fc[r];
         }
     };
     // source term of row flags rf at table row k (vcsel.py:151-156)
@@ -368,52 +416,44 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
     };
     // E of row r (any band) at table row k; hm: the H field of row i-1 (TE Hy, TM Hz)
     auto e_row = [&](int r, float hm, int k) {
-        const RowC &rc = rowc[r];
+        const RowC rc = rowc[r];
         const unsigned rf = rc.flags;
+        const bool rin = rf & R_IN;
         if (POL == 0) {
             const float hx = fb[r];
-            const float hxm = nb_dn(xb, hx, r);
+            const float dhy = fc[r] - hm, dhx = hx - nb_dn(xb, hx, r);
+            float *qx = xps_e + r * NT + j, *qy = yqe + r * yse;
+            const float ox = *qx, oy = *qy;
+            const float px = rc.bxe * ox + rc.cxe * dhy, py = bye * oy + cye * dhx;
+            *qx = t_jin ? px : ox;  // zero outside the x strips (b = c = 0)
+            *qy = rin ? py : oy;
+            const float c0 = csj[(r * NC) * NT], c1 = csj[(r * NC + 1) * NT];
             float v = fa[r];
-            if ((rf & R_IN) && (tf & T_JIN)) {  // Ez (boundaries.py:196-215)
-                const float dhy = fc[r] - hm, dhx = hx - hxm;
-                float qx = 0.f, qy = 0.f;
-                if (rf & R_XE) qx = psi_upd(rc.bxe, rc.cxe, xps_e + r * NT + j, dhy);
-                if (tf & T_YE) qy = psi_upd(ypc[2 * RS_MAXWY + sje], ypc[3 * RS_MAXWY + sje], yps_e + r * RS_MAXWY + sje, dhx);
-                const float c0 = csj[(r * NC) * NT], c1 = csj[(r * NC + 1) * NT];
-                v = c0 * v + c1 * (dhy * rc.kxe + qx - dhx * kye - qy);
-            }
-            if ((rf & (R_SRCP | R_SRCM)) && (tf & T_SRCJ)) v += src_term(rf, k);
-            if ((rf & R_XPEC) || (tf & T_JPEC)) v = 0.f;
-            if (!(tf & T_JLT)) v = 0.f;
-            fa[r] = v;
+            const float vn = c0 * v + c1 * (dhy * rc.kxe + px - dhx * kye - py);  // Ez (boundaries.py:196-215)
+            v = (rin && t_jin) ? vn : v;
+            if ((rf & (R_SRCP | R_SRCM)) && t_src) v += src_term(rf, k);
+            fa[r] = ((rf & R_XPEC) || t_zero) ? 0.f : v;
         } else {
             const float hz = fc[r];
-            const float hzl = nb_dn(xb, hz, r);
-            if ((rf & R_HOK) && (tf & T_JLT)) {  // Ex at (i+1/2, j) (boundaries.py:249-258)
-                float e = fa[r];
-                if (lossy) e = e * csj[(r * NC + 2) * NT];
-                if (tf & T_JIN) {
-                    const float d = hz - hzl;
-                    float p = 0.f;
-                    if (tf & T_YE) p = psi_upd(ypc[2 * RS_MAXWY + sje], ypc[3 * RS_MAXWY + sje], yps_e + r * RS_MAXWY + sje, d);
-                    e = e + csj[(r * NC) * NT] * (d * kye + p);
-                }
-                if (tf & T_JPEC) e = 0.f;
-                fa[r] = e;
-            }
-            if (tf & T_HX) {  // Ey at (i, j+1/2) (:259-268)
-                float e = fb[r];
-                if (lossy) e = e * csj[(r * NC + 3) * NT];
-                if (rf & R_IN) {
-                    const float d = hz - hm;
-                    float p = 0.f;
-                    if (rf & R_XE) p = psi_upd(rc.bxe, rc.cxe, xps_e + r * NT + j, d);
-                    e = e + (-csj[(r * NC + 1) * NT]) * (d * rc.kxe + p);
-                }
-                if ((rf & (R_SRCP | R_SRCM)) && (tf & T_SRCJ)) e += src_term(rf, k);
-                if (rf & R_XPEC) e = 0.f;
-                fb[r] = e;
-            }
+            const float d = hz - nb_dn(xb, hz, r), d2 = hz - hm;
+            float *qx = xps_e + r * NT + j, *qy = yqe + r * yse;
+            const float ox = *qx, oy = *qy;
+            const float py = bye * oy + cye * d, px = rc.bxe * ox + rc.cxe * d2;
+            *qy = (rf & R_HOK) ? py : oy;
+            *qx = t_hx ? px : ox;
+            // Ex at (i+1/2, j) (boundaries.py:249-258)
+            float e = fa[r] * (lossy ? csj[(r * NC + 2) * NT] : 1.f);
+            const float en = e + csj[(r * NC) * NT] * (d * kye + py);
+            e = t_jin ? en : e;
+            e = t_jpec ? 0.f : e;
+            fa[r] = ((rf & R_HOK) && t_jlt) ? e : fa[r];
+            // Ey at (i, j+1/2) (:259-268)
+            float e2 = fb[r] * (lossy ? csj[(r * NC + 3) * NT] : 1.f);
+            const float e2n = e2 + (-csj[(r * NC + 1) * NT]) * (d2 * rc.kxe + px);
+            e2 = rin ? e2n : e2;
+            if ((rf & (R_SRCP | R_SRCM)) && t_src) e2 += src_term(rf, k);
+            e2 = (rf & R_XPEC) ? 0.f : e2;
+            fb[r] = t_hx ? e2 : fb[r];
         }
     };
 
@@ -447,8 +487,7 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
             }
         } else {
 #pragma unroll
-            for (int r = 0; r + 1 < RM; ++r)
-                if (r + 1 < R) h_row(r, POL == 0 ? fa[r + 1] : fb[r + 1]);
+            for (int r = 0; r < RM; ++r) h_gen(r);
         }
         // the band's last row: the next band's first E row of the previous step
         float en = 0.f;
@@ -469,7 +508,7 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
                         fc[r] = fc[r] - ch * ((dyx * kx + z) - (dxy * kyh + z));
                     }
                 } else {
-                    h_row(r, en);
+                    h_last(r, en);
                 }
                 if (bf & B_NEXT) put_tag(h_my + hq + (u & 1) * NT, fc[r], (unsigned)(u + 1));
             }
@@ -503,8 +542,7 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
             }
         } else {
 #pragma unroll
-            for (int r = 1; r < RM; ++r)
-                if (r < R) e_row(r, fc[r - 1], k);
+            for (int r = 1; r < RM; ++r) e_row(r, fc[r - 1], k);  // rows past R change nothing
         }
         float hp = 0.f;  // the previous band's last H row of this step
         if ((bf & B_PREV) && !bad && !get_tag(h_prev_h + (u & 1) * NT, (unsigned)(u + 1), err, hp)) bad = true;
@@ -603,8 +641,8 @@ constexpr int RS_RM[RS_NRM] = {8, 11, 12, 14, 16, 20};   // row templates (the w
 
 size_t rs_smem(int rm, int W, int nc) {
     const int NT = 32 * W;
-    return (size_t)(rm * nc * NT + 2 * rm * NT + 2 * rm * RS_MAXWY + 4 * RS_MAXWY + 3 * rm * RS_MAXW) * sizeof(float) +
-           rm * sizeof(RowC) + sizeof(Band);
+    return (size_t)(rm * nc * NT + 2 * rm * NT + 2 * rm * RS_MAXWY + 4 * RS_MAXWY + 3 * rm * RS_MAXW + NT) * sizeof(float) +
+           16 + rm * sizeof(RowC) + sizeof(Band);  // 16: the row constants' alignment
 }
 
 const void *rs_kernel(int rm, bool wide) {

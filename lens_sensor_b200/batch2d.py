@@ -280,6 +280,9 @@ class Group:
         return g
 
 
+RS_PACK_ROWS = 12   # rows per band up to which the resident sweep packs instances into one launch
+
+
 class ResidentGroup:
     """FP32 instances advanced by ONE resident cooperative launch per call
     (lens_rs2d_run): every field value stays in registers from the first step
@@ -316,14 +319,16 @@ class ResidentGroup:
                 self._frames.append(t)
 
     @staticmethod
-    def fits(insts):
-        """True when lens_rs2d_plan places these instances on this device."""
+    def fits(insts, max_rows=None):
+        """True when lens_rs2d_plan places these instances on this device (with
+        at most max_rows rows per band, when given)."""
         n = len(insts)
         if n < 1 or n > N.RS_MAX_INST:
             return False
         host = (N.Inst2D * n)(*[q.s for q in insts])
         r, c, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        return N.load().lens_rs2d_plan(host, n, ctypes.byref(r), ctypes.byref(c), ctypes.byref(t)) == 0
+        ok = N.load().lens_rs2d_plan(host, n, ctypes.byref(r), ctypes.byref(c), ctypes.byref(t)) == 0
+        return ok and (max_rows is None or r.value <= max_rows)
 
     def step(self, tab, n0, nsteps, stream=None):
         N.check(self.lib.lens_rs2d_run(self.host, ctypes.c_void_p(self.dev_desc.data_ptr()), self.out,
@@ -347,10 +352,10 @@ class Sweep:
     resident state per group (None: one group).  autotune() chooses both."""
 
     def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None, tb=False,
-                 chunk=64, resident=False):
+                 chunk=64, resident=False, resident_rows=RS_PACK_ROWS):
         dev = self.dev = E._device(device)
         self.tb, self.chunk = bool(tb), int(chunk)
-        self.resident = bool(resident)
+        self.resident, self.resident_rows = bool(resident), resident_rows
         if self.resident and (self.tb or storage != 'f32'):
             raise ValueError('the resident sweep keeps FP32 state on chip: storage f32, tb False')
         if self.tb and int(steps) % (2 * N.TB_K):
@@ -391,12 +396,13 @@ class Sweep:
 
     def _resident_groups(self):
         """Instances packed into resident launches in order of height (similar
-        column counts share a launch's threads), each launch as full as the
-        chip holds."""
+        column counts share a launch's threads): an instance joins the current
+        launch while the launch's bands stay within resident_rows rows (longer
+        bands cost more per row than they save in waits)."""
         order = sorted(self.insts, key=lambda q: (q.spec.ny, q.spec.nx))
         groups, cur = [], []
         for q in order:
-            if cur and not ResidentGroup.fits(cur + [q]):
+            if cur and not ResidentGroup.fits(cur + [q], self.resident_rows):
                 groups.append(cur)
                 cur = []
             cur.append(q)

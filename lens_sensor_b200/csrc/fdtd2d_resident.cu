@@ -22,9 +22,9 @@
 // order (a band's E(n) needs the previous band's H(n), which needed this band's
 // E(n-1)) keeps a slot from being rewritten before its reader is done with it.
 //
-// Bands clear of every CPML strip, source row and domain face, and warps whose
-// columns are clear of the y strips and faces, run lean rows (no per-cell
-// tests); the others run the general rows.  The per-cell arithmetic is term for
+// Bands clear of the x CPML strips, the source rows and the x faces run lean
+// rows (the y strip and face terms by selects, no branch); the others run the
+// general rows.  The per-cell arithmetic is term for
 // term that of the batched kernels (fdtd2d_batch.cu, after
 // planar_beads/boundaries.py:164-274, source vcsel.py:151-156, loss
 // fdtd2d_core.py:796-797, TM nodes fdtd2d_core.py:458-465).  The band's
@@ -47,10 +47,12 @@ constexpr int RS_MAXWY = 64;                 // psi strip width of one y stagger
 constexpr long long RS_TRIES = 1LL << 22;    // polls per wait (each an L2 round trip, >= 0.3 us)
 constexpr unsigned FULL = 0xffffffffu;
 
+constexpr int RS_MAXCTA = 512;                // bands per launch
 struct RPlan {
-    int ninst, rows, nc;              // rows per band; coefficients per row held in shared memory
+    int ninst, rows, nc;              // most rows of a band; coefficients per row held in shared memory
     int first[LENS_RS_MAX_INST + 1];  // first CTA of instance q; first[ninst] = grid
     LensRsOut2D out[LENS_RS_MAX_INST];
+    short lo[RS_MAXCTA];              // first row of each band (a band ends where the instance's next begins)
 };
 
 // Row flags (RowC.flags): the row exists in the band, i < nx-1 (TE Hy / TM Hz
@@ -61,7 +63,6 @@ constexpr unsigned R_LEAN = R_REAL | R_HOK | R_IN;
 // Thread flags: j < ny-1, j < ny, 0 < j < ny-1, psi of a y strip (H / E), PEC y
 // face, source column (j < src.nj).
 enum : unsigned { T_HX = 1u, T_JLT = 2u, T_JIN = 4u, T_YH = 8u, T_YE = 16u, T_JPEC = 32u, T_SRCJ = 64u };
-constexpr unsigned T_LEAN_MASK = T_HX | T_JLT | T_JIN | T_YH | T_YE | T_JPEC, T_LEAN = T_HX | T_JLT | T_JIN;
 // Band flags
 enum : unsigned { B_PREV = 1u, B_NEXT = 2u, B_LOSSY = 4u, B_KAHAN = 8u };
 
@@ -138,7 +139,7 @@ __device__ __forceinline__ void band_setup(const LensInst2D *gp, const RPlan &pl
                                            RowC *rowc, float *ypc, float *cs) {
     const int lane = threadIdx.x, w = threadIdx.y;
     const int nx = gp->nx, ny = gp->ny, P = gp->pitch;
-    const int lo = (cta - pl.first[q]) * pl.rows, hi = min(nx, lo + pl.rows);
+    const int lo = pl.lo[cta], hi = cta + 1 < pl.first[q + 1] ? pl.lo[cta + 1] : nx;
     const int six = gp->src.ix;
     const bool lossy = POL == 1 && gp->c[2] != nullptr;
     if (w == 0 && lane == 0) {
@@ -293,9 +294,8 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         const unsigned f = rowc[r].flags;
         if (f & R_REAL) band_lean = band_lean && f == R_LEAN;
     }
-    // a warp of a lean band whose columns are all interior and clear of the y strips
-    // runs the lean rows (no per-cell tests); lean warps are never the first or last
-    const bool lean = band_lean && __all_sync(FULL, (tf & T_LEAN_MASK) == T_LEAN);
+    // every warp of a band clear of x strips, source rows and x faces runs the lean rows
+    const bool lean = band_lean;
     const float *csj = cs + j;
 
     // ---- state in: fields (registers), psi strips (shared memory)
@@ -408,6 +408,79 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
             fc[r] = on ? hz : fc[r];
         }
     };
+    // Rows of a band clear of x strips, source rows and x faces (every real row
+    // R_LEAN), any warp: the lean arithmetic plus the y-strip psi through the
+    // thread's psi slots (zero outside the strips) and the column selects.
+    auto h_lean = [&](int r) {  // every row: TE Hx; rows below the band's last: Hy / Hz
+        const float kx = rowc[r].kxh;
+        const bool below = r + 1 < R;
+        float *qy = yqh + r * ysh;
+        const float oy = *qy;
+        if (POL == 0) {
+            const float ez = fa[r];
+            const float d = nb_up(ez, r) - ez;
+            const float py = byh * oy + cyh * d;
+            *qy = py;
+            const float hx = fb[r] - ch * (d * kyh + py);
+            fb[r] = t_hx ? hx : fb[r];
+            if (r + 1 < RM) {
+                const float hy = fc[r] + ch * ((fa[r + 1] - ez) * kx + z);
+                fc[r] = (below && t_jlt) ? hy : fc[r];
+            }
+        } else if (r + 1 < RM) {
+            const float ex = fa[r];
+            const float dyx = fb[r + 1] - fb[r], dxy = nb_up(ex, r) - ex;
+            const bool on = below && t_hx;
+            const float py = byh * oy + cyh * dxy;
+            *qy = on ? py : oy;
+            const float hz = fc[r] - ch * ((dyx * kx + z) - (dxy * kyh + py));
+            fc[r] = on ? hz : fc[r];
+        }
+    };
+    auto h_lean_last = [&](int r, float en) {  // the band's last row from the next band's first E row
+        const float kx = rowc[r].kxh;
+        if (POL == 0) {
+            const float hy = fc[r] + ch * ((en - fa[r]) * kx + z);
+            fc[r] = t_jlt ? hy : fc[r];
+        } else {
+            float *qy = yqh + r * ysh;
+            const float oy = *qy;
+            const float ex = fa[r];
+            const float dyx = en - fb[r], dxy = nb_up(ex, r) - ex;
+            const float py = byh * oy + cyh * dxy;
+            *qy = t_hx ? py : oy;
+            const float hz = fc[r] - ch * ((dyx * kx + z) - (dxy * kyh + py));
+            fc[r] = t_hx ? hz : fc[r];
+        }
+    };
+    auto e_lean = [&](int r, float hm) {  // hm: the H field of row i-1 (TE Hy, TM Hz)
+        const float kx = rowc[r].kxe;
+        float *qy = yqe + r * yse;
+        const float oy = *qy;
+        if (POL == 0) {
+            const float hx = fb[r];
+            const float dhy = fc[r] - hm, dhx = hx - nb_dn(xb, hx, r);
+            const float py = bye * oy + cye * dhx;
+            *qy = py;
+            const float c0 = csj[(r * NC) * NT], c1 = csj[(r * NC + 1) * NT];
+            const float vn = c0 * fa[r] + c1 * (dhy * kx + z - dhx * kye - py);
+            const float v = t_jin ? vn : fa[r];
+            fa[r] = t_zero ? 0.f : v;
+        } else {
+            const float hz = fc[r];
+            const float d = hz - nb_dn(xb, hz, r), d2 = hz - hm;
+            const float py = bye * oy + cye * d;
+            *qy = py;
+            float e = fa[r] * (lossy ? csj[(r * NC + 2) * NT] : 1.f);
+            const float en = e + csj[(r * NC) * NT] * (d * kye + py);
+            e = t_jin ? en : e;
+            e = t_jpec ? 0.f : e;
+            fa[r] = t_jlt ? e : fa[r];
+            const float e2 = fb[r] * (lossy ? csj[(r * NC + 3) * NT] : 1.f);
+            const float e2n = e2 + (-csj[(r * NC + 1) * NT]) * (d2 * kx + z);
+            fb[r] = t_hx ? e2n : fb[r];
+        }
+    };
     // source term of row flags rf at table row k (vcsel.py:151-156)
     auto src_term = [&](unsigned rf, int k) {
         const float s = (__ldg(tab.env + k) * sinf(__ldg(tab.wt + k) + __ldg(((rf & R_SRCP) ? B.ph1 : B.ph2) + j))) *
@@ -462,32 +535,13 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         const int m = n0 + u - B.n_start;  // the instance's own step
         const int k = m - tab.t0;
         // ------------------------------------------------------------ H phase
-        if (lean) {  // every row below the band's last: no tests, no psi
+        if (lean) {
 #pragma unroll
-            for (int r = 0; r + 1 < RM; ++r) {
-                const float kx = rowc[r].kxh;
-                if (POL == 0) {
-                    const float ez = fa[r];
-                    const float d = nb_up(ez, r) - ez;
-                    fb[r] = fb[r] - ch * (d * kyh + z);
-                    const float d2 = fa[r + 1] - ez;
-                    const float hy = fc[r] + ch * (d2 * kx + z);
-                    fc[r] = r + 1 < R ? hy : fc[r];
-                } else {
-                    const float ex = fa[r];
-                    const float dyx = fb[r + 1] - fb[r], dxy = nb_up(ex, r) - ex;
-                    const float hz = fc[r] - ch * ((dyx * kx + z) - (dxy * kyh + z));
-                    fc[r] = r + 1 < R ? hz : fc[r];
-                }
-            }
-            if (POL == 0) {  // Hx of the template's last row (a row past R is never read)
-                const float ez = fa[RM - 1];
-                const float d = nb_up(ez, RM - 1) - ez;
-                fb[RM - 1] = fb[RM - 1] - ch * (d * kyh + z);
-            }
+            for (int r = 0; r < RM; ++r) h_lean(r);
         } else {
 #pragma unroll
-            for (int r = 0; r < RM; ++r) h_gen(r);
+            for (int r = 0; r < RM; ++r)
+                if (r < R) h_gen(r);  // short bands (x strips, source rows) skip the template's spare rows
         }
         // the band's last row: the next band's first E row of the previous step
         float en = 0.f;
@@ -498,18 +552,8 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
 #pragma unroll
         for (int r = 0; r < RM; ++r) {
             if (r == R - 1) {
-                if (lean) {  // Hx was updated above (TE); Hy / Hz from the halo row
-                    const float kx = rowc[r].kxh;
-                    if (POL == 0) {
-                        fc[r] = fc[r] + ch * ((en - fa[r]) * kx + z);
-                    } else {
-                        const float ex = fa[r];
-                        const float dyx = en - fb[r], dxy = nb_up(ex, r) - ex;
-                        fc[r] = fc[r] - ch * ((dyx * kx + z) - (dxy * kyh + z));
-                    }
-                } else {
-                    h_last(r, en);
-                }
+                if (lean) h_lean_last(r, en);
+                else h_last(r, en);
                 if (bf & B_NEXT) put_tag(h_my + hq + (u & 1) * NT, fc[r], (unsigned)(u + 1));
             }
         }
@@ -521,51 +565,16 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         // ------------------------------------------------------------ E phase
         if (lean) {  // rows 1.. (row 0 after the previous band's H row)
 #pragma unroll
-            for (int r = 1; r < RM; ++r) {
-                const float kx = rowc[r].kxe;
-                if (POL == 0) {
-                    const float hx = fb[r];
-                    const float dhy = fc[r] - fc[r - 1], dhx = hx - nb_dn(xb, hx, r);
-                    const float c0 = csj[(r * NC) * NT], c1 = csj[(r * NC + 1) * NT];
-                    fa[r] = c0 * fa[r] + c1 * (dhy * kx + z - dhx * kye - z);
-                } else {
-                    const float hz = fc[r];
-                    const float d = hz - nb_dn(xb, hz, r), d2 = hz - fc[r - 1];
-                    float e = fa[r], e2 = fb[r];
-                    if (lossy) {
-                        e = e * csj[(r * NC + 2) * NT];
-                        e2 = e2 * csj[(r * NC + 3) * NT];
-                    }
-                    fa[r] = e + csj[(r * NC) * NT] * (d * kye + z);
-                    fb[r] = e2 + (-csj[(r * NC + 1) * NT]) * (d2 * kx + z);
-                }
-            }
+            for (int r = 1; r < RM; ++r) e_lean(r, fc[r - 1]);
         } else {
 #pragma unroll
-            for (int r = 1; r < RM; ++r) e_row(r, fc[r - 1], k);  // rows past R change nothing
+            for (int r = 1; r < RM; ++r)
+                if (r < R) e_row(r, fc[r - 1], k);
         }
         float hp = 0.f;  // the previous band's last H row of this step
         if ((bf & B_PREV) && !bad && !get_tag(h_prev_h + (u & 1) * NT, (unsigned)(u + 1), err, hp)) bad = true;
-        if (lean) {
-            const float kx = rowc[0].kxe;
-            if (POL == 0) {
-                const float hx = fb[0];
-                const float dhy = fc[0] - hp, dhx = hx - nb_dn(xb, hx, 0);
-                fa[0] = csj[0] * fa[0] + csj[NT] * (dhy * kx + z - dhx * kye - z);
-            } else {
-                const float hz = fc[0];
-                const float d = hz - nb_dn(xb, hz, 0), d2 = hz - hp;
-                float e = fa[0], e2 = fb[0];
-                if (lossy) {
-                    e = e * csj[2 * NT];
-                    e2 = e2 * csj[3 * NT];
-                }
-                fa[0] = e + csj[0] * (d * kye + z);
-                fb[0] = e2 + (-csj[NT]) * (d2 * kx + z);
-            }
-        } else {
-            e_row(0, hp, k);
-        }
+        if (lean) e_lean(0, hp);
+        else e_row(0, hp, k);
         if (bf & B_PREV) put_tag(h_my + (u & 1) * NT, POL == 0 ? fa[0] : fb[0], (unsigned)(u + 1));
         const bool win = B.dft && m >= B.dft_n0 && m < B.dft_n1;
         if (POL == 0 && win && (tf & T_JLT)) {  // node DFT of Ez
@@ -680,17 +689,53 @@ bool rs_inst_ok(const LensInst2D &g) {
     return true;
 }
 
-// Plan of a resident group on this device: the row template RM, rows per band,
-// warps per CTA, the CTA count and the coefficients per row.  LENS_ERR_SIZE when
-// the group does not fit.
-int rs_plan(const LensInst2D *inst, int ninst, int &rm, int &rows, int &W, int &nctas, int &nc) {
+// Relative cost of a row: lean bands run the lean rows, a band holding any x
+// strip, source or face row runs the general rows, so such bands get fewer
+// rows.  3.4 is the ratio that gave the fastest step on the B200 (config 0:
+// 4.26 us per step at 1.6, 3.79 at 2.4, 3.29 at 3.4 and at 4.0); it also
+// covers a band's fixed costs (two barriers, two halo exchanges per step).
+constexpr int RS_COST_LEAN = 10, RS_COST_SPECIAL = 34;
+
+bool row_special(const LensInst2D &g, int i) {
+    if (i <= 0 || i >= g.nx - 1) return true;  // faces (and the row without Hy / Hz)
+    if (g.src.ix >= 0 && (i == g.src.ix || i == g.src.ix + 1)) return true;
+    const LensProfile &h = g.ax.h, &e = g.ax.e;
+    return i < h.lo || i >= h.n - h.hi || i < e.lo || i >= e.n - e.hi;  // in an x strip (H or E psi)
+}
+
+// Bands of instance g with cost at most T and at most rmx rows each (greedy:
+// every band as long as it may be); their first rows into lo (when not NULL).
+int rs_bands(const LensInst2D &g, int T, int rmx, short *lo) {
+    int n = 0;
+    for (int i = 0; i < g.nx;) {
+        int r = 0;
+        bool sp = false;
+        while (i + r < g.nx && r < rmx) {
+            const bool sp2 = sp || row_special(g, i + r);
+            if (r > 0 && (r + 1) * (sp2 ? RS_COST_SPECIAL : RS_COST_LEAN) > T) break;
+            sp = sp2;
+            ++r;
+        }
+        if (lo) lo[n] = (short)i;
+        ++n;
+        i += r;
+    }
+    return n;
+}
+
+// Plan of a resident group on this device: the row template RM, the most rows of
+// a band, warps per CTA, the CTA count, the coefficients per row and (when lo is
+// not NULL) the first row of every band, instance after instance.  The bands
+// minimise the largest band cost within the SMs' resident CTAs.  LENS_ERR_SIZE
+// when the group does not fit.
+int rs_plan(const LensInst2D *inst, int ninst, int &rm, int &rows, int &W, int &nctas, int &nc, short *lo) {
     if (!inst || ninst < 1 || ninst > LENS_RS_MAX_INST) return ninst > LENS_RS_MAX_INST ? LENS_ERR_SIZE : LENS_ERR_ARG;
     int ny_max = 0;
     nc = 2;
     for (int q = 0; q < ninst; ++q) {
         if (!rs_inst_ok(inst[q])) return LENS_ERR_ARG;
         const LensInst2D &g = inst[q];
-        if (g.ay.e.lo + g.ay.e.hi > RS_MAXWY || g.ay.h.lo + g.ay.h.hi > RS_MAXWY) return LENS_ERR_SIZE;
+        if (g.ay.e.lo + g.ay.e.hi > RS_MAXWY || g.ay.h.lo + g.ay.h.hi > RS_MAXWY || g.nx > 32767) return LENS_ERR_SIZE;
         ny_max = std::max(ny_max, g.ny);
         if (g.pol == 1 && g.c[2]) nc = 4;
     }
@@ -700,43 +745,58 @@ int rs_plan(const LensInst2D *inst, int ninst, int &rm, int &rows, int &W, int &
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         return LENS_ERR_CUDA;
-    // the fewest rows per band whose bands all fit; the smallest row template
-    // that holds them (rows past a band's end are computed and discarded)
     const bool wide = 32 * W > RS_NT_NARROW;
-    long avail[RS_NRM];
+    auto count = [&](int T, int rmx) {
+        long n = 0;
+        for (int q = 0; q < ninst; ++q) n += rs_bands(inst[q], T, rmx, nullptr);
+        return n;
+    };
+    int best_t = -1, best_rm = 0;
     for (int t = 0; t < RS_NRM; ++t) {
-        avail[t] = 0;
-        const void *k = rs_kernel(RS_RM[t], wide);
-        const size_t sm = rs_smem(RS_RM[t], W, nc);
+        const int cand = RS_RM[t];
+        const void *k = rs_kernel(cand, wide);
+        const size_t sm = rs_smem(cand, W, nc);
         if (!k || sm > (size_t)smax) continue;
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
             return LENS_ERR_CUDA;
         int per = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 32 * W, sm) != cudaSuccess) return LENS_ERR_CUDA;
-        avail[t] = (long)per * nsm;
-    }
-    for (int r = 1; r <= RS_RM[RS_NRM - 1]; ++r) {
-        long need = 0;
-        for (int q = 0; q < ninst; ++q) need += (inst[q].nx + r - 1) / r;
-        for (int t = 0; t < RS_NRM; ++t) {
-            if (RS_RM[t] < r || !rs_kernel(RS_RM[t], wide)) continue;
-            if (need <= avail[t]) {
-                rm = RS_RM[t];
-                rows = r;
-                nctas = (int)need;
-                return LENS_OK;
-            }
-            break;  // the smallest template holding r rows decides
+        const long avail = std::min((long)per * nsm, (long)RS_MAXCTA);
+        int hi_t = cand * RS_COST_SPECIAL;  // every band at most `cand` rows
+        if (avail < 1 || count(hi_t, cand) > avail) continue;
+        int lo_t = RS_COST_LEAN - 1;         // infeasible: one lean row per band is the least
+        while (hi_t - lo_t > 1) {
+            const int mid = (lo_t + hi_t) / 2;
+            if (count(mid, cand) <= avail) hi_t = mid;
+            else lo_t = mid;
+        }
+        if (best_t < 0 || hi_t < best_t) {
+            best_t = hi_t;
+            best_rm = cand;
         }
     }
-    return LENS_ERR_SIZE;
+    if (best_t < 0) return LENS_ERR_SIZE;
+    rm = best_rm;
+    nctas = 0;
+    rows = 0;
+    for (int q = 0; q < ninst; ++q) {
+        short tmp[RS_MAXCTA];
+        const int n = rs_bands(inst[q], best_t, rm, tmp);
+        for (int b = 0; b < n; ++b) {
+            const int end = b + 1 < n ? tmp[b + 1] : inst[q].nx;
+            rows = std::max(rows, end - tmp[b]);
+            if (lo) lo[nctas + b] = tmp[b];
+        }
+        nctas += n;
+    }
+    return LENS_OK;
 }
 
 }  // namespace
 
 extern "C" int lens_rs2d_plan(const LensInst2D *inst, int ninst, int *rows, int *ctas, int *threads) {
     int rm = 0, r = 0, W = 0, n = 0, nc = 0;
-    const int st = rs_plan(inst, ninst, rm, r, W, n, nc);
+    const int st = rs_plan(inst, ninst, rm, r, W, n, nc, nullptr);
     if (st != LENS_OK) {
         cudaGetLastError();
         return st;
@@ -757,7 +817,8 @@ extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst
                              size_t scratch_bytes, int *err, void *stream) {
     if (!inst_host || !inst_dev || !scratch || !err || nsteps < 0) return LENS_ERR_ARG;
     int rm = 0, rows = 0, W = 0, nctas = 0, nc = 0;
-    int st = rs_plan(inst_host, ninst, rm, rows, W, nctas, nc);
+    RPlan pl{};
+    int st = rs_plan(inst_host, ninst, rm, rows, W, nctas, nc, pl.lo);
     if (st != LENS_OK) {
         cudaGetLastError();
         return st;
@@ -778,14 +839,13 @@ extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst
         cudaGetLastError();
         return LENS_ERR_CUDA;
     }
-    RPlan pl{};
     pl.ninst = ninst;
     pl.rows = rows;
     pl.nc = nc;
     int c = 0;
     for (int q = 0; q < ninst; ++q) {
         pl.first[q] = c;
-        c += (inst_host[q].nx + rows - 1) / rows;
+        while (c < nctas && (c == pl.first[q] || pl.lo[c] != 0)) ++c;  // the next instance's bands start at row 0
         pl.out[q] = out ? out[q] : LensRsOut2D{nullptr, 0, 0, 0};
     }
     pl.first[ninst] = c;

@@ -426,8 +426,10 @@ def run_batched(plain_sample=16, count=256):
     torch.cuda.synchronize()
     t_res = e0.elapsed_time(e1) * 1e-3
     res_r = sr.results()
-    res_err = [float((r['phasor'] - ref[q]).abs().norm() / max(float(ref[q].abs().norm()), 1e-300))
-               for q, r in enumerate(res_r)]
+    res_err = []
+    for q, r in enumerate(res_r):   # on the host: relative L2 difference, NaN where non-finite
+        x, y = r['phasor'].cpu().numpy(), ref[q].cpu().numpy()
+        res_err.append(float(np.linalg.norm((x - y).ravel()) / max(float(np.linalg.norm(y.ravel())), 1e-300)))
     res_groups = [dict(instances=len(g.insts), rows=g.rows, ctas=g.ctas, threads=g.threads) for g in sr.groups]
     res_ph = [r['phasor'] for r in res_r]
     del sr, res_r
@@ -494,7 +496,8 @@ def run_batched(plain_sample=16, count=256):
                 plain_resident_sample='the same instances one at a time, each in one resident launch '
                                       '(lens_rs2d_run, fields in registers for the whole solve)',
                 batched_resident_f32=res, resident_vs_plain=res / plain, resident_vs_plain_resident=res / plain_resident,
-                resident_launches=res_groups, resident_phasor_err_vs_batched_f32_max=max(res_err),
+                resident_launches=res_groups, resident_phasor_err_vs_batched_f32_max=float(np.nanmax(res_err)),
+                resident_phasor_nonfinite=int(np.sum(~np.isfinite(res_err))),
                 tile=f'128 x {2 * by} nodes', group_budget_bytes=budget, autotune=tuned, graph_launches=launches,
                 f16_phasor_err_vs_f32_max=max(err), f16_phasor_err_vs_f32_median=float(np.median(err)),
                 K_median=float(np.median(K)), err_vs_fp64=fp64, f16_gate=gate)

@@ -44,7 +44,8 @@ class Solve2D:
     engine='persistent': the batched kernels on this one instance in one
     persistent cooperative launch per snapshot period (lens_batch2d_run, the
     grid kept on chip across steps, no launch gaps);
-    engine='batch' (default): the batched kernels on this one instance
+    engine=None (default): 'resident' when the grid fits the chip, else 'batch';
+    engine='batch': the batched kernels on this one instance
     (lens_batch2d_step, vector passes over 128 x 2*by tiles; capture() records
     the whole schedule, snapshots included, as one CUDA graph that run()
     replays); engine='tb': the temporally blocked step (lens_tb2d_step,
@@ -53,7 +54,7 @@ class Solve2D:
     single-grid engine (lens_te2d_step / lens_tm2d_step), one step per launch
     pair, with the full single-grid epilogue set."""
 
-    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None, engine='batch',
+    def __init__(self, spec: Spec2D, steps_total, periods=1, snap_every=200, device=None, geo=None, engine=None,
                  chunk=16, by=4):
         self.spec = sp = spec
         self.steps_total = int(steps_total)
@@ -68,12 +69,18 @@ class Solve2D:
             sum(np.asarray(g['src'][k]).nbytes for k in ('amp', 'ph1', 'ph2'))
         self.table = E.StepTable(0, self.steps_total, sp.dt, g['src']['omega'], self.omega,
                                  E.cw_envelope(sp.f0, sp.ramp_periods), device=device)
+        probe = None
+        if engine is None:   # the resident launch when the grid fits the chip
+            from . import batch2d as B
+            probe = B.Instance(sp, self.steps_total, torch.float32, E._device(device), g, kahan=True, window=self.dft)
+            engine = 'resident' if B.ResidentGroup.fits([probe]) else 'batch'
         self.engine = engine
         self.graph = None
         if engine == 'resident':
             from . import batch2d as B
             dev = E._device(device)
-            self.inst = B.Instance(sp, self.steps_total, torch.float32, dev, g, kahan=True, window=self.dft)
+            self.inst = probe if probe is not None else \
+                B.Instance(sp, self.steps_total, torch.float32, dev, g, kahan=True, window=self.dft)
             self.grid = self.epi = None
             shape = (sp.nx, sp.ny) if sp.pol == 's' else (sp.nx, sp.ny - 1)
             self.snaps = torch.zeros((len(self.snap_steps),) + shape, dtype=torch.float32, device=dev)

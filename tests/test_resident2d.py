@@ -181,3 +181,16 @@ def test_config0_resident_matches_batch_engine():
         assert np.abs(sb[q] - sa[q]).max() <= TOL * max(np.abs(sa[q]).max(), 1e-30), q
     e = np.linalg.norm(pb - pa) / np.linalg.norm(pa)
     assert e <= 1e-5, e
+
+
+@pytest.mark.gpu
+def test_solve2d_default_engine():
+    """Solve2D picks the resident launch when the grid fits the chip and the
+    batched launches when it does not (ny > 576 columns)."""
+    from lens_sensor_b200.solver2d import Solve2D
+    sp = _specs(1)[0]
+    assert Solve2D(sp, 40).engine == 'resident'
+    wide = replace(sp, ny=600)
+    s = Solve2D(wide, 40)
+    assert s.engine == 'batch'
+    s.capture().run()

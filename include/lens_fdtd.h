@@ -337,6 +337,16 @@ int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const
                   const LensStepTable *tab, int n0, int nsteps, void *scratch, size_t scratch_bytes, int *err,
                   void *stream);
 
+/* Watchdog self-test of the waits between bands (no counterpart in the
+ * reference): lens_rs2d_run's launch with every wait cut to 1024 polls and the
+ * second band of the first instance withholding its first E row of step 1.
+ * The first band's wait at step 2 runs out, *err becomes nonzero and every CTA
+ * leaves its step loop (no fault, no hang).  Needs a first instance of two or
+ * more bands and nsteps >= 3; the fields are left invalid.                   */
+int lens_rs2d_watchdog_test(const LensInst2D *inst_host, const LensInst2D *inst_dev, int ninst,
+                            const LensStepTable *tab, int n0, int nsteps, void *scratch, size_t scratch_bytes,
+                            int *err, void *stream);
+
 /* ---------------------------------------------------------------- 3D grid */
 /* psi arrays of the 3D CPML (boundaries3d.py:286-302), in this order.  Each is a
  * full (nx, ny, pitch) volume like the fields, so a CTA stages psi with the same

@@ -160,6 +160,8 @@ SIGNATURES = {
     'lens_rs2d_scratch_bytes': (ctypes.c_size_t, [c_int, c_int]),
     'lens_rs2d_run': (c_int, [POINTER(Inst2D), c_void_p, POINTER(RsOut2D), c_int, POINTER(StepTable), c_int, c_int,
                               c_void_p, ctypes.c_size_t, c_void_p, c_void_p]),
+    'lens_rs2d_watchdog_test': (c_int, [POINTER(Inst2D), c_void_p, c_int, POINTER(StepTable), c_int, c_int,
+                                        c_void_p, ctypes.c_size_t, c_void_p, c_void_p]),
     'lens_version': (c_int, []),
     'lens_status_string': (ctypes.c_char_p, [c_int]),
     'lens_abi_sizes': (c_int, [POINTER(c_int), c_int]),

@@ -53,6 +53,8 @@ struct RPlan {
     int first[LENS_RS_MAX_INST + 1];  // first CTA of instance q; first[ninst] = grid
     LensRsOut2D out[LENS_RS_MAX_INST];
     short lo[RS_MAXCTA];              // first row of each band (a band ends where the instance's next begins)
+    long long tries;                  // polls per wait
+    int wd_cta;                       // watchdog self-test: this band withholds its E row of step 1 (-1: none)
 };
 
 // Row flags (RowC.flags): the row exists in the band, i < nx-1 (TE Hy / TM Hz
@@ -92,7 +94,8 @@ __device__ __forceinline__ void put_tag(unsigned long long *p, float v, unsigned
 
 // Value of the word at p once its tag is `tag`; false if the wait ran out or
 // another CTA reported an error.
-__device__ __forceinline__ bool get_tag(const unsigned long long *p, unsigned tag, const int *err, float &v) {
+__device__ __forceinline__ bool get_tag(const unsigned long long *p, unsigned tag, const int *err, float &v,
+                                        long long tries) {
     for (long long t = 0;; ++t) {
         unsigned long long w;
         asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
@@ -100,7 +103,7 @@ __device__ __forceinline__ bool get_tag(const unsigned long long *p, unsigned ta
             v = __uint_as_float((unsigned)w);
             return true;
         }
-        if (t >= RS_TRIES) return false;
+        if (t >= tries) return false;
         if ((t & 255) == 255 && *reinterpret_cast<const volatile int *>(err)) return false;
     }
 }
@@ -547,7 +550,7 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         float en = 0.f;
         if (bf & B_NEXT) {
             if (u == 0) en = e_next0;
-            else if (!bad && !get_tag(h_next_e + ((u - 1) & 1) * NT, (unsigned)u, err, en)) bad = true;
+            else if (!bad && !get_tag(h_next_e + ((u - 1) & 1) * NT, (unsigned)u, err, en, pl.tries)) bad = true;
         }
 #pragma unroll
         for (int r = 0; r < RM; ++r) {
@@ -572,10 +575,11 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
                 if (r < R) e_row(r, fc[r - 1], k);
         }
         float hp = 0.f;  // the previous band's last H row of this step
-        if ((bf & B_PREV) && !bad && !get_tag(h_prev_h + (u & 1) * NT, (unsigned)(u + 1), err, hp)) bad = true;
+        if ((bf & B_PREV) && !bad && !get_tag(h_prev_h + (u & 1) * NT, (unsigned)(u + 1), err, hp, pl.tries)) bad = true;
         if (lean) e_lean(0, hp);
         else e_row(0, hp, k);
-        if (bf & B_PREV) put_tag(h_my + (u & 1) * NT, POL == 0 ? fa[0] : fb[0], (unsigned)(u + 1));
+        if ((bf & B_PREV) && !(cta == pl.wd_cta && u == 1))
+            put_tag(h_my + (u & 1) * NT, POL == 0 ? fa[0] : fb[0], (unsigned)(u + 1));
         const bool win = B.dft && m >= B.dft_n0 && m < B.dft_n1;
         if (POL == 0 && win && (tf & T_JLT)) {  // node DFT of Ez
             const float pr = __ldg(tab.pe + 2 * k), pim = __ldg(tab.pe + 2 * k + 1);
@@ -812,9 +816,11 @@ extern "C" size_t lens_rs2d_scratch_bytes(int ctas, int threads) {
     return (size_t)ctas * 4 * (size_t)threads * sizeof(unsigned long long);
 }
 
-extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const LensRsOut2D *out,
-                             int ninst, const LensStepTable *tab, int n0, int nsteps, void *scratch,
-                             size_t scratch_bytes, int *err, void *stream) {
+namespace {
+
+int rs_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const LensRsOut2D *out, int ninst,
+           const LensStepTable *tab, int n0, int nsteps, void *scratch, size_t scratch_bytes, int *err, void *stream,
+           long long tries, int wd) {
     if (!inst_host || !inst_dev || !scratch || !err || nsteps < 0) return LENS_ERR_ARG;
     int rm = 0, rows = 0, W = 0, nctas = 0, nc = 0;
     RPlan pl{};
@@ -840,6 +846,12 @@ extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst
         return LENS_ERR_CUDA;
     }
     pl.ninst = ninst;
+    pl.tries = tries;
+    pl.wd_cta = -1;
+    if (wd) {  // the second band of the first instance withholds a row: it must exist
+        if (nctas < 2 || nsteps < 3 || inst_host[0].nx <= pl.lo[1]) return LENS_ERR_ARG;
+        pl.wd_cta = 1;
+    }
     pl.rows = rows;
     pl.nc = nc;
     int c = 0;
@@ -863,4 +875,22 @@ extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst
         return LENS_ERR_CUDA;
     }
     return lens_cuda_status();
+}
+
+}  // namespace
+
+extern "C" int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const LensRsOut2D *out,
+                             int ninst, const LensStepTable *tab, int n0, int nsteps, void *scratch,
+                             size_t scratch_bytes, int *err, void *stream) {
+    return rs_run(inst_host, inst_dev, out, ninst, tab, n0, nsteps, scratch, scratch_bytes, err, stream, RS_TRIES, 0);
+}
+
+// Watchdog self-test: the same launch with every wait cut to 1024 polls and the
+// second band of the first instance withholding its first E row of step 1, so
+// the first band's wait at step 2 runs out; *err must become nonzero, every
+// CTA must leave its step loop and the stream stays usable.
+extern "C" int lens_rs2d_watchdog_test(const LensInst2D *inst_host, const LensInst2D *inst_dev, int ninst,
+                                       const LensStepTable *tab, int n0, int nsteps, void *scratch,
+                                       size_t scratch_bytes, int *err, void *stream) {
+    return rs_run(inst_host, inst_dev, nullptr, ninst, tab, n0, nsteps, scratch, scratch_bytes, err, stream, 1024, 1);
 }

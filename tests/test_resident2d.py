@@ -194,3 +194,31 @@ def test_solve2d_default_engine():
     s = Solve2D(wide, 40)
     assert s.engine == 'batch'
     s.capture().run()
+
+
+@pytest.mark.gpu
+def test_watchdog_ends_the_launch():
+    """A band that withholds one halo row (lens_rs2d_watchdog_test): its
+    neighbour's bounded wait runs out, the error word is set, the launch ends,
+    and the next launch on the same buffers runs clean."""
+    import time
+    import torch
+    from lens_sensor_b200 import batch2d as B
+    sw = B.Sweep(_specs(2), 60, 'f32', resident=True)
+    g = sw.groups[0]
+    assert g.ctas >= 2
+    lib = N.load()
+    t0 = time.perf_counter()
+    st = lib.lens_rs2d_watchdog_test(g.host, ctypes.c_void_p(g.dev_desc.data_ptr()), len(g.insts),
+                                     ctypes.byref(sw.table.s), 0, 20, ctypes.c_void_p(g.scratch.data_ptr()),
+                                     g.scratch.numel(), ctypes.c_void_p(g.err.data_ptr()), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert time.perf_counter() - t0 < 30
+    assert int(g.err.item()) != 0
+    with pytest.raises(N.LensError):
+        g.check()
+    sw.reset()
+    g.step(sw.table, 0, 20)
+    torch.cuda.synchronize()
+    g.check()

@@ -62,9 +62,10 @@ struct RPlan {
 // x face, psi of an x strip (H / E).
 enum : unsigned { R_REAL = 1u, R_HOK = 2u, R_IN = 4u, R_SRCP = 8u, R_SRCM = 16u, R_XPEC = 32u, R_XH = 64u, R_XE = 128u };
 constexpr unsigned R_LEAN = R_REAL | R_HOK | R_IN;
-// Thread flags: j < ny-1, j < ny, 0 < j < ny-1, psi of a y strip (H / E), PEC y
-// face, source column (j < src.nj).
-enum : unsigned { T_HX = 1u, T_JLT = 2u, T_JIN = 4u, T_YH = 8u, T_YE = 16u, T_JPEC = 32u, T_SRCJ = 64u };
+// Thread flags: j < ny-1, j < ny, 0 < j < ny-1, PEC y face, source column
+// (j < src.nj).  The y-strip psi needs no flag: outside the strips a column's
+// psi slot is a zero slot with b = c = 0.
+enum : unsigned { T_HX = 1u, T_JLT = 2u, T_JIN = 4u, T_JPEC = 32u, T_SRCJ = 64u };
 // Band flags
 enum : unsigned { B_PREV = 1u, B_NEXT = 2u, B_LOSSY = 4u, B_KAHAN = 8u };
 
@@ -126,13 +127,6 @@ __device__ __forceinline__ void dft_add(float *dft, bool kahan, size_t o, float 
         s.y += v * pim;
         *a = s;
     }
-}
-
-// psi = b*psi + c*d (stored); returns the new psi (the batched kernels' psi_step).
-__device__ __forceinline__ float psi_upd(float b, float c, float *q, float d) {
-    const float p = b * (*q) + c * d;
-    *q = p;
-    return p;
 }
 
 // Band constants, row constants and the band's coefficient rows of CTA `cta`
@@ -287,8 +281,6 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
     if (j < ny - 1) tf |= T_HX;
     if (j < ny) tf |= T_JLT;
     if (j > 0 && j < ny - 1) tf |= T_JIN;
-    if (sjh >= 0) tf |= T_YH;
-    if (sje >= 0) tf |= T_YE;
     if ((gp->pec[2] && j == 0) || (gp->pec[3] && j == ny - 1)) tf |= T_JPEC;
     if (j < B.snj) tf |= T_SRCJ;
     bool band_lean = true;
@@ -344,8 +336,8 @@ __device__ __forceinline__ void rs_band(const LensInst2D *__restrict__ insts, co
         return u;
     };
     // thread tests, as booleans
-    const bool t_hx = tf & T_HX, t_jlt = tf & T_JLT, t_jin = tf & T_JIN, t_yh = tf & T_YH, t_ye = tf & T_YE,
-               t_zero = (tf & T_JPEC) || !(tf & T_JLT), t_jpec = tf & T_JPEC, t_src = tf & T_SRCJ;
+    const bool t_hx = tf & T_HX, t_jlt = tf & T_JLT, t_jin = tf & T_JIN, t_zero = (tf & T_JPEC) || !(tf & T_JLT),
+               t_jpec = tf & T_JPEC, t_src = tf & T_SRCJ;
     // The general rows evaluate every update and keep it where it applies
     // (selects): psi slots exist for every row and column (zero outside the
     // strips, with b = c = 0 there), so no psi term is a branch and the

@@ -280,7 +280,9 @@ class Group:
         return g
 
 
-RS_PACK_ROWS = 12   # rows per band up to which the resident sweep packs instances into one launch
+# rows per band up to which the resident sweep packs instances into one launch: on
+# the 256-instance sweep (B200) 170 G cell-updates/s at 12, 174 G at 16, 156 G at 20
+RS_PACK_ROWS = 16
 
 
 class ResidentGroup:

@@ -326,6 +326,14 @@ typedef struct {
  * more than LENS_RS_MAX_INST instances).                                     */
 int lens_rs2d_plan(const LensInst2D *inst, int ninst, int *rows, int *ctas, int *threads);
 
+/* The plan's band partition, host only (no device is touched): the instances'
+ * rows cut into at most `ctas` bands of at most max_rows rows, a row of an x
+ * CPML strip, a source row or a face row costing 3.4 rows elsewhere, the
+ * largest band cost as small as it can be.  Writes the first row of every band,
+ * instance after instance, into first_rows (capacity entries) and returns the
+ * band count; LENS_ERR_SIZE when the rows do not fit.                        */
+int lens_rs2d_bands(const LensInst2D *inst, int ninst, int ctas, int max_rows, short *first_rows, int capacity);
+
 /* Bytes of the halo scratch of a plan (device memory, the caller's).        */
 size_t lens_rs2d_scratch_bytes(int ctas, int threads);
 

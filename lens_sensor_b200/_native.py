@@ -157,6 +157,7 @@ SIGNATURES = {
     'lens_tb2d_step': (c_int, [POINTER(TB2D), c_void_p, c_void_p, c_int, c_int, c_int, POINTER(StepTable), c_int,
                                c_int, c_void_p]),
     'lens_rs2d_plan': (c_int, [POINTER(Inst2D), c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    'lens_rs2d_bands': (c_int, [POINTER(Inst2D), c_int, c_int, c_int, POINTER(ctypes.c_short), c_int]),
     'lens_rs2d_scratch_bytes': (ctypes.c_size_t, [c_int, c_int]),
     'lens_rs2d_run': (c_int, [POINTER(Inst2D), c_void_p, POINTER(RsOut2D), c_int, POINTER(StepTable), c_int, c_int,
                               c_void_p, ctypes.c_size_t, c_void_p, c_void_p]),

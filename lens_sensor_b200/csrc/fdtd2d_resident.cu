@@ -719,6 +719,25 @@ int rs_bands(const LensInst2D &g, int T, int rmx, short *lo) {
     return n;
 }
 
+// The least band cost T with which the instances' bands (at most rmx rows each)
+// number at most avail; -1 when none does.
+int rs_threshold(const LensInst2D *inst, int ninst, int avail, int rmx) {
+    auto count = [&](int T) {
+        long n = 0;
+        for (int q = 0; q < ninst; ++q) n += rs_bands(inst[q], T, rmx, nullptr);
+        return n;
+    };
+    int hi_t = rmx * RS_COST_SPECIAL;  // every band at most rmx rows
+    if (avail < 1 || count(hi_t) > avail) return -1;
+    int lo_t = RS_COST_LEAN - 1;        // infeasible: one lean row per band is the least
+    while (hi_t - lo_t > 1) {
+        const int mid = (lo_t + hi_t) / 2;
+        if (count(mid) <= avail) hi_t = mid;
+        else lo_t = mid;
+    }
+    return hi_t;
+}
+
 // Plan of a resident group on this device: the row template RM, the most rows of
 // a band, warps per CTA, the CTA count, the coefficients per row and (when lo is
 // not NULL) the first row of every band, instance after instance.  The bands
@@ -742,11 +761,6 @@ int rs_plan(const LensInst2D *inst, int ninst, int &rm, int &rows, int &W, int &
         cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         return LENS_ERR_CUDA;
     const bool wide = 32 * W > RS_NT_NARROW;
-    auto count = [&](int T, int rmx) {
-        long n = 0;
-        for (int q = 0; q < ninst; ++q) n += rs_bands(inst[q], T, rmx, nullptr);
-        return n;
-    };
     int best_t = -1, best_rm = 0;
     for (int t = 0; t < RS_NRM; ++t) {
         const int cand = RS_RM[t];
@@ -758,16 +772,9 @@ int rs_plan(const LensInst2D *inst, int ninst, int &rm, int &rows, int &W, int &
         int per = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 32 * W, sm) != cudaSuccess) return LENS_ERR_CUDA;
         const long avail = std::min((long)per * nsm, (long)RS_MAXCTA);
-        int hi_t = cand * RS_COST_SPECIAL;  // every band at most `cand` rows
-        if (avail < 1 || count(hi_t, cand) > avail) continue;
-        int lo_t = RS_COST_LEAN - 1;         // infeasible: one lean row per band is the least
-        while (hi_t - lo_t > 1) {
-            const int mid = (lo_t + hi_t) / 2;
-            if (count(mid, cand) <= avail) hi_t = mid;
-            else lo_t = mid;
-        }
-        if (best_t < 0 || hi_t < best_t) {
-            best_t = hi_t;
+        const int tt = rs_threshold(inst, ninst, (int)avail, cand);
+        if (tt > 0 && (best_t < 0 || tt < best_t)) {
+            best_t = tt;
             best_rm = cand;
         }
     }
@@ -801,6 +808,18 @@ extern "C" int lens_rs2d_plan(const LensInst2D *inst, int ninst, int *rows, int 
     if (ctas) *ctas = n;
     if (threads) *threads = 32 * W;
     return LENS_OK;
+}
+
+extern "C" int lens_rs2d_bands(const LensInst2D *inst, int ninst, int ctas, int max_rows, short *first_rows,
+                               int capacity) {
+    if (!inst || ninst < 1 || ctas < 1 || max_rows < 1 || !first_rows || capacity < 1) return LENS_ERR_ARG;
+    for (int q = 0; q < ninst; ++q)
+        if (!rs_inst_ok(inst[q]) || inst[q].nx > 32767) return LENS_ERR_ARG;
+    const int T = rs_threshold(inst, ninst, std::min(ctas, capacity), max_rows);
+    if (T < 0) return LENS_ERR_SIZE;
+    int n = 0;
+    for (int q = 0; q < ninst; ++q) n += rs_bands(inst[q], T, max_rows, first_rows + n);
+    return n;
 }
 
 extern "C" size_t lens_rs2d_scratch_bytes(int ctas, int threads) {

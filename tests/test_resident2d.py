@@ -222,3 +222,40 @@ def test_watchdog_ends_the_launch():
     g.step(sw.table, 0, 20)
     torch.cuda.synchronize()
     g.check()
+
+
+def _strip_inst(nx, ny, strip=12, src=30):
+    """A descriptor with x CPML strips of `strip` rows at both ends and a source
+    pair at rows src, src+1 (placeholder pointers: host logic only)."""
+    s = _fake_inst(nx, ny, 0)
+    s.ax.e = N.Profile(16, 16, 16, nx, strip, strip)
+    s.ax.h = N.Profile(16, 16, 16, nx - 1, strip, strip)
+    s.src = N.Source(src, 16, 16, 16, ny, 1, ny)
+    return s
+
+
+def test_band_partition_on_the_host():
+    """lens_rs2d_bands (no device): every row in exactly one band, bands within
+    the row limit and the CTA count, bands holding x-strip / source / face rows
+    shorter than the others, each instance starting at its row 0."""
+    lib = N.load()
+    nx = 1600
+    arr = (N.Inst2D * 2)(_strip_inst(nx, 480), _strip_inst(700, 300, strip=10, src=40))
+    buf = (ctypes.c_short * 512)()
+    n = lib.lens_rs2d_bands(arr, 2, 200, 16, buf, 512)
+    assert 0 < n <= 200
+    first = list(buf[:n])
+    starts = [b for b in range(n) if first[b] == 0]
+    assert starts == [0, starts[1]] and len(starts) == 2
+    for (a, b), size in (((0, starts[1]), nx), ((starts[1], n), 700)):
+        rows = first[a:b] + [size]
+        lens = [rows[k + 1] - rows[k] for k in range(b - a)]
+        assert min(lens) >= 1 and max(lens) <= 16 and sum(lens) == size
+        if size == nx:   # rows of the x strips (H: i < 12 or i >= nx-13; E: i >= nx-12), faces, source
+            sp_row = lambda i: i < 12 or i >= nx - 13 or i in (30, 31)
+            special = lambda lo, hi: any(sp_row(i) for i in range(lo, hi))
+            sp = [ln for lo, ln in zip(rows, lens) if special(lo, lo + ln)]
+            lean = [ln for lo, ln in zip(rows, lens) if not special(lo, lo + ln)]
+            assert 2 * max(sp) <= max(lean), (sp, lean)   # a special row costs 3.4 lean rows
+    assert lib.lens_rs2d_bands(arr, 2, 20, 16, buf, 512) == ERR_SIZE        # 2300 rows in 20 bands of 16
+    assert lib.lens_rs2d_bands(arr, 2, 200, 16, buf, 0) == ERR_ARG

@@ -108,9 +108,10 @@ def split_steps(K, steps_total, n_acc):
     return K - kb, kb
 
 
-def cpu_baseline(spec, steps=16):
+def cpu_baseline(spec, steps=16, warmup=1):
     """The NumPy oracle (restatement of the reference path) on a bounded sample:
-    `steps` consecutive full-grid steps with the detector sums, one host thread."""
+    `steps` consecutive full-grid steps with the detector sums, one host thread,
+    after `warmup` untimed steps."""
     from oracle import harness as H
     from oracle import fdtd_oracle as O
     c = oracle_case(spec)
@@ -119,9 +120,10 @@ def cpu_baseline(spec, steps=16):
                  s['da'], s['src'], 'Ey' if spec.pol == 'p' else 'Ez')
     nsp = s['n_sp']
     box = (slice(64, 130), slice(100, 167), slice(nsp, spec.nz - nsp))
-    g.step(0, 0.0)
+    for n in range(max(1, warmup)):
+        g.step(n, 0.0)
     t0 = time.perf_counter()
-    for n in range(1, steps + 1):
+    for n in range(max(1, warmup), max(1, warmup) + steps):
         g.step(n, 0.5)
         g.box_e2(*box)
     dt = time.perf_counter() - t0
@@ -147,8 +149,9 @@ def reference_arm(args):
     spec, steps_total = waveguide3d_tm()
     # each step: one full-grid oracle step; bounded so the arm ends within minutes
     k = max(1, min(args.steps, 12))
-    value, info = cpu_baseline(spec, steps=k)
-    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=k, warmup=1,
+    w = max(1, min(args.warmup, 10))
+    value, info = cpu_baseline(spec, steps=k, warmup=w)
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=k, warmup=w,
                 ms_per_step=spec.nx * spec.ny * spec.nz / value * 1e3, higher_is_better=True,
                 scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
                 config=dict(workload=WORKLOAD, cells=spec.nx * spec.ny * spec.nz, steps_total=steps_total),

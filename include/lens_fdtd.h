@@ -340,7 +340,10 @@ size_t lens_rs2d_scratch_bytes(int ctas, int threads);
 /* Advance every instance by nsteps from batch step n0.  inst_host / inst_dev:
  * the same descriptors in host and device memory; out: NULL or ninst entries
  * (host memory); scratch: scratch_bytes of device memory; err: a device int.
- * The call zeroes scratch and *err on `stream` before the launch.            */
+ * The call zeroes scratch and *err on `stream` before the launch.  The launch
+ * occupies every SM it plans for (one band per SM) and its bands wait on each
+ * other: issue resident launches one after another (one stream, or streams
+ * ordered by events), not side by side with other long-running work.         */
 int lens_rs2d_run(const LensInst2D *inst_host, const LensInst2D *inst_dev, const LensRsOut2D *out, int ninst,
                   const LensStepTable *tab, int n0, int nsteps, void *scratch, size_t scratch_bytes, int *err,
                   void *stream);

@@ -303,6 +303,7 @@ def run_planar2d(cpu=True):
     s = Solve2D(sp, steps, engine=best, by=best_by)
     if best in ('batch', 'tb'):
         s.capture()
+    s.stage_host()
     s.run()
     ph, snaps = s.host_results()
     t_e2e = time.perf_counter() - t0

@@ -12,6 +12,7 @@ same windows.
 """
 import contextlib
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -20,6 +21,15 @@ from . import engine as E
 from ._native import F32 as N_F32
 from . import _native as N
 from .geometry import Spec2D, build_2d
+
+_HOST_POOL = ThreadPoolExecutor(1, thread_name_prefix='lens-host-stage-2d')
+
+
+def _touched(shape, dtype):
+    """A host array written once, so that its pages are resident before a copy lands in it."""
+    a = np.empty(shape, dtype)
+    a.view(np.uint8).fill(0)
+    return a
 
 
 def schedule_2d(sp: Spec2D, steps_total, periods=1, snap_every=200):
@@ -188,11 +198,28 @@ class Solve2D:
             return self.inst.phasor()
         return (2.0 / self.n_acc) * self.epi.phasor()
 
+    def stage_host(self):
+        """Prepare the host destinations of host_results() on a background thread
+        so that it overlaps the stepping (call before run()): a copy into pages
+        that are already resident runs at the link's pageable rate instead of
+        faulting the pages in (config 0's 30 snapshots, 92 MB: 0.04 s fresh)."""
+        shp = (self.spec.nx, self.spec.ny)
+        self._staged = _HOST_POOL.submit(lambda: (_touched(shp, np.complex64),
+                                                  _touched(tuple(self.snaps.shape), np.float32)))
+        return self
+
     def host_results(self):
         """Phasor (complex64, the reference's CW dtype) and snapshots (float32) on
-        the host; d2h_bytes counts what crossed."""
-        ph = self.phasor().to(torch.complex64).cpu().numpy()
-        snaps = self.snaps.cpu().numpy()
+        the host, into the buffers stage_host() prepared when it was called;
+        d2h_bytes counts what crossed."""
+        staged, self._staged = getattr(self, '_staged', None), None
+        ph_d = self.phasor().to(torch.complex64)
+        if staged is not None:
+            ph, snaps = staged.result()
+            torch.from_numpy(ph).copy_(ph_d)
+            torch.from_numpy(snaps).copy_(self.snaps)
+        else:
+            ph, snaps = ph_d.cpu().numpy(), self.snaps.cpu().numpy()
         self.d2h_bytes = ph.nbytes + snaps.nbytes
         return ph, snaps
 

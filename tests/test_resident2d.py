@@ -259,3 +259,19 @@ def test_band_partition_on_the_host():
             assert 2 * max(sp) <= max(lean), (sp, lean)   # a special row costs 3.4 lean rows
     assert lib.lens_rs2d_bands(arr, 2, 20, 16, buf, 512) == ERR_SIZE        # 2300 rows in 20 bands of 16
     assert lib.lens_rs2d_bands(arr, 2, 200, 16, buf, 0) == ERR_ARG
+
+
+@pytest.mark.gpu
+def test_staged_host_results_equal_direct():
+    """Solve2D.stage_host() (host buffers prepared while the device steps) gives
+    the same phasor and snapshots as the direct read-back."""
+    from lens_sensor_b200.solver2d import Solve2D
+    sp = _specs(1)[0]
+    a = Solve2D(sp, 400, snap_every=100)
+    b = Solve2D(sp, 400, snap_every=100, geo=a.geo)
+    a.run()
+    b.stage_host().run()
+    pa, sa = a.host_results()
+    pb, sb = b.host_results()
+    assert sa.shape == sb.shape == (4, sp.nx, sp.ny)
+    assert np.array_equal(pa, pb) and np.array_equal(sa, sb)

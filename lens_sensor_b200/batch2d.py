@@ -512,7 +512,7 @@ class Sweep:
 
 
 def gated_sweep(specs, steps, storage='f16', tol=1e-4, probe_every=16, by=8, budget=None, device=None,
-                geos=None):
+                geos=None, resident=True):
     """A sweep whose FP16 / BF16 field storage is accepted only where it meets
     `tol` (relative L2 phasor error).
 
@@ -522,7 +522,8 @@ def gated_sweep(specs, steps, storage='f16', tol=1e-4, probe_every=16, by=8, bud
     storage and FP32; a polarisation keeps the reduced storage for its other
     instances only if every one of its probes' phasor error against FP32 is
     within tol / 2 (half the bar, as margin for the instances not probed), and
-    runs in FP32 otherwise.  Probes keep their FP32 results.
+    runs in FP32 otherwise.  Probes keep their FP32 results.  resident: the FP32
+    runs use resident launches (Sweep(resident=True)) where the instances fit.
 
     Returns (results in the order of specs, each with its 'storage', and a
     report: the probes' errors, the accepted polarisations and the instance
@@ -536,8 +537,16 @@ def gated_sweep(specs, steps, storage='f16', tol=1e-4, probe_every=16, by=8, bud
         idx = [q for q in range(n) if specs[q].pol == pol]
         probes += idx[::max(1, int(probe_every))]
     probes.sort()
-    sub = lambda ids, st: Sweep([specs[q] for q in ids], steps, st, by=by, budget=budget, device=device,
-                                geos=[geos[q] for q in ids])
+    def sub(ids, st):
+        """The sweep of instances ids in storage st; FP32 on resident launches
+        when `resident` and they fit the chip, else on the batched launches."""
+        kw = dict(by=by, budget=budget, device=device, geos=[geos[q] for q in ids])
+        if st == 'f32' and resident:
+            try:
+                return Sweep([specs[q] for q in ids], steps, st, resident=True, **kw)
+            except ValueError:
+                pass
+        return Sweep([specs[q] for q in ids], steps, st, **kw)
     out = [None] * n
     errs = {}
     if probes:

@@ -169,7 +169,7 @@ class _FakeSweep:
     storage adds a relative error of 1e-6 (TE) or 1e-3 (TM)."""
     runs = []
 
-    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None):
+    def __init__(self, specs, steps, storage='f32', by=8, budget=None, device=None, geos=None, resident=False):
         self.specs, self.storage = specs, storage
         _FakeSweep.runs.append((storage, [sp.tag for sp in specs]))
 
